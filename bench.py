@@ -1,0 +1,326 @@
+"""Benchmark of the PageRank hot path (one JSON line on rank 0).
+
+Default workload (the headline): plain PageRank on a directed R-MAT scale-22
+graph (4,194,304 vertices, edgefactor 16, a/b/c/d 0.57/0.19/0.19/0.05,
+seed 1, self-loops and duplicates removed, unweighted), alpha 0.85.  A step
+is one full solve of SWEEPS sweeps with tol = 0 (the reference's stop rule
+ends a scale-22 solve after one sweep, so throughput is measured at a fixed
+sweep count): set-up, SWEEPS fused sweeps, the FP64 correction sweep and the
+normalisation.  value = GTEPS per sweep = nnz * SWEEPS / step time, summed
+over ranks (replicas: every rank solves its own copy; scaling "weak").
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload rmat22|rmat25w|ppr|batch|serving]
+
+--impl reference times the reference's own CPU algorithm for the path (the
+oracle's port of cpp_easygraph's OpenMP _pagerank, all host threads) on the
+same workload and prints the same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PageRank GTEPS/iter + HBM GB/s; PPR solves/s and p99 at L1 err ≤1e-6"
+L2_BYTES = 126 * 2**20
+SWEEPS = 20
+
+
+def _rank_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel_file):
+    """dram bytes per launch recorded by an ncu capture summary under profiles/."""
+    p = ROOT / "profiles" / kernel_file
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch_full:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        ids = [x.strip() for x in vis.split(",")] if vis else None
+        self.index = ids[local_rank] if ids and local_rank < len(ids) else str(local_rank)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.index], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_port(csr, alpha, budget_s=10.0):
+    """The oracle's port of the reference's OpenMP CPU PageRank, timed on this host."""
+    from oracle import oracle
+
+    threads = oracle.max_threads()
+    sweeps_done, t_total = 0, 0.0
+    while t_total < budget_s or sweeps_done < 2:
+        t0 = time.perf_counter()
+        _, sw = oracle.cpu_pagerank_omp(csr.V, csr.E, csr.W, alpha=alpha, max_iter=2, threshold=0.0, threads=threads)
+        t_total += time.perf_counter() - t0
+        sweeps_done += sw
+    return {"value": csr.m * sweeps_done / t_total / 1e9, "unit": "GTEPS/iter", "cores": threads, "kind": "port",
+            "sample": f"{sweeps_done} sweeps of the same graph in solves of 2 sweeps (tol 0), "
+                      f"{t_total:.1f} s, OpenMP push with atomics (cpp_easygraph pagerank.cpp:21-122 port)"}
+
+
+def make_workload(name):
+    from eggpu_b200 import synth
+
+    if name == "rmat22":
+        csr = synth.rmat(scale=22, edgefactor=16, seed=1)
+        desc = ("R-MAT scale 22 (4,194,304 vertices, edgefactor 16, a/b/c/d 0.57/0.19/0.19/0.05, seed 1, "
+                "self-loops and duplicates removed, unweighted), alpha 0.85")
+    elif name == "rmat25w":
+        csr = synth.rmat(scale=25, edgefactor=16, seed=2, weighted=True)
+        desc = ("R-MAT scale 25 (33,554,432 vertices, edgefactor 16, seed 2), weights i.i.d. U(0,1] FP32, "
+                "weighted out-degree normalisation, alpha 0.85")
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return csr, desc
+
+
+def run_reference(args):
+    rank, world, _ = _rank_env()
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    csr, desc = make_workload(args.workload)
+    threads = oracle.max_threads()
+    sweeps = 2
+    for _ in range(args.warmup):
+        oracle.cpu_pagerank_omp(csr.V, csr.E, csr.W, alpha=0.85, max_iter=1, threshold=0.0, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, sw = oracle.cpu_pagerank_omp(csr.V, csr.E, csr.W, alpha=0.85, max_iter=sweeps, threshold=0.0,
+                                        threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    value = csr.m * sweeps / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS/iter", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {desc}", "n": csr.n, "nnz": csr.m, "sweeps_per_step": sweeps,
+                   "tol": 0.0},
+        "cpu_baseline": {"value": value, "unit": "GTEPS/iter", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} solves of {sweeps} sweeps on the full graph; OpenMP port of "
+                                   "cpp_easygraph/functions/pagerank/pagerank.cpp:21-122 (the reference's C++ "
+                                   "CPU PageRank needs pybind11/CPython to build, so the port is timed)"},
+        "e2e": {"value": value, "unit": "GTEPS/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    from eggpu_b200 import _native
+
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", device_id=torch.device("cuda", local))
+        dist = dist_mod
+    csr, desc = make_workload(args.workload)
+    pg = _native.PreparedGraph(csr.V, csr.E, csr.W)
+    nnz = pg.nnz
+    stream = torch.cuda.Stream()
+    pg.set_stream(stream.cuda_stream)
+    sweeps = args.sweeps
+
+    def timed(k, n_sweeps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(k):
+            pg.enqueue(alpha=0.85, max_iter=n_sweeps, tol=0.0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        _, st = pg.collect(copy=False)
+        return e0.elapsed_time(e1) / k / 1e3, st
+
+    for _ in range(max(args.warmup, 3)):
+        pg.enqueue(alpha=0.85, max_iter=sweeps, tol=0.0)
+    pg.collect(copy=False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_step, st = timed(args.steps, sweeps)
+        t_step2, st2 = timed(max(1, args.steps // 2), 2 * sweeps)
+    torch.cuda.synchronize()
+    if dist:
+        tt = torch.tensor([t_step, t_step2], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step, t_step2 = tt.tolist()
+        dist.barrier()
+    t_sweep = max((t_step2 - t_step) / sweeps, 1e-9)
+    bytes_per_iter = st["bytes_per_iter"]
+    value = world * nnz * sweeps / t_step / 1e9
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_iter / t_sweep / 1e9
+    traffic = profile_traffic(f"k_sweep_{args.workload}.md")
+    launches_per_step = st["launches"]
+
+    # end-to-end through the drop-in C ABI entry, host CSR in pinned memory
+    Vp = torch.from_numpy(csr.V).pin_memory().numpy()
+    Ep = torch.from_numpy(csr.E).pin_memory().numpy()
+    Wp = None if csr.W is None else torch.from_numpy(csr.W).pin_memory().numpy()
+    e2e_steps = max(2, min(args.steps, 5))
+    _native.cache_reset()
+    _native.pagerank_csr(Vp, Ep, Wp, 10**9 + rank, 0.85, sweeps, 0.0)  # warm the code path
+    _native.cache_reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        _native.pagerank_csr(Vp, Ep, Wp, 2 * 10**9 + i, 0.85, sweeps, 0.0)
+        _native.cache_reset()
+    t_e2e = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = tt.item()
+    h2d = csr.V.nbytes + csr.E.nbytes + (0 if csr.W is None else csr.W.nbytes)
+    e2e = {"value": world * nnz * sweeps / t_e2e / 1e9, "unit": "GTEPS/iter", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(8 * csr.n), "ms_per_step": t_e2e * 1e3,
+           "path": "egpr_pagerank_csr (drop-in for gpu_easygraph::pagerank): H2D of the out-edge CSR, GPU "
+                   "preparation, solve, D2H of FP64 ranks, every step"}
+
+    # reference stop rule on the same graph (one sweep at this size) and its accuracy vs the FP64 oracle
+    parity = None
+    if rank == 0 and not args.no_parity:
+        from oracle import oracle
+
+        ranks, pst = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+        ref, it_ref, _ = oracle.pagerank_pull(csr.V, csr.E, csr.W, alpha=0.85, max_iter=100, tol=1e-6)
+        parity = {"iterations": pst["iterations"], "oracle_iterations": it_ref,
+                  "l1_vs_fp64_oracle": float(np.abs(ranks - ref).sum()),
+                  "max_abs_vs_fp64_oracle": float(np.abs(ranks - ref).max()),
+                  "solve_ms": pst["kernel_seconds"] * 1e3}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(csr, 0.85, budget_s=args.cpu_seconds)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GTEPS/iter", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {desc}", "n": csr.n, "nnz": int(nnz),
+                       "sweeps_per_step": sweeps, "tol": 0.0, "parallelism": f"replicas{world}",
+                       "l2": f"inputs larger than L2 (inbound CSR {(4 * (csr.n + 1) + 4 * nnz) / 1e6:.0f} MB > "
+                             f"{L2_BYTES / 1e6:.0f} MB); the FP32 rank vectors are meant to stay L2-resident",
+                       "precision": "FP32 ranks and products, FP64 residual/dangling/sums, final FP64 sweep"},
+            "hbm_gbs": bytes_per_iter * sweeps / t_step / 1e9,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_sweep<float> (fused sweep)", "peak_source": peak_kind,
+                         "bytes_per_launch": bytes_per_iter, "launch_ms": t_sweep * 1e3,
+                         "timing": "CUDA events on the launch stream; per-sweep time = (T(2S) - T(S)) / S"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches_per_step * args.steps + st2["launches"] * max(1, args.steps // 2)),
+            "gpu_launches_per_step": launches_per_step,
+            "clocks": clk.summary(),
+            "parity": parity,
+        }
+        print(json.dumps(line), flush=True)
+    pg.set_stream(None)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="rmat22")
+    ap.add_argument("--sweeps", type=int, default=SWEEPS)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,319 @@
+"""ctypes binding of libegpr.so (the C ABI declared in include/egpr.h).
+
+This module is the only place Python touches the native engine.  Importing it
+loads ``eggpu_b200/libegpr.so``; if the library is missing the import fails
+with instructions to build it — there is no CPU fallback.  Every pointer handed
+to the library is a host pointer to a contiguous numpy array.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libegpr.so"
+
+# Status codes (include/egpr.h); 0..6 keep gpu_easygraph's EG_GPU_STATUS_CODE numbering.
+EGPR_SUCC = 0
+EGPR_FAILED_TO_ALLOCATE_HOST_MEM = 1
+EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM = 2
+EGPR_DEVICE_ERR = 3
+EGPR_UNKNOWN_ERROR = 4
+EGPR_UNSUPPORTED_GRAPH = 5
+EGPR_NEGATIVE_CYCLE = 6
+EGPR_TIMEOUT = 7
+EGPR_INVALID_ARGUMENT = 8
+
+EGPR_FLAG_NO_CORRECTION = 1
+
+
+class EgprStats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", c_int32),
+        ("converged", c_int32),
+        ("residual", c_double),
+        ("kernel_seconds", c_double),
+        ("total_seconds", c_double),
+        ("bytes_per_iter", c_int64),
+        ("launches", c_int32),
+        ("reserved", c_int32),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class EgprGraphInfo(ctypes.Structure):
+    _fields_ = [
+        ("n", c_int32),
+        ("device", c_int32),
+        ("m_input", c_int64),
+        ("nnz", c_int64),
+        ("weighted", c_int32),
+        ("n_dangling", c_int32),
+        ("device_bytes", c_int64),
+        ("prep_seconds", c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class EgprCacheStats(ctypes.Structure):
+    _fields_ = [
+        ("graphs", c_int64),
+        ("device_bytes", c_int64),
+        ("hits", c_int64),
+        ("misses", c_int64),
+        ("evictions", c_int64),
+        ("budget_bytes", c_int64),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# (name, restype, argtypes) for every entry point of include/egpr.h.
+_SIGNATURES = [
+    ("egpr_status_string", c_char_p, [c_int]),
+    ("egpr_last_error", c_char_p, []),
+    ("egpr_graph_create", c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_int64, POINTER(c_void_p)]),
+    ("egpr_graph_destroy", c_int, [c_void_p]),
+    ("egpr_graph_info_get", c_int, [c_void_p, POINTER(EgprGraphInfo)]),
+    ("egpr_graph_export_inbound", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("egpr_graph_set_stream", c_int, [c_void_p, c_void_p]),
+    ("egpr_pagerank", c_int, [c_void_p, c_double, c_int32, c_double, c_void_p, c_uint32, c_void_p, POINTER(EgprStats)]),
+    ("egpr_pagerank_enqueue", c_int, [c_void_p, c_double, c_int32, c_double, c_uint32]),
+    ("egpr_pagerank_collect", c_int, [c_void_p, c_void_p, POINTER(EgprStats)]),
+    ("egpr_pagerank_batch", c_int,
+     [c_void_p, c_double, c_int32, c_double, c_int32, c_void_p, c_uint32, c_void_p, c_void_p]),
+    ("egpr_pagerank_seeds", c_int,
+     [c_void_p, c_double, c_int32, c_double, c_int32, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
+    ("egpr_pagerank_multi", c_int,
+     [c_int32, c_void_p, c_double, c_int32, c_double, c_uint32, c_void_p, c_void_p]),
+    ("egpr_pagerank_csr", c_int,
+     [c_void_p, c_int32, c_void_p, c_int64, c_void_p, c_uint64, c_double, c_int32, c_double, c_void_p,
+      POINTER(c_double)]),
+    ("egpr_cache_stats_get", c_int, [POINTER(EgprCacheStats)]),
+    ("egpr_cache_reset", c_int, []),
+    ("egpr_cache_set_budget", c_int, [c_int64]),
+]
+
+EXPORTED_SYMBOLS = tuple(name for name, _, _ in _SIGNATURES)
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is not built; run `python -m eggpu_b200.build` (needs nvcc). "
+            "eggpu_b200 has no CPU fallback."
+        )
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, restype, argtypes in _SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    return lib
+
+
+lib = _load()
+
+
+class EgprError(RuntimeError):
+    """A non-zero status from libegpr (message = egpr_status_string + detail)."""
+
+    def __init__(self, status: int, where: str = ""):
+        self.status = int(status)
+        detail = lib.egpr_last_error().decode(errors="replace")
+        msg = lib.egpr_status_string(self.status).decode(errors="replace")
+        if detail:
+            msg = f"{msg} ({detail})"
+        if where:
+            msg = f"{where}: {msg}"
+        super().__init__(msg)
+
+
+def check(status: int, where: str = "") -> None:
+    if status != EGPR_SUCC:
+        raise EgprError(status, where)
+
+
+def status_string(status: int) -> str:
+    return lib.egpr_status_string(int(status)).decode()
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(c_void_p)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class PreparedGraph:
+    """A graph prepared on the current CUDA device (owns an ``egpr_graph``).
+
+    ``V``/``E``/``W`` form an out-edge CSR: ``V`` int32[n+1], ``E`` int32[m],
+    ``W`` float64[m] or None for unit weights.
+    """
+
+    def __init__(self, V, E, W=None):
+        V = _i32(V)
+        E = _i32(E)
+        W = None if W is None else _f64(W)
+        n = int(V.shape[0]) - 1
+        m = int(E.shape[0])
+        if W is not None and W.shape[0] != m:
+            raise ValueError("W must have one weight per CSR entry")
+        h = c_void_p()
+        check(lib.egpr_graph_create(_ptr(V), _ptr(E), _ptr(W), n, m, ctypes.byref(h)), "egpr_graph_create")
+        self._h = h
+        self._lock = threading.Lock()
+        info = self.info()
+        self.n = info["n"]
+        self.nnz = info["nnz"]
+        self.m_input = info["m_input"]
+        self.weighted = bool(info["weighted"])
+        self.device = info["device"]
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("PreparedGraph is closed")
+        return self._h
+
+    def info(self) -> dict:
+        inf = EgprGraphInfo()
+        check(lib.egpr_graph_info_get(self.handle, ctypes.byref(inf)), "egpr_graph_info_get")
+        return inf.as_dict()
+
+    def export_inbound(self):
+        """(in_row, in_col, in_w float32, dangling01, out_weight_sum) copied to the host."""
+        n, nnz = self.n, self.nnz
+        in_row = np.empty(n + 1, np.int32)
+        in_col = np.empty(max(nnz, 1), np.int32)
+        in_w = np.empty(max(nnz, 1), np.float32)
+        dang = np.empty(n, np.int32)
+        outw = np.empty(n, np.float64)
+        check(lib.egpr_graph_export_inbound(self.handle, _ptr(in_row), _ptr(in_col), _ptr(in_w), _ptr(dang), _ptr(outw)),
+              "egpr_graph_export_inbound")
+        return in_row, in_col[:nnz], in_w[:nnz], dang, outw
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(lib.egpr_graph_set_stream(self.handle, None if not stream_ptr else c_void_p(int(stream_ptr))),
+              "egpr_graph_set_stream")
+
+    def pagerank(self, alpha=0.85, max_iter=100, tol=1e-6, personalization=None, correction=True, out=None):
+        """Returns (ranks float64[n], stats dict)."""
+        res = np.empty(self.n, np.float64) if out is None else out
+        pers = None if personalization is None else _f64(personalization)
+        if pers is not None and pers.shape[0] != self.n:
+            raise ValueError("personalization must have n entries")
+        st = EgprStats()
+        flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
+        check(lib.egpr_pagerank(self.handle, float(alpha), int(max_iter), float(tol), _ptr(pers), flags, _ptr(res),
+                                ctypes.byref(st)), "egpr_pagerank")
+        return res, st.as_dict()
+
+    def enqueue(self, alpha=0.85, max_iter=100, tol=1e-6, correction=True) -> None:
+        flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
+        check(lib.egpr_pagerank_enqueue(self.handle, float(alpha), int(max_iter), float(tol), flags),
+              "egpr_pagerank_enqueue")
+
+    def collect(self, out=None, copy=True):
+        res = None
+        if copy:
+            res = np.empty(self.n, np.float64) if out is None else out
+        st = EgprStats()
+        check(lib.egpr_pagerank_collect(self.handle, _ptr(res), ctypes.byref(st)), "egpr_pagerank_collect")
+        return res, st.as_dict()
+
+    def pagerank_batch(self, teleport, alpha=0.85, max_iter=100, tol=1e-6, correction=True):
+        """teleport: (k, n) array of non-negative vectors. Returns ((k, n) ranks, [stats])."""
+        T = _f64(teleport)
+        if T.ndim != 2 or T.shape[1] != self.n:
+            raise ValueError("teleport must have shape (k, n)")
+        k = T.shape[0]
+        res = np.empty((k, self.n), np.float64)
+        sts = (EgprStats * k)()
+        flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
+        check(lib.egpr_pagerank_batch(self.handle, float(alpha), int(max_iter), float(tol), k, _ptr(T), flags,
+                                      _ptr(res), ctypes.cast(sts, c_void_p)), "egpr_pagerank_batch")
+        return res, [s.as_dict() for s in sts]
+
+    def pagerank_seeds(self, seed_sets, alpha=0.85, max_iter=100, tol=1e-6, correction=True):
+        """seed_sets: list of vertex-id sequences (uniform teleport over each)."""
+        k = len(seed_sets)
+        ptr = np.zeros(k + 1, np.int32)
+        for j, s in enumerate(seed_sets):
+            ptr[j + 1] = ptr[j] + len(s)
+        seeds = np.concatenate([np.asarray(s, np.int32) for s in seed_sets]) if k else np.zeros(0, np.int32)
+        seeds = _i32(seeds)
+        res = np.empty((k, self.n), np.float64)
+        sts = (EgprStats * k)()
+        flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
+        check(lib.egpr_pagerank_seeds(self.handle, float(alpha), int(max_iter), float(tol), k, _ptr(ptr),
+                                      _ptr(seeds) if seeds.size else None, flags, _ptr(res),
+                                      ctypes.cast(sts, c_void_p)), "egpr_pagerank_seeds")
+        return res, [s.as_dict() for s in sts]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            lib.egpr_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6, correction=True):
+    """Solves many prepared graphs in one persistent launch per sweep."""
+    count = len(graphs)
+    handles = (c_void_p * count)(*[g.handle for g in graphs])
+    outs = [np.empty(g.n, np.float64) for g in graphs]
+    out_ptrs = (c_void_p * count)(*[o.ctypes.data for o in outs])
+    sts = (EgprStats * count)()
+    flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
+    check(lib.egpr_pagerank_multi(count, ctypes.cast(handles, c_void_p), float(alpha), int(max_iter), float(tol),
+                                  flags, ctypes.cast(out_ptrs, c_void_p), ctypes.cast(sts, c_void_p)),
+          "egpr_pagerank_multi")
+    return outs, [s.as_dict() for s in sts]
+
+
+def pagerank_csr(V, E, W, graph_id, alpha, max_iter, threshold):
+    """Drop-in for gpu_easygraph::pagerank: returns (PR float64[n], kernel_seconds)."""
+    V = _i32(V)
+    E = _i32(E)
+    W = None if W is None or len(W) == 0 else _f64(W)
+    n = int(V.shape[0]) - 1
+    PR = np.empty(max(n, 0), np.float64)
+    ks = c_double(0.0)
+    check(lib.egpr_pagerank_csr(_ptr(V), int(V.shape[0]), _ptr(E), int(E.shape[0]), _ptr(W), int(graph_id) & (2**64 - 1),
+                                float(alpha), int(max_iter), float(threshold), _ptr(PR), ctypes.byref(ks)),
+          "egpr_pagerank_csr")
+    return PR, ks.value
+
+
+def cache_stats() -> dict:
+    cs = EgprCacheStats()
+    check(lib.egpr_cache_stats_get(ctypes.byref(cs)), "egpr_cache_stats_get")
+    return cs.as_dict()
+
+
+def cache_reset() -> None:
+    check(lib.egpr_cache_reset(), "egpr_cache_reset")
+
+
+def cache_set_budget(nbytes: int) -> None:
+    check(lib.egpr_cache_set_budget(int(nbytes)), "egpr_cache_set_budget")

@@ -1,0 +1,193 @@
+// Internal declarations shared by the CUDA translation units of libegpr.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/egpr.h"
+
+namespace egpr {
+
+// ---------------------------------------------------------------------------
+// Work decomposition.
+//
+// A graph's merge path has n + nnz items (one "row end" per vertex plus one
+// item per inbound entry).  It is cut into sub-tiles of kSubItems items; a
+// CTA processes one sub-tile at a time entirely in shared memory.  Runs of
+// consecutive sub-tiles form chunks, the unit of the persistent work queue.
+// A row cut by a chunk boundary is a "span": each chunk it touches leaves a
+// partial sum, and the last of them to finish combines the partials in
+// chunk order (no waiting, deterministic).
+// ---------------------------------------------------------------------------
+constexpr int kThreads = 256;
+constexpr int kItemsPerThread = 8;
+constexpr int kSubItems = kThreads * kItemsPerThread;
+
+// Chunk flags.
+constexpr int32_t kHasHead = 1;    // the chunk's first row began in an earlier chunk
+constexpr int32_t kHasTail = 2;    // the chunk's last row continues into a later chunk
+constexpr int32_t kInterior = 4;   // the chunk lies inside one row (head and tail are that row)
+
+struct Chunk {
+    int32_t sub_begin;   // first sub-tile (index into the graph's sub_coord table)
+    int32_t sub_end;     // one past the last sub-tile
+    int32_t graph;       // slot in the plan's graph table
+    int32_t flags;
+    int32_t head_ta;     // global chunk id where the head row's span starts
+    int32_t tail_tb;     // global chunk id where the tail row's span ends
+    int32_t tail_row;    // vertex id of the tail row (span rows are finalised by row id)
+    int32_t pad;
+};
+
+// Per-graph device view used by the sweep kernels.
+struct GraphDev {
+    const int32_t* in_row;   // n+1
+    const int32_t* in_col;   // nnz
+    const float* in_w;       // nnz, NULL = unit weights
+    const int2* sub_coord;   // merge-path coordinates (row, entry) of sub-tile starts
+    const double* outw;      // n, FP64 out-weight sums
+    const float* scale;      // n, alpha/outw (FP32) or -1 for dangling vertices
+    const float* tele;       // n, personalisation (NULL = uniform)
+    float* x[2];             // ranks, double-buffered
+    float* z[2];             // x * scale: the value each out-edge carries
+    double* out;             // n, FP64 result
+    double* z64;             // n, FP64 carried values for the correction sweep
+    int32_t n;
+    int32_t chunk_begin;     // this graph's global chunk id range
+    int32_t chunk_end;
+    int32_t pad;
+};
+
+struct GraphState {
+    double alpha;
+    double c1;         // (1 - alpha) / n
+    double tol_n;      // tol * n
+    double dmass;      // alpha * (dangling mass) / n for the next sweep
+    double dmass_prev; // the value used by the last completed sweep
+    double residual;   // L1 of the last sweep
+    double residual64; // L1 of the FP64 correction sweep against x_{k-1}
+    double xsum;       // sum of the last sweep's ranks (FP64 sweep: of the result)
+    double dsum;       // dangling mass of the last sweep's ranks
+    int32_t iter;
+    int32_t max_iter;
+    int32_t done;
+    int32_t converged;
+    uint32_t arrive;   // chunk arrivals in the running launch
+    int32_t personalised;  // teleport from GraphDev::tele instead of 1/n
+};
+
+struct Ctl {
+    uint32_t queue;    // work-queue head
+    uint32_t exited;   // CTAs that left the queue loop
+    int32_t active;    // graphs still iterating
+    int32_t launches;  // sweep launches so far
+    int32_t cap;       // hard cap on sweep launches
+    int32_t error;
+};
+
+struct SweepParams {
+    const Chunk* chunks;
+    int32_t nchunks;
+    int32_t mode;            // 0 = FP32 sweep, 1 = FP64 correction sweep
+    const GraphDev* graphs;
+    GraphState* states;
+    double* chunk_part;      // 3 per chunk: err, dsum, xsum of rows finalised by the chunk
+    double* piece;           // 2 per chunk: head piece, tail piece
+    uint32_t* span_cnt;      // per chunk (span start)
+    double* span_part;       // 3 per chunk (span start): err, dsum, xsum of span rows
+    Ctl* ctl;
+    cudaGraphConditionalHandle cond;
+    int32_t use_cond;
+};
+
+// ---- device buffers --------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int alloc(size_t b);
+    void release();
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// ---- the work plan over one or more prepared graphs -------------------------
+struct Plan {
+    int32_t ngraphs = 0;
+    int32_t nchunks = 0;
+    int32_t grid = 0;        // CTAs of an FP32 sweep
+    int32_t grid_final = 0;  // CTAs of the FP64 correction sweep
+    int32_t max_n = 0;
+    DevBuf d_chunks, d_graphs, d_states, d_ndang, d_chunk_part, d_piece, d_span_cnt, d_span_part, d_ctl;
+    std::vector<Chunk> h_chunks;      // a graph's own chunk table (local ids)
+    std::vector<Chunk> h_chunks_all;  // the plan's table (global ids)
+    cudaGraph_t cg = nullptr;
+    cudaGraphExec_t cg_exec = nullptr;
+    cudaGraphConditionalHandle cond = 0;
+    bool cg_failed = false;
+    ~Plan();
+    void release();
+};
+
+// ---- prepared graph handle ---------------------------------------------------
+}  // namespace egpr
+
+struct egpr_graph {
+    std::mutex mu;
+    int device = -1;
+    int32_t n = 0;
+    int64_t m_input = 0;
+    int64_t nnz = 0;
+    int32_t weighted = 0;
+    int32_t n_dangling = 0;        // out-weight <= 0 (reference mask)
+    int32_t n_dangling_solve = 0;  // out-weight <= 1e-15 (EasyGraph CPU rule)
+    double prep_seconds = 0.0;
+    int32_t nsub = 0;              // sub-tiles
+    int32_t chunk_subs = 1;        // sub-tiles per chunk
+    // prepared graph
+    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord;
+    // solve workspace
+    egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
+    egpr::Plan plan;               // single-graph plan
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr; // active stream (own or user-given)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // state of an enqueued solve
+    bool pending = false;
+    int32_t pending_launches = 0;
+    double pending_t0 = 0.0;
+    int64_t device_bytes() const;
+};
+
+namespace egpr {
+
+// Status helpers.
+int set_cuda_error(cudaError_t e, const char* what);
+int check_device(const egpr_graph* g);
+double wall_seconds();
+
+// Preparation (prep.cu).
+int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
+
+// Plans and sweeps (sweep.cu).
+int sweep_occupancy_grid(int mode);
+int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_t stream);
+int plan_capture_loop(Plan& plan, cudaStream_t stream);
+GraphDev graph_dev_view(const egpr_graph* g);
+int launch_init(Plan& plan, double alpha, int32_t max_iter, double tol, bool personalised,
+                cudaStream_t stream);
+int launch_loop(Plan& plan, int32_t max_iter, cudaStream_t stream, int32_t* launches);
+int launch_finish(Plan& plan, bool correction, cudaStream_t stream, int32_t* launches);
+
+// SpMM personalised PageRank (spmm.cu).
+int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, int32_t k,
+                    const double* teleport_dense, const int32_t* seed_ptr, const int32_t* seeds,
+                    uint32_t flags, double* out, egpr_stats* stats);
+
+// Scan / sort helpers (prep.cu), exposed for the SpMM set-up.
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, cudaStream_t s);
+
+}  // namespace egpr

@@ -1,0 +1,495 @@
+// Device-side graph preparation.
+//
+// Replaces the reference's single-threaded host pass build_inbound_from_csr
+// (gpu_easygraph/functions/centrality/pagerank.cu:286-347) and its H2D of the
+// result (:472-518) with GPU kernels over the uploaded out-edge CSR:
+//
+//   k_out_weight     FP64 out-weight sum per source, accumulated in row order
+//                    after sanitising each weight (pagerank.cu:301-316)
+//   k_in_degree      in-degree histogram over valid endpoints (:315)
+//   exclusive scan   in_row (:319-320)
+//   radix sort       stable LSD sort of entry ids by destination: entries of
+//                    one destination keep ascending entry order, i.e. the
+//                    ascending-source order of the reference's sequential
+//                    scatter (:328-346)
+//   k_gather_inbound in_col / in_w from the sorted entry ids
+//   k_dangling       dangling mask outw <= 0 (:323-326) and the counts used by
+//                    the solver
+//   k_sub_coord      merge-path coordinates of every sub-tile start
+//
+// The results are bit-identical to build_inbound_from_csr for in_row, in_col,
+// the dangling mask and the FP64 out-weight sums.  The engine stores raw
+// (sanitised) FP32 weights instead of the alpha-scaled in_val, so a prepared
+// graph does not depend on alpha.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "egpr_internal.cuh"
+
+namespace egpr {
+namespace {
+
+constexpr int kScanPerThread = 8;
+constexpr int kScanTile = kThreads * kScanPerThread;
+constexpr int kRadixBits = 8;
+constexpr int kDigits = 1 << kRadixBits;
+constexpr int kSortPerLane = 16;
+constexpr int kWarps = kThreads / 32;
+constexpr int kSortTile = kThreads * kSortPerLane;
+
+// ---------------------------------------------------------------- scan -----
+// Exclusive scan of uint32 values, tile by tile; tile totals go to tile_sums.
+__global__ void __launch_bounds__(kThreads)
+k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int64_t len,
+             uint32_t* __restrict__ tile_sums) {
+    __shared__ uint32_t s[kScanTile];
+    __shared__ uint32_t warp_tot[kWarps];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < kScanPerThread; ++i) {
+        int64_t idx = base + tid + (int64_t)i * kThreads;
+        s[tid + i * kThreads] = idx < len ? in[idx] : 0u;
+    }
+    __syncthreads();
+    uint32_t v[kScanPerThread];
+    uint32_t run = 0;
+#pragma unroll
+    for (int i = 0; i < kScanPerThread; ++i) {
+        v[i] = run;
+        run += s[tid * kScanPerThread + i];
+    }
+    // inclusive warp scan of the thread totals
+    const int lane = tid & 31, warp = tid >> 5;
+    uint32_t inc = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    uint32_t warp_off = 0, block_tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        if (w < warp) warp_off += warp_tot[w];
+        block_tot += warp_tot[w];
+    }
+    const uint32_t excl = warp_off + inc - run;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kScanPerThread; ++i) s[tid * kScanPerThread + i] = v[i] + excl;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kScanPerThread; ++i) {
+        int64_t idx = base + tid + (int64_t)i * kThreads;
+        if (idx < len) out[idx] = s[tid + i * kThreads];
+    }
+    if (tid == 0 && tile_sums) tile_sums[blockIdx.x] = block_tot;
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, int64_t len, const uint32_t* __restrict__ tile_off) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < len) out[i] += tile_off[i / kScanTile];
+}
+
+// -------------------------------------------------------------- radix ------
+__global__ void __launch_bounds__(kThreads)
+k_radix_hist(const uint32_t* __restrict__ keys, int64_t len, int shift, int64_t ntiles,
+             uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[kDigits];
+    for (int d = threadIdx.x; d < kDigits; d += kThreads) h[d] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    for (int i = threadIdx.x; i < kSortTile; i += kThreads) {
+        int64_t idx = base + i;
+        if (idx < len) atomicAdd(&h[(keys[idx] >> shift) & (kDigits - 1)], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kDigits; d += kThreads) hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
+}
+
+// Stable scatter: within a tile, warp w owns items [w*32*kSortPerLane, ...) in
+// order; inside a warp, rounds of 32 consecutive items rank equal digits by
+// lane order.  Global order = tile order (digit-major scanned histogram),
+// then warp order, then item order.
+__global__ void __launch_bounds__(kThreads)
+k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t len,
+                int shift, int64_t ntiles, const uint32_t* __restrict__ offsets) {
+    __shared__ uint32_t warp_hist[kWarps][kDigits];
+    __shared__ uint32_t tile_off[kDigits];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < kWarps * kDigits; i += kThreads) (&warp_hist[0][0])[i] = 0;
+    for (int d = tid; d < kDigits; d += kThreads) tile_off[d] = offsets[(int64_t)d * ntiles + blockIdx.x];
+    __syncthreads();
+    const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortPerLane;
+    uint32_t key[kSortPerLane], val[kSortPerLane], rank[kSortPerLane];
+    const uint32_t lt_mask = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kSortPerLane; ++r) {
+        const int64_t idx = wbase + (int64_t)r * 32 + lane;
+        const bool valid = idx < len;
+        key[r] = valid ? keys_in[idx] : 0u;
+        val[r] = valid ? vals_in[idx] : 0u;
+        const uint32_t d = (key[r] >> shift) & (kDigits - 1);
+        const uint32_t tag = valid ? d : (uint32_t)(kDigits + lane);
+        const uint32_t peers = __match_any_sync(0xffffffffu, tag);
+        const uint32_t before = valid ? warp_hist[warp][d] : 0u;
+        __syncwarp();
+        if (valid && (peers & lt_mask) == 0u) warp_hist[warp][d] = before + __popc(peers);
+        __syncwarp();
+        rank[r] = before + __popc(peers & lt_mask);
+    }
+    __syncthreads();
+    for (int d = tid; d < kDigits; d += kThreads) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            uint32_t c = warp_hist[w][d];
+            warp_hist[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortPerLane; ++r) {
+        const int64_t idx = wbase + (int64_t)r * 32 + lane;
+        if (idx < len) {
+            const uint32_t d = (key[r] >> shift) & (kDigits - 1);
+            const uint32_t dst = tile_off[d] + warp_hist[warp][d] + rank[r];
+            keys_out[dst] = key[r];
+            vals_out[dst] = val[r];
+        }
+    }
+}
+
+// -------------------------------------------------------------- graph ------
+__device__ __forceinline__ double sanitize_w(double w) {
+    return (!isfinite(w) || w < 0.0) ? 0.0 : w;
+}
+
+// FP64 out-weight sum per source in entry order (pagerank.cu:301-316).  For
+// unit weights the sum is a count, which is exact in any order.
+__global__ void k_out_weight(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
+                             const double* __restrict__ W, int32_t n, double* __restrict__ outw) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = V[u], e = V[u + 1];
+        double s = 0.0;
+        if (W) {
+            for (int32_t p = b; p < e; ++p) {
+                const int32_t v = E[p];
+                if (v >= 0 && v < n) s += sanitize_w(W[p]);
+            }
+        } else {
+            int32_t c = 0;
+            for (int32_t p = b; p < e; ++p) {
+                const int32_t v = E[p];
+                c += (v >= 0 && v < n) ? 1 : 0;
+            }
+            s = (double)c;
+        }
+        outw[u] = s;
+    }
+}
+
+// In-degree histogram and the sort keys: destination, or n for an entry whose
+// destination is outside [0, n) (those sort last and are dropped).
+__global__ void k_in_degree_keys(const int32_t* __restrict__ E, int64_t m, int32_t n,
+                                 uint32_t* __restrict__ indeg, uint32_t* __restrict__ keys,
+                                 uint32_t* __restrict__ vals) {
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < m;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = E[p];
+        const bool ok = v >= 0 && v < n;
+        if (ok) atomicAdd(&indeg[v], 1u);
+        keys[p] = ok ? (uint32_t)v : (uint32_t)n;
+        vals[p] = (uint32_t)p;
+    }
+}
+
+// Source id of every entry: one warp per row writes its range.
+__global__ void k_expand_src(const int32_t* __restrict__ V, int32_t n, int32_t* __restrict__ src) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = warp; u < n; u += nwarps) {
+        const int32_t b = V[u], e = V[u + 1];
+        for (int32_t p = b + lane; p < e; p += 32) src[p] = (int32_t)u;
+    }
+}
+
+__global__ void k_gather_inbound(const uint32_t* __restrict__ sorted_ids, int64_t nnz,
+                                 const int32_t* __restrict__ src, const double* __restrict__ W,
+                                 int32_t* __restrict__ in_col, float* __restrict__ in_w) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = sorted_ids[i];
+        in_col[i] = src[p];
+        if (in_w) in_w[i] = (float)sanitize_w(W[p]);
+    }
+}
+
+__global__ void k_dangling(const double* __restrict__ outw, int32_t n, int32_t* __restrict__ mask,
+                           unsigned long long* __restrict__ counts) {
+    __shared__ unsigned long long c0, c1;
+    if (threadIdx.x == 0) { c0 = 0; c1 = 0; }
+    __syncthreads();
+    unsigned long long a = 0, b = 0;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const double w = outw[u];
+        const int d = w <= 0.0 ? 1 : 0;
+        mask[u] = d;
+        a += d;
+        b += (w <= 1e-15) ? 1 : 0;
+    }
+    atomicAdd(&c0, a);
+    atomicAdd(&c1, b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(&counts[0], c0);
+        atomicAdd(&counts[1], c1);
+    }
+}
+
+// Merge-path coordinate of diagonal d over (row ends = in_row[1..n], entries).
+__device__ __forceinline__ int2 merge_search(const int32_t* __restrict__ in_row, int32_t n,
+                                             int64_t nnz, int64_t d) {
+    int64_t lo = d - nnz > 0 ? d - nnz : 0;
+    int64_t hi = d < n ? d : n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)in_row[mid + 1] <= d - mid - 1) lo = mid + 1;
+        else hi = mid;
+    }
+    return make_int2((int32_t)lo, (int32_t)(d - lo));
+}
+
+__global__ void k_sub_coord(const int32_t* __restrict__ in_row, int32_t n, int64_t nnz, int32_t nsub,
+                            int2* __restrict__ coord) {
+    const int64_t total = (int64_t)n + nnz;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s <= nsub;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        int64_t d = s * (int64_t)kSubItems;
+        if (d > total) d = total;
+        coord[s] = merge_search(in_row, n, nnz, d);
+    }
+}
+
+// (row, entry, in_row[row]) at each chunk boundary, for the host-side span table.
+__global__ void k_chunk_bounds(const int2* __restrict__ coord, const int32_t* __restrict__ in_row,
+                               int32_t nsub, int32_t chunk_subs, int32_t nchunks, int32_t n,
+                               int4* __restrict__ out) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= nchunks; c += gridDim.x * blockDim.x) {
+        int s = c * chunk_subs;
+        if (s > nsub) s = nsub;
+        const int2 rc = coord[s];
+        const int32_t start = rc.x < n ? in_row[rc.x] : in_row[n];
+        out[c] = make_int4(rc.x, rc.y, start, 0);
+    }
+}
+
+inline int grid_for(int64_t work, int per_block = kThreads) {
+    int64_t g = (work + per_block - 1) / per_block;
+    if (g < 1) g = 1;
+    if (g > 148 * 32) g = 148 * 32;
+    return (int)g;
+}
+
+int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SUCC : set_cuda_error(e, what); }
+
+struct TmpAlloc {
+    cudaStream_t s;
+    std::vector<void*> ptrs;
+    explicit TmpAlloc(cudaStream_t st) : s(st) {}
+    ~TmpAlloc() {
+        for (void* p : ptrs) cudaFreeAsync(p, s);
+    }
+    template <typename T>
+    T* get(size_t count, int* rc) {
+        void* p = nullptr;
+        cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s);
+        if (e != cudaSuccess) {
+            set_cuda_error(e, "cudaMallocAsync (preparation scratch)");
+            *rc = EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM;
+            return nullptr;
+        }
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+};
+
+int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                     int64_t len, int bits, cudaStream_t s, TmpAlloc& tmp, bool* result_in_alt) {
+    *result_in_alt = false;
+    if (len <= 1 || bits <= 0) return EGPR_SUCC;
+    int rc = EGPR_SUCC;
+    const int64_t ntiles = (len + kSortTile - 1) / kSortTile;
+    uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles * kDigits, &rc);
+    if (!hist) return rc;
+    uint32_t *kin = keys, *vin = vals, *kout = keys_alt, *vout = vals_alt;
+    for (int shift = 0; shift < bits; shift += kRadixBits) {
+        k_radix_hist<<<(unsigned)ntiles, kThreads, 0, s>>>(kin, len, shift, ntiles, hist);
+        rc = exclusive_scan_u32(hist, hist, ntiles * kDigits, s);
+        if (rc) return rc;
+        k_radix_scatter<<<(unsigned)ntiles, kThreads, 0, s>>>(kin, vin, kout, vout, len, shift, ntiles, hist);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    *result_in_alt = (kin == keys_alt);
+    return cuda_ok(cudaGetLastError(), "radix sort");
+}
+
+}  // namespace
+
+int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, cudaStream_t s) {
+    if (len <= 0) return EGPR_SUCC;
+    const int64_t ntiles = (len + kScanTile - 1) / kScanTile;
+    if (ntiles == 1) {
+        k_scan_tiles<<<1, kThreads, 0, s>>>(in, out, len, nullptr);
+        return cuda_ok(cudaGetLastError(), "scan");
+    }
+    uint32_t* sums = nullptr;
+    cudaError_t e = cudaMallocAsync(&sums, (size_t)ntiles * sizeof(uint32_t), s);
+    if (e != cudaSuccess) {
+        set_cuda_error(e, "cudaMallocAsync (scan)");
+        return EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM;
+    }
+    k_scan_tiles<<<(unsigned)ntiles, kThreads, 0, s>>>(in, out, len, sums);
+    int rc = exclusive_scan_u32(sums, sums, ntiles, s);
+    if (rc == EGPR_SUCC) {
+        k_scan_add<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(out, len, sums);
+        rc = cuda_ok(cudaGetLastError(), "scan add");
+    }
+    cudaFreeAsync(sums, s);
+    return rc;
+}
+
+int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W) {
+    const int32_t n = g->n;
+    const int64_t m = g->m_input;
+    cudaStream_t s = g->own_stream;
+    int rc = EGPR_SUCC;
+    const double t0 = wall_seconds();
+    cudaEventRecord(g->ev0, s);
+    {
+        TmpAlloc tmp(s);
+        int32_t* dV = tmp.get<int32_t>((size_t)n + 1, &rc);
+        int32_t* dE = tmp.get<int32_t>((size_t)m, &rc);
+        double* dW = W ? tmp.get<double>((size_t)m, &rc) : nullptr;
+        uint32_t* indeg = tmp.get<uint32_t>((size_t)n + 1, &rc);
+        uint32_t* keys = tmp.get<uint32_t>((size_t)m, &rc);
+        uint32_t* vals = tmp.get<uint32_t>((size_t)m, &rc);
+        uint32_t* keys2 = tmp.get<uint32_t>((size_t)m, &rc);
+        uint32_t* vals2 = tmp.get<uint32_t>((size_t)m, &rc);
+        int32_t* src = tmp.get<int32_t>((size_t)m, &rc);
+        unsigned long long* counts = tmp.get<unsigned long long>(2, &rc);
+        if (rc) return rc;
+        if ((rc = g->in_row.alloc(((size_t)n + 1) * sizeof(int32_t))) ||
+            (rc = g->outw.alloc((size_t)n * sizeof(double))) ||
+            (rc = g->dangling01.alloc((size_t)n * sizeof(int32_t))))
+            return rc;
+        if ((rc = cuda_ok(cudaMemcpyAsync(dV, V, ((size_t)n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D offsets")))
+            return rc;
+        if (m > 0 && (rc = cuda_ok(cudaMemcpyAsync(dE, E, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D indices")))
+            return rc;
+        if (W && m > 0 && (rc = cuda_ok(cudaMemcpyAsync(dW, W, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s), "H2D weights")))
+            return rc;
+        cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * sizeof(uint32_t), s);
+        cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s);
+        k_out_weight<<<grid_for(n), kThreads, 0, s>>>(dV, dE, dW, n, g->outw.as<double>());
+        if (m > 0) k_in_degree_keys<<<grid_for(m), kThreads, 0, s>>>(dE, m, n, indeg, keys, vals);
+        if ((rc = exclusive_scan_u32(indeg, reinterpret_cast<uint32_t*>(g->in_row.as<int32_t>()), (int64_t)n + 1, s)))
+            return rc;
+        int32_t nnz32 = 0;
+        if ((rc = cuda_ok(cudaMemcpyAsync(&nnz32, g->in_row.as<int32_t>() + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H nnz")) ||
+            (rc = cuda_ok(cudaStreamSynchronize(s), "preparation")))
+            return rc;
+        g->nnz = nnz32;
+        const int64_t nnz = g->nnz;
+        if ((rc = g->in_col.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(int32_t) + 64)))
+            return rc;
+        if (W && (rc = g->in_w.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(float) + 64)))
+            return rc;
+        if (m > 0) {
+            int bits = 0;
+            while (bits < 32 && ((uint64_t)n >> bits) != 0) ++bits;
+            bool alt = false;
+            if ((rc = radix_sort_pairs(keys, vals, keys2, vals2, m, bits, s, tmp, &alt))) return rc;
+            const uint32_t* sorted_ids = alt ? vals2 : vals;
+            k_expand_src<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, n, src);
+            if (nnz > 0)
+                k_gather_inbound<<<grid_for(nnz), kThreads, 0, s>>>(sorted_ids, nnz, src, dW, g->in_col.as<int32_t>(),
+                                                                   W ? g->in_w.as<float>() : nullptr);
+        }
+        k_dangling<<<grid_for(n), kThreads, 0, s>>>(g->outw.as<double>(), n, g->dangling01.as<int32_t>(), counts);
+        unsigned long long hc[2] = {0, 0};
+        if ((rc = cuda_ok(cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s), "D2H counts")))
+            return rc;
+        // merge-path sub-tiles and chunks
+        const int64_t total = (int64_t)n + nnz;
+        g->nsub = (int32_t)((total + kSubItems - 1) / kSubItems);
+        if (g->nsub < 1) g->nsub = 1;
+        if ((rc = g->sub_coord.alloc(((size_t)g->nsub + 1) * sizeof(int2)))) return rc;
+        k_sub_coord<<<grid_for((int64_t)g->nsub + 1), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, nnz, g->nsub,
+                                                                       g->sub_coord.as<int2>());
+        // Chunks: about two per resident CTA so the queue can balance.
+        const int grid = sweep_occupancy_grid(0);
+        int32_t target_chunks = std::max(1, 2 * grid);
+        g->chunk_subs = std::max<int32_t>(1, (g->nsub + target_chunks - 1) / target_chunks);
+        const int32_t nch = (g->nsub + g->chunk_subs - 1) / g->chunk_subs;
+        int4* bounds = tmp.get<int4>((size_t)nch + 1, &rc);
+        if (!bounds) return rc;
+        k_chunk_bounds<<<grid_for((int64_t)nch + 1), kThreads, 0, s>>>(g->sub_coord.as<int2>(), g->in_row.as<int32_t>(),
+                                                                      g->nsub, g->chunk_subs, nch, n, bounds);
+        std::vector<int4> hb((size_t)nch + 1);
+        if ((rc = cuda_ok(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int4), cudaMemcpyDeviceToHost, s), "D2H chunk bounds")) ||
+            (rc = cuda_ok(cudaStreamSynchronize(s), "preparation")))
+            return rc;
+        g->n_dangling = (int32_t)hc[0];
+        g->n_dangling_solve = (int32_t)hc[1];
+        // Span table (chunk ids local to this graph; plans add an offset).
+        std::vector<Chunk>& ch = g->plan.h_chunks;
+        ch.assign((size_t)nch, Chunk{});
+        for (int32_t c = 0; c < nch; ++c) {
+            Chunk& k = ch[(size_t)c];
+            k.sub_begin = c * g->chunk_subs;
+            k.sub_end = std::min(g->nsub, (c + 1) * g->chunk_subs);
+            k.graph = 0;
+            const int4 a = hb[(size_t)c], b = hb[(size_t)c + 1];
+            const bool head = a.y > a.z;                 // first row began earlier
+            const bool tail = b.x < n && b.y > b.z;      // last row continues
+            int32_t f = 0;
+            if (head) f |= kHasHead;
+            if (tail) f |= kHasTail;
+            if (head && tail && a.x == b.x) f |= kInterior;
+            k.flags = f;
+            k.tail_row = tail ? b.x : -1;
+            k.head_ta = -1;
+            k.tail_tb = -1;
+        }
+        for (int32_t c = 0; c < nch; ++c) {
+            Chunk& k = ch[(size_t)c];
+            if (k.flags & kHasHead) k.head_ta = (ch[(size_t)c - 1].flags & kInterior) ? ch[(size_t)c - 1].head_ta : c - 1;
+        }
+        for (int32_t c = nch - 1; c >= 0; --c) {
+            Chunk& k = ch[(size_t)c];
+            if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
+        }
+    }
+    cudaEventRecord(g->ev1, s);
+    if ((rc = cuda_ok(cudaStreamSynchronize(s), "preparation"))) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    g->prep_seconds = ms * 1e-3;
+    (void)t0;
+    return EGPR_SUCC;
+}
+
+}  // namespace egpr

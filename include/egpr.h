@@ -1,0 +1,216 @@
+/*
+ * egpr.h — C ABI of the B200 PageRank engine (libegpr.so).
+ *
+ * This is the native boundary that replaces the reference's PageRank
+ * binding and library entry:
+ *
+ *   cpp_easygraph.cpp_gpu_pagerank_dense(G, alpha, max_iterator, threshold, weight)
+ *       cpp_easygraph/cpp_easygraph.cpp:120,
+ *       impl cpp_easygraph/functions/pagerank/pagerank.cpp:176-223
+ *   int gpu_easygraph::pagerank(V, E, W, alpha, max_iter_num, threshold, PR, kernel_seconds)
+ *       gpu_easygraph/gpu_easygraph.h:95-104,
+ *       impl gpu_easygraph/functions/centrality/centrality.cpp:150-179 and
+ *            gpu_easygraph/functions/centrality/pagerank.cu:352-713
+ *
+ * Conventions: plain pointers and sizes only; every pointer argument is a
+ * HOST pointer; no device pointer ever crosses this ABI; no exception or
+ * longjmp crosses it.  Every call returns an int status (EGPR_*), whose
+ * values 0..6 keep the numbering of the reference's EG_GPU_STATUS_CODE
+ * (gpu_easygraph/common/err.h:7-15).  A graph handle is bound to the CUDA
+ * device that was current when it was created; calling it while another
+ * device is current returns EGPR_DEVICE_ERR (the reference's fixed-device
+ * rule, pagerank.cu:369-378).  Calls on one handle are serialised by the
+ * library; distinct handles may be used from distinct host threads at once.
+ *
+ * Arithmetic: the maths of the reference's EasyGraph power iteration
+ * (easygraph/functions/centrality/pagerank.py:75-139): uniform start 1/n,
+ * out-weight normalisation, uniform redistribution of dangling mass, the
+ * (1-alpha)/n teleport term, the L1 stop rule err < tol*n checked after each
+ * sweep, at most max(1, max_iter) sweeps, one final normalisation.  Ranks and
+ * the sparse products are FP32; dangling mass, residual and sums are FP64; a
+ * final FP64 sweep recomputes the last iterate unless disabled.
+ */
+#ifndef EGPR_H
+#define EGPR_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define EGPR_API __attribute__((visibility("default")))
+#else
+#define EGPR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  0..6 = gpu_easygraph EG_GPU_STATUS_CODE (err.h:7-15). */
+#define EGPR_SUCC 0
+#define EGPR_FAILED_TO_ALLOCATE_HOST_MEM 1
+#define EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM 2
+#define EGPR_DEVICE_ERR 3
+#define EGPR_UNKNOWN_ERROR 4
+#define EGPR_UNSUPPORTED_GRAPH 5
+#define EGPR_NEGATIVE_CYCLE 6
+/* Added by this engine. */
+#define EGPR_TIMEOUT 7          /* a bounded device wait gave up */
+#define EGPR_INVALID_ARGUMENT 8 /* malformed CSR, bad sizes, NULL output ... */
+
+/* Solve flags (egpr_solve_opts.flags). */
+#define EGPR_FLAG_NO_CORRECTION 1u /* skip the final FP64 sweep */
+
+typedef struct egpr_graph egpr_graph; /* opaque prepared graph (device resident) */
+
+typedef struct egpr_stats {
+    int32_t iterations;    /* sweeps run, counted like pagerank.py's loop */
+    int32_t converged;     /* 1 when the L1 rule stopped the loop, else 0 */
+    double residual;       /* FP64 L1 difference of the last sweep */
+    double kernel_seconds; /* device time of the solve (CUDA events) */
+    double total_seconds;  /* host wall time of the call */
+    int64_t bytes_per_iter;/* algorithmic HBM bytes of one sweep */
+    int32_t launches;      /* kernels this library launched for the solve */
+    int32_t reserved;
+} egpr_stats;
+
+typedef struct egpr_graph_info {
+    int32_t n;             /* vertices */
+    int32_t device;        /* CUDA device the handle lives on */
+    int64_t m_input;       /* entries of the out-edge CSR given at create */
+    int64_t nnz;           /* inbound entries kept (valid endpoints) */
+    int32_t weighted;      /* 1 if a weight array was given */
+    int32_t n_dangling;    /* vertices with out-weight sum <= 0 */
+    int64_t device_bytes;  /* device memory held by the handle */
+    double prep_seconds;   /* device time of the preparation */
+} egpr_graph_info;
+
+typedef struct egpr_cache_stats {
+    int64_t graphs;        /* live prepared graphs (all handles) */
+    int64_t device_bytes;  /* device bytes they hold */
+    int64_t hits;          /* egpr_pagerank_csr reuses of a prepared graph */
+    int64_t misses;        /* egpr_pagerank_csr preparations */
+    int64_t evictions;     /* prepared graphs dropped by the csr cache */
+    int64_t budget_bytes;  /* byte budget of the csr cache */
+} egpr_cache_stats;
+
+/* ---- status -------------------------------------------------------- */
+
+/* Replaces gpu_easygraph::err_code_detail (gpu_easygraph/common/err.cpp:9-31). */
+EGPR_API const char* egpr_status_string(int status);
+
+/* Text of the last CUDA error seen on this host thread ("" if none). */
+EGPR_API const char* egpr_last_error(void);
+
+/* ---- prepared graphs ------------------------------------------------ */
+
+/*
+ * Uploads an out-edge CSR and prepares it on the current device: FP64
+ * out-weight sums, inbound CSR with entries in ascending source order,
+ * dangling mask, merge-path work tiles.  Replaces the host-side
+ * build_inbound_from_csr + H2D of pagerank.cu:286-347,472-518, done on the
+ * GPU.  V[n+1] must be non-decreasing with V[0]==0 and V[n]==m (the CSR the
+ * reference's gen_CSR / load_csr_files produce); destinations outside [0,n)
+ * are skipped like pagerank.cu:310; non-finite or negative weights count as
+ * 0 (pagerank.cu:311).  W may be NULL (unit weights, centrality.cpp:170).
+ */
+EGPR_API int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32_t n, int64_t m,
+                      egpr_graph** out);
+EGPR_API int egpr_graph_destroy(egpr_graph* g);
+EGPR_API int egpr_graph_info_get(const egpr_graph* g, egpr_graph_info* info);
+
+/*
+ * Copies the prepared inbound CSR back to the host, for parity checks
+ * against build_inbound_from_csr (pagerank.cu:286-347).  in_w may be NULL;
+ * every other pointer must hold the sizes given by egpr_graph_info_get.
+ */
+EGPR_API int egpr_graph_export_inbound(const egpr_graph* g, int32_t* in_row /* n+1 */,
+                              int32_t* in_col /* nnz */, float* in_w /* nnz, nullable */,
+                              int32_t* dangling01 /* n */, double* out_weight_sum /* n */);
+
+/*
+ * Runs launches on the given cudaStream_t (passed as void*) instead of the
+ * handle's own stream; NULL restores the handle's stream.
+ */
+EGPR_API int egpr_graph_set_stream(egpr_graph* g, void* stream);
+
+/* ---- solves ---------------------------------------------------------- */
+
+/*
+ * PageRank / personalised PageRank on a prepared graph.  personalization
+ * (nullable, n values >= 0, not all zero) replaces the uniform teleport
+ * vector after normalisation to sum 1; dangling mass stays uniform.
+ * out_ranks[n] receives the normalised FP64 ranks.  stats may be NULL.
+ */
+EGPR_API int egpr_pagerank(egpr_graph* g, double alpha, int32_t max_iter, double tol,
+                  const double* personalization, uint32_t flags, double* out_ranks,
+                  egpr_stats* stats);
+
+/*
+ * Asynchronous form of egpr_pagerank without personalisation: enqueues the
+ * whole solve on the handle's stream and returns; egpr_pagerank_collect
+ * waits for it and copies the ranks (out_ranks may be NULL to skip the copy).
+ * Enqueueing again before collecting is allowed: the solves run back to back
+ * in stream order on the same workspace and collect reports the last one.
+ */
+EGPR_API int egpr_pagerank_enqueue(egpr_graph* g, double alpha, int32_t max_iter, double tol,
+                          uint32_t flags);
+EGPR_API int egpr_pagerank_collect(egpr_graph* g, double* out_ranks, egpr_stats* stats);
+
+/*
+ * Batched personalised PageRank: k teleport vectors solved together as one
+ * CSR x dense SpMM per sweep (each inbound entry is loaded once per sweep
+ * for a tile of columns).  teleport is k*n row-major (vector j at j*n);
+ * every vector is normalised to sum 1.  Each column stops on its own L1
+ * rule and keeps its own iteration count.  out is k*n.  stats (nullable)
+ * holds k entries.
+ */
+EGPR_API int egpr_pagerank_batch(egpr_graph* g, double alpha, int32_t max_iter, double tol, int32_t k,
+                        const double* teleport, uint32_t flags, double* out, egpr_stats* stats);
+
+/*
+ * Batched personalised PageRank with sparse seed sets: column j teleports
+ * uniformly to seeds[seed_ptr[j] .. seed_ptr[j+1]) (vertex ids, duplicates
+ * count once).  Same maths and outputs as egpr_pagerank_batch.
+ */
+EGPR_API int egpr_pagerank_seeds(egpr_graph* g, double alpha, int32_t max_iter, double tol, int32_t k,
+                        const int32_t* seed_ptr, const int32_t* seeds, uint32_t flags, double* out,
+                        egpr_stats* stats);
+
+/*
+ * Many independent graphs in one persistent launch per sweep: the work
+ * tiles of all graphs form one queue; every graph keeps its own residual,
+ * stop rule and iteration count.  outs[i] receives graph i's n_i ranks.
+ * stats (nullable) holds count entries.
+ */
+EGPR_API int egpr_pagerank_multi(int32_t count, egpr_graph* const* graphs, double alpha, int32_t max_iter,
+                        double tol, uint32_t flags, double* const* outs, egpr_stats* stats);
+
+/* ---- drop-in for gpu_easygraph::pagerank ----------------------------- */
+
+/*
+ * Same contract as int gpu_easygraph::pagerank(V, E, W, alpha,
+ * max_iter_num, threshold, PR, kernel_seconds) (gpu_easygraph.h:95-104):
+ * len_V = n+1, W NULL when the reference passes an empty vector, PR[n]
+ * receives FP64 ranks, *kernel_seconds the device time (nullable).  n <= 0
+ * returns EGPR_SUCC with nothing written (centrality.cpp:160-165).
+ * graph_id names one immutable host CSR, as CSRGraph::cache_id does
+ * (cpp_easygraph/classes/csr_graph.h:33-47): calls with the same id and the
+ * same CSR signature reuse the prepared device graph (alpha is not part of
+ * the key: nothing prepared depends on it).
+ */
+EGPR_API int egpr_pagerank_csr(const int32_t* V, int32_t len_V, const int32_t* E, int64_t len_E,
+                      const double* W, uint64_t graph_id, double alpha, int32_t max_iter_num,
+                      double threshold, double* PR, double* kernel_seconds);
+
+/* Counters of the prepared-graph cache behind egpr_pagerank_csr. */
+EGPR_API int egpr_cache_stats_get(egpr_cache_stats* out);
+/* Drops every graph held by the egpr_pagerank_csr cache. */
+EGPR_API int egpr_cache_reset(void);
+/* Byte budget of that cache (0 = max(free/4, 256 MiB) at first use). */
+EGPR_API int egpr_cache_set_budget(int64_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EGPR_H */

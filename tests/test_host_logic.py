@@ -1,0 +1,190 @@
+"""Host-side contracts of the PageRank path that need no GPU: the dense
+read-only result mapping, the dense-shape contract, env defaults, graph ->
+CSR conversion, the prepared-graph context and its invalidation, bulk CSR
+manifests, and the easygraph install hook (exercised with a fake native
+backend, like the reference's test_eggpu_cache_contracts.py:190-221)."""
+
+import json
+import types
+
+import numpy as np
+import pytest
+
+from eggpu_b200 import backend, bulk
+from eggpu_b200 import api as prmod
+from oracle import oracle
+from tests.graphs import DiGraph, Graph, MultiDiGraph, golden_small_cases
+
+
+def test_dense_value_dict_is_a_read_only_mapping():
+    r = backend.DenseValueDict(["a", "b", "c"], np.array([0.2, 0.3, 0.5]))
+    assert dict(r) == {"a": 0.2, "b": 0.3, "c": 0.5}
+    assert r == {"a": 0.2, "b": 0.3, "c": 0.5}
+    assert list(r) == ["a", "b", "c"] and len(r) == 3 and "b" in r and "z" not in r
+    assert r.get("z", 7) == 7
+    with pytest.raises(KeyError):
+        r["z"]
+    with pytest.raises(TypeError):
+        r["a"] = 1.0
+    with pytest.raises(ValueError):
+        r.to_numpy()[0] = 1.0
+    assert json.dumps(dict(r))
+    rng = backend.DenseValueDict(range(3), np.array([1.0, 2.0, 3.0]))
+    assert rng[2] == 3.0 and 3 not in rng and True not in rng
+
+
+def test_dense_shape_contract():
+    # gpu_eggpu_backend.py:1092-1126 / test_eggpu_cache_contracts.py:199-221
+    with pytest.raises(backend.DenseResultShapeError, match=r"expected \(3,\) or \(4,\)"):
+        backend.normalize_dense_array(np.zeros(5), 3, allow_leading_sentinel=True, result_name="PageRank values_dense")
+    assert backend.normalize_dense_array(np.arange(4.0), 3, allow_leading_sentinel=True).tolist() == [1.0, 2.0, 3.0]
+
+
+def test_env_defaults_and_clamping(monkeypatch):
+    assert prmod._effective_limits(None, None) == (200, 1e-6)
+    monkeypatch.setenv("EASYGRAPH_CPU_PR_MAX_ITER", "0")
+    monkeypatch.setenv("EASYGRAPH_CPU_PR_TOL", "-1")
+    assert prmod._effective_limits(None, None) == (1, 0.0)
+    assert prmod._effective_limits(-5, -2.0) == (1, 0.0)
+
+
+def test_runtime_switches(monkeypatch):
+    # gpu_runtime.py:10-15 / test_eggpu_runtime.py:37-56
+    for val, want in (("TRUE", True), ("1", True), ("on", True), ("yes", True), ("false", False), ("", False)):
+        monkeypatch.setenv("EASYGRAPH_ENABLE_GPU", val)
+        assert prmod.gpu_runtime_enabled() is want
+
+
+def test_multigraph_and_empty_graph():
+    G = MultiDiGraph()
+    G.add_edge(0, 1)
+    with pytest.raises(prmod.EasyGraphNotImplemented):
+        prmod.pagerank(G)
+    assert prmod.pagerank(DiGraph()) == {}
+    assert prmod.pagerank(Graph()) == {}
+
+
+@pytest.mark.parametrize("case", golden_small_cases(), ids=lambda c: c[0])
+def test_graph_csr_matches_restated_gen_csr(case):
+    name, G, kw, _ = case
+    prepared = backend.prepare_graph_context(G)
+    weight = kw.get("weight")
+    V, E, W = backend.graph_csr(G, prepared, weight)
+    V2, E2, W2 = oracle.graph_to_csr(list(G.nodes), G._adj, G.is_directed(), weight)
+    assert np.array_equal(V, V2) and np.array_equal(E, E2)
+    if weight is not None:
+        assert np.array_equal(W, W2)
+
+
+def test_prepared_context_reuse_and_mutation_invalidation():
+    G = DiGraph()
+    G.add_edge(0, 1, weight=8.0)
+    G.add_edge(1, 0, weight=1.0)
+    p1 = backend.prepare_graph_context(G)
+    assert backend.prepare_graph_context(G) is p1
+    G[0][1]["weight"] = 0.25  # graph.py:17-40: attribute mutation bumps the generation
+    p2 = backend.prepare_graph_context(G)
+    assert p2 is not p1 and p2["ctx_id"] != p1["ctx_id"]
+    V, E, W = backend.graph_csr(G, p2, "weight")
+    assert W.tolist() == [0.25, 1.0]
+
+
+def test_prepared_context_full_stamp_check(monkeypatch):
+    G = DiGraph()
+    G.add_edges_from([(0, 1), (1, 2)])
+    p = backend.prepare_graph_context(G)
+    monkeypatch.setattr(backend, "_GRAPH_CTX_VALIDATE_EVERY", 1)
+    # change the adjacency behind the generation counter: the stamp catches it
+    dict.__setitem__(G._adj[2], 0, {})
+    assert backend.prepare_graph_context(G) is not p
+
+
+def test_fake_native_backend_wrong_length_raises(monkeypatch):
+    G = DiGraph()
+    G.add_edges_from([(0, 1), (1, 2), (2, 0)])
+    monkeypatch.setattr(backend, "prepared_native", lambda G, p, w=None: object())
+    monkeypatch.setattr(backend, "cpp_gpu_pagerank_dense",
+                        lambda *a, **k: {"values_dense": np.zeros(5), "kernel_seconds": 0.0})
+    with pytest.raises(backend.DenseResultShapeError, match=r"expected \(3,\) or \(4,\)"):
+        backend.pagerank(G)
+    monkeypatch.setattr(backend, "cpp_gpu_pagerank_dense",
+                        lambda *a, **k: {"values_dense": np.array([9.0, 0.2, 0.3, 0.5]), "kernel_seconds": 0.5})
+    res = backend.pagerank(G)
+    assert dict(res) == {0: 0.2, 1: 0.3, 2: 0.5}
+    assert backend.get_last_kernel_time("pagerank") == 0.5
+
+
+def test_personalization_vector_validation():
+    G = DiGraph()
+    G.add_edges_from([("a", "b"), ("b", "c")])
+    p = backend.prepare_graph_context(G)
+    assert backend._personalization_vector({"b": 2.0}, p).tolist() == [0.0, 2.0, 0.0]
+    with pytest.raises(KeyError):
+        backend._personalization_vector({"zz": 1.0}, p)
+    with pytest.raises(ValueError):
+        backend._personalization_vector({"a": 0.0}, p)
+    with pytest.raises(ValueError):
+        backend._personalization_vector({"a": -1.0, "b": 2.0}, p)
+
+
+def test_bulk_manifest_roundtrip_and_validation(tmp_path):
+    V = np.array([0, 2, 3, 3], np.int32)
+    E = np.array([1, 2, 0], np.int32)
+    W = np.array([1.0, 2.0, 3.0])
+    path = bulk.write_eggpu_csr(tmp_path, "tiny", V, E, W, directed=True)
+    G = bulk.read_eggpu_csr(path)
+    assert len(G) == 3 and list(G.nodes) == [0, 1, 2] and G.has_weight("weight")
+    assert np.array_equal(G.csr_arrays("weight")[2], W)
+    with pytest.raises(NotImplementedError, match="weighted PageRank requires an EGGPU CSR artifact"):
+        G.csr_arrays("other")
+    meta = json.loads(path.read_text())
+    meta["format"] = "bogus"
+    bad = tmp_path / "bad.json"
+    bad.write_text(json.dumps(meta))
+    with pytest.raises(ValueError, match="unsupported CSR artifact format"):
+        bulk.read_eggpu_csr(bad)
+    with pytest.raises(ValueError, match="endpoint is outside"):
+        bulk.BulkCSRGraph(V, np.array([1, 5, 0], np.int32))
+    with pytest.raises(ValueError, match="final offset"):
+        bulk.BulkCSRGraph(np.array([0, 1], np.int32), np.array([0, 0], np.int32))
+    with pytest.raises(ValueError, match="finite"):
+        bulk.BulkCSRGraph(V, E, np.array([1.0, np.nan, 1.0]), weight_key="weight")
+    p = backend.prepare_graph_context(G)
+    assert p["bulk_csr"] and p["nodes"] == range(3)
+    assert backend.prepare_graph_context(G) is p
+
+
+def test_install_hook_with_fake_easygraph(monkeypatch):
+    import sys
+
+    calls = {}
+    fake_backend = types.SimpleNamespace(pagerank=lambda *a, **k: "orig-backend")
+    fake_pr = types.SimpleNamespace(pagerank=lambda G, **k: calls.setdefault("cpu", k) or "cpu")
+    fake_eg = types.ModuleType("easygraph")
+    fake_eg.pagerank = fake_pr.pagerank
+    fake_utils = types.ModuleType("easygraph.utils")
+    fake_utils.gpu_eggpu_backend = fake_backend
+    fake_funcs = types.ModuleType("easygraph.functions")
+    fake_cent = types.ModuleType("easygraph.functions.centrality")
+    fake_cent.pagerank = fake_pr
+    for name, mod in (("easygraph", fake_eg), ("easygraph.utils", fake_utils),
+                      ("easygraph.utils.gpu_eggpu_backend", fake_backend), ("easygraph.functions", fake_funcs),
+                      ("easygraph.functions.centrality", fake_cent),
+                      ("easygraph.functions.centrality.pagerank", fake_pr)):
+        monkeypatch.setitem(sys.modules, name, mod)
+    monkeypatch.setattr(prmod, "_INSTALLED", {})
+    assert prmod.install() is True
+    assert fake_eg.pagerank is fake_pr.pagerank
+    G = DiGraph()
+    G.add_edge(0, 1)
+    fake_eg.pagerank(G, alpha=0.5)  # GPU switch off -> easygraph's own CPU code
+    assert calls["cpu"]["alpha"] == 0.5
+    with pytest.raises(ValueError, match="personalization needs the GPU"):
+        fake_eg.pagerank(G, personalization={0: 1.0})
+    seen = {}
+    monkeypatch.setattr(backend, "pagerank", lambda G, **k: seen.update(k) or {"ok": 1})
+    monkeypatch.setenv("EASYGRAPH_ENABLE_GPU", "TRUE")
+    assert fake_eg.pagerank(G, alpha=0.6, personalization={0: 1.0}) == {"ok": 1}
+    assert seen["alpha"] == 0.6 and seen["personalization"] == {0: 1.0}
+    assert fake_backend.pagerank(G, alpha=0.7, max_iter=3, eps=1e-3) == {"ok": 1}
+    assert seen["max_iter"] == 3 and seen["eps"] == 1e-3
