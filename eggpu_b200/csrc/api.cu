@@ -316,6 +316,7 @@ static void destroy_graph_object(egpr_graph* g) {
     cudaGetDevice(&cur);
     if (g->device >= 0 && cur != g->device) cudaSetDevice(g->device);
     if (g->own_stream) cudaStreamSynchronize(g->own_stream);
+    spmm_work_release(g);
     g->plan.release();
     for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord, &g->scale, &g->tele,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})

@@ -132,6 +132,8 @@ struct Plan {
     void release();
 };
 
+struct SpmmWork;  // batched personalised PageRank workspace (spmm.cu)
+
 // ---- prepared graph handle ---------------------------------------------------
 }  // namespace egpr
 
@@ -152,6 +154,7 @@ struct egpr_graph {
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
     egpr::Plan plan;               // single-graph plan
+    egpr::SpmmWork* spmm = nullptr; // batched personalised PageRank workspace
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr; // active stream (own or user-given)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -171,6 +174,7 @@ double wall_seconds();
 
 // Preparation (prep.cu).
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
+int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
 
 // Plans and sweeps (sweep.cu).
 int sweep_occupancy_grid(int mode);
@@ -183,6 +187,7 @@ int launch_loop(Plan& plan, int32_t max_iter, cudaStream_t stream, int32_t* laun
 int launch_finish(Plan& plan, bool correction, cudaStream_t stream, int32_t* launches);
 
 // SpMM personalised PageRank (spmm.cu).
+void spmm_work_release(egpr_graph* g);
 int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, int32_t k,
                     const double* teleport_dense, const int32_t* seed_ptr, const int32_t* seeds,
                     uint32_t flags, double* out, egpr_stats* stats);

@@ -371,6 +371,50 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, cudaStrea
     return rc;
 }
 
+// Chunk table over a graph's sub-tiles: runs of chunk_subs sub-tiles, with the
+// span links of rows cut by chunk boundaries (chunk ids local to the graph).
+int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& ch, cudaStream_t s) {
+    const int32_t n = g->n;
+    const int32_t nch = (g->nsub + chunk_subs - 1) / chunk_subs;
+    int4* bounds = nullptr;
+    int rc = cuda_ok(cudaMallocAsync(&bounds, ((size_t)nch + 1) * sizeof(int4), s), "cudaMallocAsync (chunks)");
+    if (rc) return rc;
+    k_chunk_bounds<<<grid_for((int64_t)nch + 1), kThreads, 0, s>>>(g->sub_coord.as<int2>(), g->in_row.as<int32_t>(),
+                                                                  g->nsub, chunk_subs, nch, n, bounds);
+    std::vector<int4> hb((size_t)nch + 1);
+    rc = cuda_ok(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int4), cudaMemcpyDeviceToHost, s), "D2H chunk bounds");
+    cudaFreeAsync(bounds, s);
+    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "chunk table"))) return rc;
+    ch.assign((size_t)nch, Chunk{});
+    for (int32_t c = 0; c < nch; ++c) {
+        Chunk& k = ch[(size_t)c];
+        k.sub_begin = c * chunk_subs;
+        k.sub_end = std::min(g->nsub, (c + 1) * chunk_subs);
+        k.graph = 0;
+        const int4 a = hb[(size_t)c], b = hb[(size_t)c + 1];
+        const bool head = a.y > a.z;             // first row began earlier
+        const bool tail = b.x < n && b.y > b.z;  // last row continues
+        int32_t f = 0;
+        if (head) f |= kHasHead;
+        if (tail) f |= kHasTail;
+        if (head && tail && a.x == b.x) f |= kInterior;
+        k.flags = f;
+        k.tail_row = tail ? b.x : -1;
+        k.head_ta = -1;
+        k.tail_tb = -1;
+        k.pad = 0;
+    }
+    for (int32_t c = 0; c < nch; ++c) {
+        Chunk& k = ch[(size_t)c];
+        if (k.flags & kHasHead) k.head_ta = (ch[(size_t)c - 1].flags & kInterior) ? ch[(size_t)c - 1].head_ta : c - 1;
+    }
+    for (int32_t c = nch - 1; c >= 0; --c) {
+        Chunk& k = ch[(size_t)c];
+        if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
+    }
+    return EGPR_SUCC;
+}
+
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W) {
     const int32_t n = g->n;
     const int64_t m = g->m_input;
@@ -439,49 +483,13 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         if ((rc = g->sub_coord.alloc(((size_t)g->nsub + 1) * sizeof(int2)))) return rc;
         k_sub_coord<<<grid_for((int64_t)g->nsub + 1), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, nnz, g->nsub,
                                                                        g->sub_coord.as<int2>());
-        // Chunks: about two per resident CTA so the queue can balance.
-        const int grid = sweep_occupancy_grid(0);
-        int32_t target_chunks = std::max(1, 2 * grid);
-        g->chunk_subs = std::max<int32_t>(1, (g->nsub + target_chunks - 1) / target_chunks);
-        const int32_t nch = (g->nsub + g->chunk_subs - 1) / g->chunk_subs;
-        int4* bounds = tmp.get<int4>((size_t)nch + 1, &rc);
-        if (!bounds) return rc;
-        k_chunk_bounds<<<grid_for((int64_t)nch + 1), kThreads, 0, s>>>(g->sub_coord.as<int2>(), g->in_row.as<int32_t>(),
-                                                                      g->nsub, g->chunk_subs, nch, n, bounds);
-        std::vector<int4> hb((size_t)nch + 1);
-        if ((rc = cuda_ok(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int4), cudaMemcpyDeviceToHost, s), "D2H chunk bounds")) ||
-            (rc = cuda_ok(cudaStreamSynchronize(s), "preparation")))
-            return rc;
         g->n_dangling = (int32_t)hc[0];
         g->n_dangling_solve = (int32_t)hc[1];
-        // Span table (chunk ids local to this graph; plans add an offset).
-        std::vector<Chunk>& ch = g->plan.h_chunks;
-        ch.assign((size_t)nch, Chunk{});
-        for (int32_t c = 0; c < nch; ++c) {
-            Chunk& k = ch[(size_t)c];
-            k.sub_begin = c * g->chunk_subs;
-            k.sub_end = std::min(g->nsub, (c + 1) * g->chunk_subs);
-            k.graph = 0;
-            const int4 a = hb[(size_t)c], b = hb[(size_t)c + 1];
-            const bool head = a.y > a.z;                 // first row began earlier
-            const bool tail = b.x < n && b.y > b.z;      // last row continues
-            int32_t f = 0;
-            if (head) f |= kHasHead;
-            if (tail) f |= kHasTail;
-            if (head && tail && a.x == b.x) f |= kInterior;
-            k.flags = f;
-            k.tail_row = tail ? b.x : -1;
-            k.head_ta = -1;
-            k.tail_tb = -1;
-        }
-        for (int32_t c = 0; c < nch; ++c) {
-            Chunk& k = ch[(size_t)c];
-            if (k.flags & kHasHead) k.head_ta = (ch[(size_t)c - 1].flags & kInterior) ? ch[(size_t)c - 1].head_ta : c - 1;
-        }
-        for (int32_t c = nch - 1; c >= 0; --c) {
-            Chunk& k = ch[(size_t)c];
-            if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
-        }
+        // Chunks: about two per resident CTA so the queue can balance.
+        const int grid = sweep_occupancy_grid(0);
+        const int32_t target_chunks = std::max(1, 2 * grid);
+        g->chunk_subs = std::max<int32_t>(1, (g->nsub + target_chunks - 1) / target_chunks);
+        if ((rc = build_chunk_table(g, g->chunk_subs, g->plan.h_chunks, s))) return rc;
     }
     cudaEventRecord(g->ev1, s);
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "preparation"))) return rc;

@@ -44,6 +44,10 @@ struct SweepSmem {
     Real rowval[kSubItems];
     Real carry_val[kThreads];
     int32_t carry_row[kThreads];
+    Real wlast_val[kWarps];
+    Real wcarry[kWarps];
+    int32_t wlast_row[kWarps];
+    int32_t wfirst_row[kWarps];
     double red[3][kWarps];
     Real sub_carry;
     Real head_val;
@@ -51,6 +55,43 @@ struct SweepSmem {
     int32_t tile;
     int32_t is_last;
 };
+
+// Block-wide inclusive segmented scan of (row, value) pairs in thread order,
+// rows non-decreasing: returns, for this thread, the sum of the values of the
+// threads from the start of its row's run up to itself.  Leaves every
+// thread's row and scanned value in S.carry_row / S.carry_val.  Fixed
+// combination order, so the result is deterministic.
+template <typename Real>
+__device__ __forceinline__ Real segmented_scan(SweepSmem<Real>& S, int32_t row, Real v) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Real up = __shfl_up_sync(0xffffffffu, v, o);
+        const int32_t rup = __shfl_up_sync(0xffffffffu, row, o);
+        if (lane >= o && rup == row) v += up;
+    }
+    const int32_t wfirst = __shfl_sync(0xffffffffu, row, 0);
+    if (lane == 31) {
+        S.wlast_row[warp] = row;
+        S.wlast_val[warp] = v;
+        S.wfirst_row[warp] = wfirst;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Real prefix = Real(0);
+        for (int w = 0; w < kWarps; ++w) {
+            const Real cin = (w > 0 && S.wfirst_row[w] == S.wlast_row[w - 1]) ? prefix : Real(0);
+            S.wcarry[w] = cin;
+            prefix = S.wlast_val[w] + (S.wlast_row[w] == S.wfirst_row[w] ? cin : Real(0));
+        }
+    }
+    __syncthreads();
+    if (row == wfirst) v += S.wcarry[warp];
+    S.carry_row[threadIdx.x] = row;
+    S.carry_val[threadIdx.x] = v;
+    __syncthreads();
+    return v;
+}
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
@@ -95,6 +136,41 @@ struct SweepView {
     int32_t personalised;
 };
 
+// Row data the epilogue needs, loaded ahead of time.
+constexpr int kRowPre = 2;
+struct RowPre {
+    float xin;
+    float scale;
+    float tele;
+};
+
+__device__ __forceinline__ void load_row(const GraphDev& G, const SweepView& W, int32_t v, RowPre& p) {
+    p.xin = W.xin[v];
+    p.scale = G.scale[v];
+    p.tele = W.personalised ? G.tele[v] : 0.f;
+}
+
+template <typename Real>
+__device__ __forceinline__ void finish_row_pre(const GraphDev& G, const SweepView& W, int32_t v, double acc,
+                                               const RowPre& p, double& err, double& dsum, double& xsum) {
+    double val;
+    if (W.personalised) val = (acc + W.one_minus_alpha * (double)p.tele) + W.dmass;
+    else val = acc + W.jump;
+    const double prev = (double)p.xin;
+    if constexpr (std::is_same<Real, float>::value) {
+        const float xo = (float)val;
+        err += fabs((double)xo - prev);
+        W.xout[v] = xo;
+        W.zout[v] = p.scale >= 0.f ? xo * p.scale : 0.f;
+        if (p.scale < 0.f) dsum += (double)xo;
+        xsum += (double)xo;
+    } else {
+        err += fabs(val - prev);
+        G.out[v] = val;
+        xsum += val;
+    }
+}
+
 // Finishes row v given its gathered sum; accumulates residual / dangling /
 // rank sums.  FP32 sweep: writes x_new and z_new.  FP64 correction sweep:
 // writes the FP64 result.
@@ -105,15 +181,18 @@ __device__ __forceinline__ void finish_row(const GraphDev& G, const SweepView& W
     if (W.personalised) val = (acc + W.one_minus_alpha * (double)G.tele[v]) + W.dmass;
     else val = acc + W.jump;
     const double prev = (double)W.xin[v];
-    err += fabs(val - prev);
     if constexpr (std::is_same<Real, float>::value) {
+        // The residual compares the stored FP32 iterates, so the loop can stop
+        // once they no longer change even when tol*n is below FP32 resolution.
         const float xo = (float)val;
+        err += fabs((double)xo - prev);
         W.xout[v] = xo;
         const float sc = G.scale[v];
         W.zout[v] = sc >= 0.f ? xo * sc : 0.f;
         if (sc < 0.f) dsum += (double)xo;
         xsum += (double)xo;
     } else {
+        err += fabs(val - prev);
         G.out[v] = val;
         xsum += val;
     }
@@ -220,35 +299,54 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, SweepSmem<Real>& 
         S.head_val = Real(0);
         S.head_pending = (ck.flags & kHasHead) ? 1 : 0;
     }
+    // Software pipeline: the column indices of sub-tile s+1 are loaded while
+    // sub-tile s is gathered and reduced, and each sub-tile's row data (x, scale)
+    // is loaded together with its gathers, so a sub-tile waits on about one
+    // memory round trip.
+    int2 a = G.sub_coord[ck.sub_begin];
+    int2 b = G.sub_coord[ck.sub_begin + 1];
+    int32_t col[kItemsPerThread];
+#pragma unroll
+    for (int u = 0; u < kItemsPerThread; ++u) {
+        const int32_t i = tid + u * kThreads;
+        col[u] = i < b.y - a.y ? __ldcs(in_col + a.y + i) : -1;
+    }
     for (int32_t sidx = ck.sub_begin; sidx < ck.sub_end; ++sidx) {
-        const int2 a = G.sub_coord[sidx];
-        const int2 b = G.sub_coord[sidx + 1];
         const int32_t ra = a.x, ka = a.y;
         const int32_t nnz_sub = b.y - a.y;
         const int32_t nrows = b.x - a.x;
-        // Phase 1: stage the products of this sub-tile's entries.
-        int32_t col[kItemsPerThread];
-#pragma unroll
-        for (int u = 0; u < kItemsPerThread; ++u) {
-            const int32_t i = tid + u * kThreads;
-            col[u] = i < nnz_sub ? __ldcs(in_col + ka + i) : -1;
-        }
+        const bool has_next = sidx + 1 < ck.sub_end;
+        const int2 bn = has_next ? G.sub_coord[sidx + 2] : b;
+        // Phase 1: gathers of this sub-tile, next sub-tile's indices, row data.
         Real val[kItemsPerThread];
 #pragma unroll
         for (int u = 0; u < kItemsPerThread; ++u) val[u] = col[u] >= 0 ? gsrc[col[u]] : Real(0);
+        float wv[kItemsPerThread];
         if (in_w) {
 #pragma unroll
             for (int u = 0; u < kItemsPerThread; ++u) {
                 const int32_t i = tid + u * kThreads;
-                if (i < nnz_sub) val[u] *= (Real)__ldcs(in_w + ka + i);
+                wv[u] = i < nnz_sub ? __ldcs(in_w + ka + i) : 0.f;
             }
         }
+        const int32_t nnz_next = bn.y - b.y;
 #pragma unroll
         for (int u = 0; u < kItemsPerThread; ++u) {
             const int32_t i = tid + u * kThreads;
-            if (i < nnz_sub) S.prod[i] = val[u];
+            col[u] = (has_next && i < nnz_next) ? __ldcs(in_col + b.y + i) : -1;
+        }
+        RowPre pre[kRowPre];
+#pragma unroll
+        for (int q = 0; q < kRowPre; ++q) {
+            const int32_t r = tid + q * kThreads;
+            if (r < nrows) load_row(G, W, ra + r, pre[q]);
         }
         for (int32_t i = tid; i < nrows; i += kThreads) S.rowend[i] = in_row[ra + i + 1] - ka;
+#pragma unroll
+        for (int u = 0; u < kItemsPerThread; ++u) {
+            const int32_t i = tid + u * kThreads;
+            if (i < nnz_sub) S.prod[i] = in_w ? val[u] * (Real)wv[u] : val[u];
+        }
         __syncthreads();
         // Phase 2: each thread walks its items of the merge path.
         const int32_t total = nrows + nnz_sub;
@@ -274,42 +372,41 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, SweepSmem<Real>& 
                 ++j;
             }
         }
-        S.carry_row[tid] = i;
-        S.carry_val[tid] = acc;
-        __syncthreads();
-        // Phase 2b: add the carries of earlier threads to each thread's first row.
+        // Phase 2b: each thread's carry (the partial sum of the row it stopped
+        // in) is added to the row's completion by a segmented inclusive scan
+        // over threads keyed by row (rows never decrease along the path).  The
+        // carry from the previous sub-tile belongs to local row 0: it joins
+        // thread 0's carry, or thread 0's first row if thread 0 completed it.
         const Real cin = S.sub_carry;
+        Real seg = acc;
+        if (tid == 0 && first != 0) seg += cin;
+        seg = segmented_scan(S, i, seg);
         if (first >= 0) {
             Real v = S.rowval[first];
-            int32_t t = tid - 1;
-            while (t >= 0 && S.carry_row[t] == first) {
-                v += S.carry_val[t];
-                --t;
-            }
-            if (t < 0 && first == 0) v += cin;
+            if (tid == 0) v += cin;  // first == 0 here: thread 0 starts in row 0
+            else if (S.carry_row[tid - 1] == first) v += S.carry_val[tid - 1];
             S.rowval[first] = v;
         }
-        Real out_carry = Real(0);
-        if (tid == kThreads - 1) {
-            int32_t t = kThreads - 1;
-            while (t >= 0 && S.carry_row[t] == nrows) {
-                out_carry += S.carry_val[t];
-                --t;
-            }
-            if (t < 0 && nrows == 0) out_carry += cin;
-        }
         __syncthreads();
-        if (tid == kThreads - 1) S.sub_carry = out_carry;
+        if (tid == kThreads - 1) S.sub_carry = seg;  // the last thread always stops in row nrows
         // Phase 3: finish the rows that ended in this sub-tile (coalesced).
-        for (int32_t r = tid; r < nrows; r += kThreads) {
-            const Real racc = S.rowval[r];
-            if (r == 0 && S.head_pending) {
-                S.head_val = racc;  // the chunk's head row: completed through its span
-                continue;
+#pragma unroll
+        for (int q = 0; q < kRowPre; ++q) {
+            const int32_t r = tid + q * kThreads;
+            if (r < nrows) {
+                const Real racc = S.rowval[r];
+                if (r == 0 && S.head_pending) S.head_val = racc;  // the chunk's head row: finished through its span
+                else finish_row_pre<Real>(G, W, ra + r, (double)racc, pre[q], err, dsum, xsum);
             }
-            finish_row<Real>(G, W, ra + r, (double)racc, err, dsum, xsum);
+        }
+        for (int32_t r = tid + kRowPre * kThreads; r < nrows; r += kThreads) {
+            RowPre rp;
+            load_row(G, W, ra + r, rp);
+            finish_row_pre<Real>(G, W, ra + r, (double)S.rowval[r], rp, err, dsum, xsum);
         }
         if (tid == 0 && nrows > 0) S.head_pending = 0;
+        a = b;
+        b = bn;
     }
     __syncthreads();
     block_sum3(S, err, dsum, xsum);
@@ -337,7 +434,7 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, SweepSmem<Real>& 
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(kThreads) k_sweep(SweepParams P) {
+__global__ void __launch_bounds__(kThreads, 3) k_sweep(SweepParams P) {
     __shared__ SweepSmem<Real> S;
     constexpr bool kFinal = std::is_same<Real, double>::value;
     const bool idle = !kFinal && ldcg(&P.ctl->active) <= 0;

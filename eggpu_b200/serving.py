@@ -1,0 +1,275 @@
+"""Continuous-batching request loop for PageRank and personalised PageRank.
+
+Requests (plain PageRank or PPR over a seed set) arrive for graphs held in a
+registry.  The server keeps prepared graphs (inbound CSR and rank state) on
+the device, admits graphs by HBM bytes with least-recently-used eviction of
+idle graphs, and serves requests as they arrive:
+
+* every graph has at most one solve in flight; requests that arrive while it
+  runs queue up and are folded into that graph's next solve: all queued PPR
+  requests become the columns of one batched SpMM solve
+  (``egpr_pagerank_seeds``), all queued plain requests share one solve (their
+  answer is identical);
+* solves on different graphs run concurrently from a pool of worker threads,
+  each prepared graph on its own CUDA stream, so their kernels overlap on the
+  device;
+* plain requests for several small graphs that are all waiting are folded into
+  one persistent multi-graph launch (``egpr_pagerank_multi``).
+
+Every result is the answer the same request gets alone (the batched solve
+keeps per-column stop rules and iteration counts); tests/test_serving.py
+checks that within the engine's stated tolerance.  Latency is measured from a
+request's arrival to the moment its result is on the host.
+"""
+
+from __future__ import annotations
+
+import collections
+import heapq
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native
+
+
+@dataclass
+class Request:
+    graph: object
+    kind: str  # "pr" or "ppr"
+    seeds: np.ndarray | None = None
+    alpha: float = 0.85
+    max_iter: int = 100
+    tol: float = 1e-6
+    arrival: float = 0.0
+    future: Future = field(default_factory=Future)
+    done_at: float = 0.0
+    iterations: int = 0
+
+
+class GraphRegistry:
+    """Device-resident prepared graphs, admitted by HBM bytes (LRU eviction of idle graphs)."""
+
+    def __init__(self, sources, budget_bytes):
+        self.sources = dict(sources)  # graph id -> (V, E, W)
+        self.budget = int(budget_bytes)
+        self.resident = collections.OrderedDict()  # id -> PreparedGraph
+        self.busy = collections.Counter()
+        self.lock = threading.Condition()
+        self.evictions = 0
+        self.admissions = 0
+
+    def _bytes(self):
+        return sum(pg.info()["device_bytes"] for pg in self.resident.values())
+
+    @staticmethod
+    def estimate_bytes(V, E, W):
+        n = len(V) - 1
+        m = len(E)
+        return 4 * (n + 1) + 4 * m * (2 if W is not None else 1) + 8 * n + 4 * n + 24 * n + 16 * n + 64 * 1024
+
+    def acquire(self, gid):
+        """The prepared graph for gid, marked busy; waits for HBM room if needed."""
+        with self.lock:
+            while True:
+                pg = self.resident.get(gid)
+                if pg is not None:
+                    self.resident.move_to_end(gid)
+                    self.busy[gid] += 1
+                    return pg
+                V, E, W = self.sources[gid]
+                need = self.estimate_bytes(V, E, W)
+                used = self._bytes()
+                for victim in list(self.resident):
+                    if used + need <= self.budget:
+                        break
+                    if self.busy[victim] == 0:
+                        used -= self.resident[victim].info()["device_bytes"]
+                        self.resident.pop(victim).close()
+                        self.evictions += 1
+                if used + need <= self.budget or not any(self.busy.values()):
+                    pg = _native.PreparedGraph(V, E, W)
+                    self.resident[gid] = pg
+                    self.admissions += 1
+                    self.busy[gid] += 1
+                    return pg
+                self.lock.wait(0.01)
+
+    def release(self, gid):
+        with self.lock:
+            self.busy[gid] -= 1
+            self.lock.notify_all()
+
+    def close(self):
+        with self.lock:
+            for pg in self.resident.values():
+                pg.close()
+            self.resident.clear()
+
+
+class Server:
+    """Serves Request objects; submit() returns a Future resolving to (ranks, stats)."""
+
+    def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True):
+        self.registry = registry
+        self.max_columns = int(max_columns)
+        self.multi_max_n = int(multi_max_n)
+        self.fold_multi = fold_multi
+        self.queues = collections.defaultdict(collections.deque)  # graph id -> pending requests
+        self.running = set()  # graph ids with a solve in flight
+        self.cv = threading.Condition()
+        self.stop = False
+        self.stats = collections.Counter()
+        self.threads = [threading.Thread(target=self._worker, daemon=True) for _ in range(int(workers))]
+        for t in self.threads:
+            t.start()
+
+    def submit(self, req: Request) -> Future:
+        if not req.arrival:
+            req.arrival = time.perf_counter()
+        with self.cv:
+            self.queues[req.graph].append(req)
+            self.cv.notify()
+        return req.future
+
+    def close(self):
+        with self.cv:
+            self.stop = True
+            self.cv.notify_all()
+        for t in self.threads:
+            t.join()
+
+    # -- scheduling ------------------------------------------------------
+    def _take_work(self):
+        """Picks the graph whose oldest waiting request arrived first; may add small PR-only graphs."""
+        best, best_t = None, None
+        for gid, q in self.queues.items():
+            if q and gid not in self.running:
+                t = q[0].arrival
+                if best_t is None or t < best_t:
+                    best, best_t = gid, t
+        if best is None:
+            return None
+        self.running.add(best)
+        reqs = list(self.queues.pop(best))
+        work = [(best, reqs)]
+        if self.fold_multi and all(r.kind == "pr" for r in reqs) and self._small(best):
+            for gid, q in list(self.queues.items()):
+                if len(work) >= 64:
+                    break
+                if q and gid not in self.running and all(r.kind == "pr" for r in q) and self._small(gid):
+                    self.running.add(gid)
+                    work.append((gid, list(self.queues.pop(gid))))
+        return work
+
+    def _small(self, gid):
+        V = self.registry.sources[gid][0]
+        return len(V) - 1 <= self.multi_max_n
+
+    def _worker(self):
+        while True:
+            with self.cv:
+                work = None
+                while not self.stop:
+                    work = self._take_work()
+                    if work is not None:
+                        break
+                    self.cv.wait(0.005)
+                if work is None:
+                    return
+            try:
+                self._run(work)
+            except BaseException as exc:  # noqa: BLE001 - delivered to every waiting request
+                for _, reqs in work:
+                    for r in reqs:
+                        if not r.future.done():
+                            r.future.set_exception(exc)
+            finally:
+                with self.cv:
+                    for gid, _ in work:
+                        self.running.discard(gid)
+                    self.cv.notify_all()
+
+    def _finish(self, req, ranks, stats):
+        req.done_at = time.perf_counter()
+        req.iterations = int(stats["iterations"])
+        req.future.set_result((ranks, stats))
+
+    def _run(self, work):
+        if len(work) > 1:
+            self._run_multi(work)
+            return
+        gid, reqs = work[0]
+        pg = self.registry.acquire(gid)
+        try:
+            by_params = collections.defaultdict(list)
+            for r in reqs:
+                by_params[(r.kind, r.alpha, r.max_iter, r.tol)].append(r)
+            for (kind, alpha, max_iter, tol), group in by_params.items():
+                if kind == "pr":
+                    ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol)
+                    self.stats["pr_solves"] += 1
+                    for r in group:
+                        self._finish(r, ranks, st)
+                else:
+                    for s in range(0, len(group), self.max_columns):
+                        part = group[s:s + self.max_columns]
+                        ranks, sts = pg.pagerank_seeds([r.seeds for r in part], alpha=alpha, max_iter=max_iter,
+                                                       tol=tol)
+                        self.stats["ppr_batches"] += 1
+                        self.stats["ppr_columns"] += len(part)
+                        for j, r in enumerate(part):
+                            self._finish(r, ranks[j], sts[j])
+        finally:
+            self.registry.release(gid)
+
+    def _run_multi(self, work):
+        gids = [gid for gid, _ in work]
+        pgs = []
+        try:
+            for gid in gids:
+                pgs.append(self.registry.acquire(gid))
+            by_params = collections.defaultdict(list)
+            for (gid, reqs), pg in zip(work, pgs):
+                for r in reqs:
+                    by_params[(r.alpha, r.max_iter, r.tol)].append((pg, r))
+            for (alpha, max_iter, tol), items in by_params.items():
+                uniq = list(dict.fromkeys(pg for pg, _ in items))
+                outs, sts = _native.pagerank_multi(uniq, alpha=alpha, max_iter=max_iter, tol=tol)
+                self.stats["multi_launches"] += 1
+                self.stats["multi_graphs"] += len(uniq)
+                res = {id(pg): (o, s) for pg, o, s in zip(uniq, outs, sts)}
+                for pg, r in items:
+                    o, s = res[id(pg)]
+                    self._finish(r, o, s)
+        finally:
+            for gid in gids[:len(pgs)]:
+                self.registry.release(gid)
+
+
+def poisson_arrivals(rate, count, seed):
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=count))
+
+
+def replay(server, requests, times):
+    """Submits requests at the given offsets (seconds from now); returns when all are done."""
+    t0 = time.perf_counter()
+    for req, t in zip(requests, times):
+        delay = t0 + t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        req.arrival = time.perf_counter()
+        server.submit(req)
+    for req in requests:
+        req.future.result()
+    return time.perf_counter() - t0
+
+
+def latency_summary(requests):
+    lat = np.array([r.done_at - r.arrival for r in requests])
+    return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3), "max_ms": float(lat.max() * 1e3), "count": int(lat.size)}

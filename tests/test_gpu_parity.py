@@ -234,13 +234,13 @@ def test_edge_cases(name, V, E, W):
     E = np.array(E, np.int32)
     W = None if W is None else np.array(W, np.float64)
     pg = _native.PreparedGraph(V, E, W)
-    ranks, stats = pg.pagerank(alpha=0.85, max_iter=50, tol=1e-9)
+    ranks, stats = pg.pagerank(alpha=0.85, max_iter=50, tol=1e-6)
     n = V.shape[0] - 1
     inb = oracle.build_inbound(V, E, W)
     if inb[0][-1] == 0:
         assert np.allclose(ranks, 1.0 / n) and stats["iterations"] == 0
         return
-    ref, it, _ = oracle.pagerank_pull(V, E, W, alpha=0.85, max_iter=50, tol=1e-9, inbound=inb)
+    ref, it, _ = oracle.pagerank_pull(V, E, W, alpha=0.85, max_iter=50, tol=1e-6, inbound=inb)
     assert abs(stats["iterations"] - it) <= 1
     assert np.abs(ranks - ref).sum() <= L1_TOL
     assert ranks.sum() == pytest.approx(1.0, abs=1e-12)
@@ -282,3 +282,68 @@ def test_scale22_full_size_properties_and_parity():
     assert np.array_equal(fixed, again) and st["iterations"] == 5
     ref5, _, _ = oracle.pagerank_pull(g.V, g.E, None, alpha=0.85, max_iter=5, tol=0.0)
     assert np.abs(fixed - ref5).sum() <= L1_TOL
+
+
+def _seed_teleport(n, s):
+    p = np.zeros(n)
+    p[np.unique(s)] = 1.0
+    return p / p.sum()
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_ppr_batch_seed_sets_match_oracle(weighted):
+    g = synth.rmat(scale=12, edgefactor=16, seed=31, weighted=weighted)
+    sets = synth.seed_sets(g.n, 40, 1, 64, seed=3)  # 40 columns: one full panel and a partial one
+    pg = _native.PreparedGraph(g.V, g.E, g.W)
+    ranks, stats = pg.pagerank_seeds(sets, alpha=0.85, max_iter=100, tol=1e-6)
+    assert ranks.shape == (40, g.n)
+    for j in range(0, 40, 3):
+        _check_against_oracle(g.V, g.E, g.W, ranks[j], stats[j], 0.85, 100, 1e-6, teleport=_seed_teleport(g.n, sets[j]))
+    # the same columns solved one at a time through the plain path
+    for j in (0, 33):
+        single, st = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6, personalization=_seed_teleport(g.n, sets[j]))
+        assert st["iterations"] == stats[j]["iterations"]
+        assert np.abs(single - ranks[j]).sum() <= L1_TOL
+
+
+def test_ppr_batch_fixed_iterations_and_dense_teleport():
+    g = synth.rmat(scale=13, edgefactor=16, seed=32)
+    rng = np.random.default_rng(0)
+    T = rng.random((5, g.n))
+    T[1] = 0.0
+    T[1, 7] = 2.0
+    pg = _native.PreparedGraph(g.V, g.E)
+    ranks, stats = pg.pagerank_batch(T, alpha=0.85, max_iter=15, tol=0.0)
+    for j in range(5):
+        assert stats[j]["iterations"] == 15
+        _check_against_oracle(g.V, g.E, None, ranks[j], stats[j], 0.85, 15, 0.0, teleport=T[j] / T[j].sum())
+
+
+def test_ppr_batch_uniform_column_reproduces_plain_pagerank():
+    g = synth.rmat(scale=12, edgefactor=16, seed=33)
+    pg = _native.PreparedGraph(g.V, g.E)
+    plain, st = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+    ranks, stats = pg.pagerank_batch(np.full((1, g.n), 1.0), alpha=0.85, max_iter=100, tol=1e-6)
+    assert stats[0]["iterations"] == st["iterations"]
+    assert np.abs(ranks[0] - plain).sum() <= L1_TOL
+
+
+def test_ppr_batch_is_deterministic_and_columns_independent():
+    g = synth.rmat(scale=12, edgefactor=16, seed=34)
+    sets = synth.seed_sets(g.n, 64, 1, 16, seed=9)
+    pg = _native.PreparedGraph(g.V, g.E)
+    a, _ = pg.pagerank_seeds(sets, alpha=0.85, max_iter=30, tol=1e-6)
+    b, _ = pg.pagerank_seeds(sets, alpha=0.85, max_iter=30, tol=1e-6)
+    assert np.array_equal(a, b)
+    sub, _ = pg.pagerank_seeds(sets[5:9], alpha=0.85, max_iter=30, tol=1e-6)
+    assert np.abs(sub - a[5:9]).sum(axis=1).max() <= L1_TOL
+
+
+def test_ppr_through_the_api_batch():
+    G = DiGraph()
+    G.add_edges_from([("a", "b"), ("b", "c"), ("c", "a"), ("c", "d"), ("d", "a")])
+    res = prmod.pagerank_batch(G, [{"a": 1.0}, {"d": 1.0, "b": 1.0}])
+    V, E, _ = oracle.graph_to_csr(list(G.nodes), G._adj, True)
+    for r, p in zip(res, ([1, 0, 0, 0], [0, 0.5, 0, 0.5])):
+        ref, _, _ = oracle.pagerank_push(V, E, None, teleport=np.array(p, float))
+        assert np.allclose(r.to_numpy(), ref, rtol=2e-5, atol=1e-7)

@@ -1,0 +1,165 @@
+"""Serving loop: scheduling and admission on CPU with a fake native engine,
+and on the GPU that every request's answer in the mix equals its answer alone."""
+
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from eggpu_b200 import _native, serving, synth
+from oracle import oracle
+
+
+class FakePrepared:
+    """Stands in for _native.PreparedGraph: answers with the oracle, records calls."""
+
+    calls = []
+    live = 0
+    lock = threading.Lock()
+
+    def __init__(self, V, E, W=None):
+        self.V, self.E, self.W = V, E, W
+        self.n = len(V) - 1
+        with FakePrepared.lock:
+            FakePrepared.live += 1
+
+    def info(self):
+        return {"device_bytes": serving.GraphRegistry.estimate_bytes(self.V, self.E, self.W)}
+
+    def pagerank(self, alpha, max_iter, tol, personalization=None):
+        FakePrepared.calls.append(("pr", self.n))
+        time.sleep(0.002)
+        r, it, res = oracle.pagerank_push(self.V, self.E, self.W, alpha=alpha, max_iter=max_iter, tol=tol)
+        return r, {"iterations": it}
+
+    def pagerank_seeds(self, seed_sets, alpha, max_iter, tol):
+        FakePrepared.calls.append(("ppr", self.n, len(seed_sets)))
+        time.sleep(0.002)
+        outs, sts = [], []
+        for s in seed_sets:
+            p = np.zeros(self.n)
+            p[np.unique(s)] = 1.0
+            r, it, _ = oracle.pagerank_push(self.V, self.E, self.W, alpha=alpha, max_iter=max_iter, tol=tol,
+                                            teleport=p / p.sum())
+            outs.append(r)
+            sts.append({"iterations": it})
+        return np.array(outs), sts
+
+    def close(self):
+        with FakePrepared.lock:
+            FakePrepared.live -= 1
+
+
+def fake_multi(graphs, alpha, max_iter, tol):
+    FakePrepared.calls.append(("multi", len(graphs)))
+    outs, sts = [], []
+    for g in graphs:
+        r, st = g.pagerank(alpha, max_iter, tol)
+        outs.append(r)
+        sts.append(st)
+    return outs, sts
+
+
+@pytest.fixture
+def fake_engine(monkeypatch):
+    FakePrepared.calls = []
+    FakePrepared.live = 0
+    monkeypatch.setattr(_native, "PreparedGraph", FakePrepared)
+    monkeypatch.setattr(_native, "pagerank_multi", fake_multi)
+    yield
+
+
+def _sources(k=5):
+    out = {}
+    for i in range(k):
+        c = synth.erdos_renyi(200 + 150 * i, 6.0, seed=2000 + i)
+        out[i] = (c.V, c.E, None)
+    return out
+
+
+def test_requests_are_folded_and_answers_match_standalone(fake_engine):
+    src = _sources()
+    reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
+    srv = serving.Server(reg, workers=2)
+    rng = np.random.default_rng(0)
+    reqs = []
+    for i in range(60):
+        gid = int(rng.integers(0, len(src)))
+        if i % 2:
+            reqs.append(serving.Request(gid, "ppr", seeds=rng.choice(src[gid][0].shape[0] - 1, 3, replace=False)))
+        else:
+            reqs.append(serving.Request(gid, "pr"))
+    for r in reqs:  # a burst: everything arrives at once
+        srv.submit(r)
+    for r in reqs:
+        ranks, st = r.future.result(timeout=60)
+        V, E, W = src[r.graph]
+        tele = None
+        if r.kind == "ppr":
+            p = np.zeros(V.shape[0] - 1)
+            p[np.unique(r.seeds)] = 1.0
+            tele = p / p.sum()
+        alone, it, _ = oracle.pagerank_push(V, E, W, teleport=tele)
+        assert np.array_equal(ranks, alone) and st["iterations"] == it
+    srv.close()
+    solves = [c for c in FakePrepared.calls if c[0] in ("pr", "ppr")]
+    assert len(solves) < len(reqs)  # folding happened
+    assert any(c[0] == "ppr" and c[2] > 1 for c in solves)
+    lat = serving.latency_summary(reqs)
+    assert lat["count"] == 60 and lat["p99_ms"] >= lat["p50_ms"]
+
+
+def test_admission_by_bytes_evicts_idle_graphs(fake_engine):
+    src = _sources()
+    sizes = [serving.GraphRegistry.estimate_bytes(*src[i]) for i in src]
+    reg = serving.GraphRegistry(src, budget_bytes=max(sizes) * 2 + 1)
+    for gid in list(src) * 2:
+        pg = reg.acquire(gid)
+        assert pg is reg.resident[gid]
+        assert sum(g.info()["device_bytes"] for g in reg.resident.values()) <= reg.budget
+        reg.release(gid)
+    assert reg.evictions > 0 and FakePrepared.live == len(reg.resident) <= 2
+    reg.close()
+
+
+def test_poisson_arrivals_are_seeded():
+    a = serving.poisson_arrivals(1000.0, 500, seed=1)
+    assert np.array_equal(a, serving.poisson_arrivals(1000.0, 500, seed=1))
+    assert 0.3 < a[-1] < 0.7 and np.all(np.diff(a) > 0)
+
+
+@pytest.mark.gpu
+def test_served_results_equal_standalone_results_on_gpu():
+    src = {}
+    for i, (scale, ef) in enumerate(((10, 8), (12, 16), (13, 12), (11, 32))):
+        c = synth.rmat(scale=scale, edgefactor=ef, seed=2000 + i)
+        src[i] = (c.V, c.E, None)
+    reg = serving.GraphRegistry(src, budget_bytes=1 << 34)
+    srv = serving.Server(reg, workers=3)
+    rng = np.random.default_rng(1)
+    reqs = []
+    for i in range(300):
+        gid = int(rng.integers(0, len(src)))
+        n = src[gid][0].shape[0] - 1
+        if i % 2:
+            reqs.append(serving.Request(gid, "ppr", seeds=rng.choice(n, int(rng.integers(1, 17)), replace=False)))
+        else:
+            reqs.append(serving.Request(gid, "pr"))
+    times = serving.poisson_arrivals(2000.0, len(reqs), seed=2)
+    serving.replay(srv, reqs, times)
+    srv.close()
+    alone = {gid: _native.PreparedGraph(*src[gid]) for gid in src}
+    for r in reqs:
+        ranks, st = r.future.result()
+        pg = alone[r.graph]
+        if r.kind == "pr":
+            ref, rst = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+        else:
+            p = np.zeros(pg.n)
+            p[np.unique(r.seeds)] = 1.0
+            ref, rst = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6, personalization=p)
+        assert abs(st["iterations"] - rst["iterations"]) <= 1
+        assert np.abs(ranks - ref).sum() <= 1e-6
+    assert srv.stats["ppr_columns"] >= srv.stats["ppr_batches"]
+    reg.close()
