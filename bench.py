@@ -305,6 +305,207 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _ppr_teleport(n, s):
+    p = np.zeros(n)
+    p[np.unique(s)] = 1.0
+    return p / p.sum()
+
+
+def run_ppr(args):
+    """Batched PPR (R-MAT scale 20, seed 3, k=256 seed sets of 1-64 vertices) against
+    k plain single-vector solves on the same GPU; accuracy against the FP64 oracle."""
+    import torch
+
+    from eggpu_b200 import _native, synth
+    from oracle import oracle
+
+    torch.cuda.set_device(0)
+    g = synth.rmat(scale=20, edgefactor=16, seed=3)
+    sets = synth.seed_sets(g.n, 256, 1, 64, seed=3)
+    pg = _native.PreparedGraph(g.V, g.E)
+    out = {}
+    for label, max_iter, tol in (("rule", 100, 1e-6), ("fixed20", 20, 0.0)):
+        pg.pagerank_seeds(sets, alpha=0.85, max_iter=max_iter, tol=tol)  # warm-up
+        t0 = time.perf_counter()
+        reps = max(1, args.steps // 50)
+        for _ in range(reps):
+            ranks, sts = pg.pagerank_seeds(sets, alpha=0.85, max_iter=max_iter, tol=tol)
+        wall = (time.perf_counter() - t0) / reps
+        dev = sts[0]["kernel_seconds"]
+        sample = list(range(0, 256, 32))
+        t0 = time.perf_counter()
+        dev_single = 0.0
+        for j in sample:
+            _, st = pg.pagerank(alpha=0.85, max_iter=max_iter, tol=tol, personalization=_ppr_teleport(g.n, sets[j]))
+            dev_single += st["kernel_seconds"]
+        wall_single = (time.perf_counter() - t0) / len(sample)
+        dev_single /= len(sample)
+        errs = []
+        for j in sample[:4]:
+            ref, it, _ = oracle.pagerank_pull(g.V, g.E, None, alpha=0.85, max_iter=max_iter, tol=tol,
+                                              teleport=_ppr_teleport(g.n, sets[j]))
+            errs.append((float(np.abs(ranks[j] - ref).sum()), float(np.abs(ranks[j] - ref).max()),
+                         sts[j]["iterations"], it))
+        out[label] = {
+            "batched_solves_per_s_device": 256 / dev, "batched_solves_per_s_e2e": 256 / wall,
+            "plain_solves_per_s_device": 1 / dev_single, "plain_solves_per_s_e2e": 1 / wall_single,
+            "speedup_device": (256 / dev) / (1 / dev_single), "speedup_e2e": (256 / wall) / (1 / wall_single),
+            "iterations": sts[0]["iterations"], "batch_device_ms": dev * 1e3, "batch_wall_ms": wall * 1e3,
+            "max_l1_vs_fp64_oracle": max(e[0] for e in errs), "max_abs_vs_fp64_oracle": max(e[1] for e in errs),
+            "iterations_vs_oracle": [(e[2], e[3]) for e in errs],
+            "bytes_per_sweep_ppr": sts[0]["bytes_per_iter"],
+        }
+    line = {"metric": METRIC, "value": out["rule"]["batched_solves_per_s_e2e"], "unit": "PPR solves/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "ppr: R-MAT scale 20 (seed 3, edgefactor 16), k=256 teleport vectors uniform over "
+                                   "seed sets of 1-64 vertices (numpy PCG64 seed 3), alpha 0.85; 'rule' = tol 1e-6 "
+                                   "max_iter 100, 'fixed20' = 20 sweeps", "n": g.n, "nnz": pg.nnz},
+            "ppr": out}
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args):
+    """512 independent Erdos-Renyi graphs in one persistent launch per sweep vs one solve per graph."""
+    import torch
+
+    from eggpu_b200 import _native, synth
+
+    torch.cuda.set_device(0)
+    rng = np.random.Generator(np.random.PCG64(1000))
+    count = 512
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(2e5), size=count)).astype(np.int64)
+    ds = rng.uniform(8.0, 32.0, size=count)
+    graphs, nnz = [], 0
+    for i in range(count):
+        c = synth.erdos_renyi(int(ns[i]), float(ds[i]), seed=1000 + i)
+        pg = _native.PreparedGraph(c.V, c.E)
+        nnz += pg.nnz
+        graphs.append(pg)
+    _native.pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6)
+    reps = max(1, args.steps // 50)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        outs, sts = _native.pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6)
+    wall = (time.perf_counter() - t0) / reps
+    dev = sts[0]["kernel_seconds"]
+    its = [s["iterations"] for s in sts]
+    t0 = time.perf_counter()
+    dev_single = 0.0
+    for pg in graphs:
+        _, st = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+        dev_single += st["kernel_seconds"]
+    wall_single = time.perf_counter() - t0
+    sweeps_edges = sum(pg.nnz * it for pg, it in zip(graphs, its))
+    line = {"metric": METRIC, "value": count / wall, "unit": "graph solves/s", "higher_is_better": True,
+            "n_gpus": 1, "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "batch: 512 directed Erdos-Renyi graphs, n log-uniform in [1e3, 2e5], mean "
+                                   "out-degree uniform in [8, 32] (numpy PCG64 seed 1000), graph seeds 1000-1511, "
+                                   "alpha 0.85, tol 1e-6", "total_nnz": int(nnz)},
+            "batch": {"multi_solves_per_s_e2e": count / wall, "multi_solves_per_s_device": count / dev,
+                      "plain_solves_per_s_e2e": count / wall_single, "plain_solves_per_s_device": count / dev_single,
+                      "speedup_e2e": wall_single / wall, "speedup_device": dev_single / dev,
+                      "multi_device_ms": dev * 1e3, "multi_wall_ms": wall * 1e3,
+                      "iterations_min_max": [min(its), max(its)], "gteps_device": sweeps_edges / dev / 1e9}}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Poisson arrivals (1000 req/s, 50/50 PageRank/PPR with 1-16 seeds) over 64 R-MAT graphs
+    (n log-uniform in [1e3, 1e7], edgefactor uniform in [8, 32], seeds 2000-2063)."""
+    import torch
+
+    from eggpu_b200 import _native, serving, synth
+
+    torch.cuda.set_device(0)
+    rng = np.random.Generator(np.random.PCG64(2000))
+    count = 64
+    max_n = int(args.serving_max_n)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(max_n), size=count)).astype(np.int64)
+    efs = rng.integers(8, 33, size=count)
+    src = {}
+    for i in range(count):
+        scale = int(np.ceil(np.log2(ns[i])))
+        c = synth.rmat(scale=scale, edgefactor=int(efs[i]), seed=2000 + i, keep_n=int(ns[i]))
+        src[i] = (c.V, c.E, None)
+    n_req = int(args.serving_requests)
+    kinds = rng.random(n_req) < 0.5
+    gids = rng.integers(0, count, size=n_req)
+    reqs = []
+    for k, gid in zip(kinds, gids):
+        n = src[int(gid)][0].shape[0] - 1
+        if k:
+            reqs.append(serving.Request(int(gid), "pr"))
+        else:
+            size = int(rng.integers(1, 17))
+            reqs.append(serving.Request(int(gid), "ppr", seeds=rng.choice(n, min(size, n), replace=False)))
+    budget = int(args.serving_hbm_gb * 2**30)
+    reg = serving.GraphRegistry(src, budget_bytes=budget)
+    srv = serving.Server(reg, workers=4)
+    times = serving.poisson_arrivals(1000.0, n_req, seed=2001)
+    wall = serving.replay(srv, reqs, times)
+    srv.close()
+    lat = serving.latency_summary(reqs)
+    # plain unbatched per-request solves of a sample, on the same GPU
+    sample = reqs[:: max(1, n_req // 200)]
+    plain_lat = []
+    for r in sample:
+        pg = reg.acquire(r.graph)
+        try:
+            t0 = time.perf_counter()
+            if r.kind == "pr":
+                pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+            else:
+                pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6, personalization=_ppr_teleport(pg.n, r.seeds))
+            plain_lat.append(time.perf_counter() - t0)
+        finally:
+            reg.release(r.graph)
+    plain = np.array(plain_lat)
+    line = {"metric": METRIC, "value": n_req / wall, "unit": "solves/s", "higher_is_better": True, "n_gpus": 1,
+            "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "serving: Poisson arrivals at 1000 req/s, 50/50 PageRank/PPR (1-16 seeds), 64 "
+                                   f"R-MAT graphs n log-uniform in [1e3, {max_n:.0e}] (ids >= n dropped), edgefactor "
+                                   "uniform in [8, 32], seeds 2000-2063, alpha 0.85, tol 1e-6",
+                       "requests": n_req, "hbm_budget_gb": args.serving_hbm_gb,
+                       "total_nnz": int(sum(len(v[1]) for v in src.values()))},
+            "serving": {"latency": lat, "solves_per_s": n_req / wall, "offered_req_per_s": 1000.0,
+                        "server_stats": dict(srv.stats), "admissions": reg.admissions, "evictions": reg.evictions,
+                        "plain_unbatched_service_ms": {"p50": float(np.percentile(plain, 50) * 1e3),
+                                                       "p99": float(np.percentile(plain, 99) * 1e3),
+                                                       "mean": float(plain.mean() * 1e3)},
+                        "plain_unbatched_capacity_solves_per_s": float(1.0 / plain.mean())}}
+    reg.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_precision25(args):
+    """R-MAT scale 25 weighted (seed 2), tol 1e-7: error of the engine against the FP64 oracle."""
+    import torch
+
+    from eggpu_b200 import _native, synth
+    from oracle import oracle
+
+    torch.cuda.set_device(0)
+    g = synth.rmat(scale=25, edgefactor=16, seed=2, weighted=True)
+    pg = _native.PreparedGraph(g.V, g.E, g.W)
+    res = {}
+    for label, max_iter, tol, corr in (("rule_tol1e-7", 100, 1e-7, True), ("fixed10", 10, 0.0, True),
+                                       ("fixed10_no_correction", 10, 0.0, False)):
+        ranks, st = pg.pagerank(alpha=0.85, max_iter=max_iter, tol=tol, correction=corr)
+        ref, it, _ = oracle.pagerank_pull(g.V, g.E, g.W, alpha=0.85, max_iter=max_iter, tol=tol)
+        res[label] = {"iterations": st["iterations"], "oracle_iterations": it,
+                      "l1_vs_fp64_oracle": float(np.abs(ranks - ref).sum()),
+                      "max_abs_vs_fp64_oracle": float(np.abs(ranks - ref).max()),
+                      "solve_ms": st["kernel_seconds"] * 1e3}
+    ranks, st = pg.pagerank(alpha=0.85, max_iter=20, tol=0.0)
+    gteps = pg.nnz * 20 / st["kernel_seconds"] / 1e9
+    line = {"metric": METRIC, "value": gteps, "unit": "GTEPS/iter", "higher_is_better": True, "n_gpus": 1,
+            "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "rmat25w: R-MAT scale 25 (seed 2, edgefactor 16), weights U(0,1] FP32, alpha 0.85",
+                       "n": g.n, "nnz": pg.nnz},
+            "precision": res, "hbm_gbs_20_sweeps": st["bytes_per_iter"] * 20 / st["kernel_seconds"] / 1e9}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,9 +518,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serving-max-n", type=float, default=1e7)
+    ap.add_argument("--serving-requests", type=int, default=10000)
+    ap.add_argument("--serving-hbm-gb", type=float, default=64.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ppr":
+        run_ppr(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "serving":
+        run_serving(args)
+    elif args.workload == "precision25":
+        run_precision25(args)
     else:
         run_ours(args)
 

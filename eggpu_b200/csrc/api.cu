@@ -87,7 +87,11 @@ void Plan::release() {
     d_span_cnt.release();
     d_span_part.release();
     d_ctl.release();
-    ngraphs = nchunks = grid = grid_final = max_n = 0;
+    d_groups.release();
+    d_group_cnt.release();
+    d_group_part.release();
+    d_span_list.release();
+    ngraphs = nchunks = grid = grid_final = max_n = ngroups = 0;
 }
 
 int check_device(const egpr_graph* g) {
@@ -301,6 +305,8 @@ static uint64_t bits_of(double x) {
 
 int64_t egpr_graph::device_bytes() const {
     return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes + sub_coord.bytes +
+                     tile_coord.bytes + plan.d_groups.bytes + plan.d_group_cnt.bytes + plan.d_group_part.bytes +
+                     plan.d_span_list.bytes +
                      scale.bytes + tele.bytes + x0.bytes + x1.bytes + z0.bytes + z1.bytes + out.bytes + z64.bytes +
                      plan.d_chunks.bytes + plan.d_graphs.bytes + plan.d_states.bytes + plan.d_ndang.bytes +
                      plan.d_chunk_part.bytes + plan.d_piece.bytes + plan.d_span_cnt.bytes + plan.d_span_part.bytes +
@@ -318,7 +324,8 @@ static void destroy_graph_object(egpr_graph* g) {
     if (g->own_stream) cudaStreamSynchronize(g->own_stream);
     spmm_work_release(g);
     g->plan.release();
-    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord, &g->scale, &g->tele,
+    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord, &g->tile_coord,
+                      &g->scale, &g->tele,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})
         b->release();
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -382,7 +389,7 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
     }
     const size_t nf = (size_t)n * sizeof(float), nd = (size_t)n * sizeof(double);
     if ((rc = g->scale.alloc(nf)) || (rc = g->tele.alloc(nf)) || (rc = g->x0.alloc(nf)) || (rc = g->x1.alloc(nf)) ||
-        (rc = g->z0.alloc(nf)) || (rc = g->z1.alloc(nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd))) {
+        (rc = g->z0.alloc(2 * nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd))) {
         destroy_graph_object(g);
         return rc;
     }
@@ -391,6 +398,7 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
         destroy_graph_object(g);
         return rc;
     }
+    plan_set_l2_window(g->plan, g->z0.p, 2 * nf);
     *out = g;
     return EGPR_SUCC;
 }

@@ -33,13 +33,27 @@ constexpr int32_t kHasTail = 2;    // the chunk's last row continues into a late
 constexpr int32_t kInterior = 4;   // the chunk lies inside one row (head and tail are that row)
 
 struct Chunk {
-    int32_t sub_begin;   // first sub-tile (index into the graph's sub_coord table)
-    int32_t sub_end;     // one past the last sub-tile
+    int32_t sub_begin;   // first sub-tile (index into the graph's tile-coordinate table)
+    int32_t sub_end;     // one past the last sub-tile (coordinate sub_end closes the chunk)
     int32_t graph;       // slot in the plan's graph table
     int32_t flags;
     int32_t head_ta;     // global chunk id where the head row's span starts
     int32_t tail_tb;     // global chunk id where the tail row's span ends
     int32_t tail_row;    // vertex id of the tail row (span rows are finalised by row id)
+    int32_t group;       // global reduction group (sweep chunks only)
+};
+
+// The sweep's warp tiles: kTileItems merge items per warp sub-tile, chunks of
+// whole rows (cut only inside rows longer than a chunk), and reduction groups
+// of at most kGroupChunks consecutive chunks of one graph.
+constexpr int kLaneItems = 8;
+constexpr int kTileItems = 32 * kLaneItems;
+constexpr int kGroupChunks = 64;
+
+struct Group {
+    int32_t chunk_begin;
+    int32_t chunk_end;
+    int32_t graph;
     int32_t pad;
 };
 
@@ -48,7 +62,7 @@ struct GraphDev {
     const int32_t* in_row;   // n+1
     const int32_t* in_col;   // nnz
     const float* in_w;       // nnz, NULL = unit weights
-    const int2* sub_coord;   // merge-path coordinates (row, entry) of sub-tile starts
+    const int2* sub_coord;   // merge-path coordinates (row, entry) of the sweep's warp tiles
     const double* outw;      // n, FP64 out-weight sums
     const float* scale;      // n, alpha/outw (FP32) or -1 for dangling vertices
     const float* tele;       // n, personalisation (NULL = uniform)
@@ -59,6 +73,10 @@ struct GraphDev {
     int32_t n;
     int32_t chunk_begin;     // this graph's global chunk id range
     int32_t chunk_end;
+    int32_t group_begin;     // this graph's global reduction groups
+    int32_t group_end;
+    int32_t span_begin;      // this graph's entries of the span list (span start chunks)
+    int32_t span_end;
     int32_t pad;
 };
 
@@ -99,9 +117,14 @@ struct SweepParams {
     double* piece;           // 2 per chunk: head piece, tail piece
     uint32_t* span_cnt;      // per chunk (span start)
     double* span_part;       // 3 per chunk (span start): err, dsum, xsum of span rows
+    const Group* groups;
+    uint32_t* group_cnt;     // chunk arrivals per group
+    double* group_part;      // 3 per group
+    const int32_t* span_list;  // span start chunks, per graph ranges
     Ctl* ctl;
     cudaGraphConditionalHandle cond;
     int32_t use_cond;
+    int32_t total_warps;     // warps of the launch (exit accounting)
 };
 
 // ---- device buffers --------------------------------------------------------
@@ -121,13 +144,20 @@ struct Plan {
     int32_t grid = 0;        // CTAs of an FP32 sweep
     int32_t grid_final = 0;  // CTAs of the FP64 correction sweep
     int32_t max_n = 0;
-    DevBuf d_chunks, d_graphs, d_states, d_ndang, d_chunk_part, d_piece, d_span_cnt, d_span_part, d_ctl;
+    DevBuf d_chunks, d_graphs, d_states, d_ndang, d_chunk_part, d_piece, d_span_cnt, d_span_part, d_ctl,
+        d_groups, d_group_cnt, d_group_part, d_span_list;
     std::vector<Chunk> h_chunks;      // a graph's own chunk table (local ids)
+    std::vector<Group> h_groups;      // a graph's own groups (local ids)
+    std::vector<int32_t> h_spans;     // a graph's span start chunks (local ids)
     std::vector<Chunk> h_chunks_all;  // the plan's table (global ids)
+    int32_t ngroups = 0;
     cudaGraph_t cg = nullptr;
     cudaGraphExec_t cg_exec = nullptr;
     cudaGraphConditionalHandle cond = 0;
     bool cg_failed = false;
+    void* l2_base = nullptr;  // persisting L2 window over the gathered vectors
+    size_t l2_bytes = 0;
+    float l2_hit_ratio = 0.f;
     ~Plan();
     void release();
 };
@@ -149,8 +179,9 @@ struct egpr_graph {
     double prep_seconds = 0.0;
     int32_t nsub = 0;              // sub-tiles
     int32_t chunk_subs = 1;        // sub-tiles per chunk
+    int32_t ntiles = 0;            // warp tiles of the sweep
     // prepared graph
-    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord;
+    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord, tile_coord;
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
     egpr::Plan plan;               // single-graph plan
@@ -175,11 +206,15 @@ double wall_seconds();
 // Preparation (prep.cu).
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
 int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
+int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s);
+int sweep_resident_warps();
+int chunks_per_warp();
 
 // Plans and sweeps (sweep.cu).
 int sweep_occupancy_grid(int mode);
 int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_t stream);
 int plan_capture_loop(Plan& plan, cudaStream_t stream);
+void plan_set_l2_window(Plan& plan, void* base, size_t bytes);
 GraphDev graph_dev_view(const egpr_graph* g);
 int launch_init(Plan& plan, double alpha, int32_t max_iter, double tol, bool personalised,
                 cudaStream_t stream);

@@ -371,6 +371,136 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, cudaStrea
     return rc;
 }
 
+namespace {
+
+// (row, entry, start of that row, diagonal) at ideal chunk boundaries d = c * chunk_items.
+__global__ void k_ideal_bounds(const int32_t* __restrict__ in_row, int32_t n, int64_t nnz, int64_t chunk_items,
+                               int32_t count, int4* __restrict__ out) {
+    const int64_t total = (int64_t)n + nnz;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= count; c += gridDim.x * blockDim.x) {
+        int64_t d = (int64_t)c * chunk_items;
+        if (d > total) d = total;
+        const int2 rc = merge_search(in_row, n, nnz, d);
+        out[c] = make_int4(rc.x, rc.y, rc.x < n ? in_row[rc.x] : (int32_t)nnz, 0);
+    }
+}
+
+// Coordinates of every warp tile: chunk c owns slots [off_c, off_c + subs_c], slot s
+// at diagonal min(d_c + s * kTileItems, d_{c+1}).
+__global__ void k_tile_coords(const int32_t* __restrict__ in_row, int32_t n, int64_t nnz,
+                              const int64_t* __restrict__ chunk_d, const int32_t* __restrict__ chunk_off,
+                              int32_t nchunks, int2* __restrict__ coord) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
+        const int64_t d0 = chunk_d[c], d1 = chunk_d[c + 1];
+        const int32_t off = chunk_off[c], subs = chunk_off[c + 1] - off - 1;
+        for (int32_t s = 0; s <= subs; ++s) {
+            int64_t d = d0 + (int64_t)s * kTileItems;
+            if (d > d1) d = d1;
+            coord[off + s] = merge_search(in_row, n, nnz, d);
+        }
+    }
+}
+
+}  // namespace
+
+// The sweep's work decomposition.  Chunk boundaries start at ideal diagonals
+// c * chunk_items and are moved back to the start of the row they fall in, so
+// a chunk holds whole rows; only a row longer than a chunk is cut (a span).
+// Chunks are cut into warp tiles of kTileItems items and grouped by
+// kGroupChunks for the reduction tree.
+int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s) {
+    const int32_t n = g->n;
+    const int64_t nnz = g->nnz;
+    const int64_t total = (int64_t)n + nnz;
+    const int32_t ideal = (int32_t)std::max<int64_t>(1, (total + chunk_items - 1) / chunk_items);
+    int4* bounds = nullptr;
+    int rc = cuda_ok(cudaMallocAsync(&bounds, ((size_t)ideal + 1) * sizeof(int4), s), "cudaMallocAsync (bounds)");
+    if (rc) return rc;
+    k_ideal_bounds<<<grid_for((int64_t)ideal + 1), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, nnz, chunk_items,
+                                                                     ideal, bounds);
+    std::vector<int4> hb((size_t)ideal + 1);
+    rc = cuda_ok(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int4), cudaMemcpyDeviceToHost, s), "D2H bounds");
+    cudaFreeAsync(bounds, s);
+    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "sweep tiles"))) return rc;
+    // Snap: (row, entry, row start) per boundary.
+    struct B {
+        int32_t r, k, rs;
+        int64_t d;
+    };
+    std::vector<B> bs;
+    bs.push_back(B{0, 0, 0, 0});
+    for (int32_t c = 1; c < ideal; ++c) {
+        const int4 b = hb[(size_t)c];
+        B snapped{b.x, b.z, b.z, (int64_t)b.x + b.z};
+        B cut{b.x, b.y, b.z, (int64_t)b.x + b.y};
+        if (snapped.d > bs.back().d) bs.push_back(snapped);
+        else if (cut.d > bs.back().d) bs.push_back(cut);
+    }
+    if (total > bs.back().d) bs.push_back(B{n, (int32_t)nnz, (int32_t)nnz, total});
+    const int32_t nch = (int32_t)bs.size() - 1;
+    std::vector<int64_t> cd((size_t)nch + 1);
+    std::vector<int32_t> off((size_t)nch + 1);
+    off[0] = 0;
+    for (int32_t c = 0; c < nch; ++c) {
+        cd[(size_t)c] = bs[(size_t)c].d;
+        const int64_t items = bs[(size_t)c + 1].d - bs[(size_t)c].d;
+        const int32_t subs = (int32_t)std::max<int64_t>(1, (items + kTileItems - 1) / kTileItems);
+        off[(size_t)c + 1] = off[(size_t)c] + subs + 1;
+    }
+    cd[(size_t)nch] = bs[(size_t)nch].d;
+    const int32_t slots = off[(size_t)nch];
+    if ((rc = g->tile_coord.alloc((size_t)slots * sizeof(int2)))) return rc;
+    int64_t* d_cd = nullptr;
+    int32_t* d_off = nullptr;
+    if ((rc = cuda_ok(cudaMallocAsync(&d_cd, cd.size() * sizeof(int64_t), s), "cudaMallocAsync")) ||
+        (rc = cuda_ok(cudaMallocAsync(&d_off, off.size() * sizeof(int32_t), s), "cudaMallocAsync")))
+        return rc;
+    cudaMemcpyAsync(d_cd, cd.data(), cd.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    k_tile_coords<<<grid_for(nch), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, nnz, d_cd, d_off, nch,
+                                                      g->tile_coord.as<int2>());
+    cudaFreeAsync(d_cd, s);
+    cudaFreeAsync(d_off, s);
+    if ((rc = cuda_ok(cudaStreamSynchronize(s), "sweep tiles"))) return rc;
+    // Chunk table (local ids), spans and groups.
+    std::vector<Chunk>& ch = g->plan.h_chunks;
+    ch.assign((size_t)nch, Chunk{});
+    for (int32_t c = 0; c < nch; ++c) {
+        Chunk& k = ch[(size_t)c];
+        const B& a = bs[(size_t)c];
+        const B& b = bs[(size_t)c + 1];
+        k.sub_begin = off[(size_t)c];
+        k.sub_end = off[(size_t)c + 1] - 1;
+        k.graph = 0;
+        const bool head = a.k > a.rs;
+        const bool tail = b.r < n && b.k > b.rs;
+        int32_t f = 0;
+        if (head) f |= kHasHead;
+        if (tail) f |= kHasTail;
+        if (head && tail && a.r == b.r) f |= kInterior;
+        k.flags = f;
+        k.tail_row = tail ? b.r : -1;
+        k.head_ta = -1;
+        k.tail_tb = -1;
+        k.group = c / kGroupChunks;
+    }
+    g->plan.h_spans.clear();
+    for (int32_t c = 0; c < nch; ++c) {
+        Chunk& k = ch[(size_t)c];
+        if (k.flags & kHasHead) k.head_ta = (ch[(size_t)c - 1].flags & kInterior) ? ch[(size_t)c - 1].head_ta : c - 1;
+        if ((k.flags & kHasTail) && !(k.flags & kInterior)) g->plan.h_spans.push_back(c);
+    }
+    for (int32_t c = nch - 1; c >= 0; --c) {
+        Chunk& k = ch[(size_t)c];
+        if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
+    }
+    g->plan.h_groups.clear();
+    for (int32_t c = 0; c < nch; c += kGroupChunks)
+        g->plan.h_groups.push_back(Group{c, std::min(nch, c + kGroupChunks), 0, 0});
+    g->ntiles = slots - nch;
+    return EGPR_SUCC;
+}
+
 // Chunk table over a graph's sub-tiles: runs of chunk_subs sub-tiles, with the
 // span links of rows cut by chunk boundaries (chunk ids local to the graph).
 int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& ch, cudaStream_t s) {
@@ -402,7 +532,7 @@ int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& ch,
         k.tail_row = tail ? b.x : -1;
         k.head_ta = -1;
         k.tail_tb = -1;
-        k.pad = 0;
+        k.group = 0;
     }
     for (int32_t c = 0; c < nch; ++c) {
         Chunk& k = ch[(size_t)c];
@@ -485,11 +615,12 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                                                                        g->sub_coord.as<int2>());
         g->n_dangling = (int32_t)hc[0];
         g->n_dangling_solve = (int32_t)hc[1];
-        // Chunks: about two per resident CTA so the queue can balance.
-        const int grid = sweep_occupancy_grid(0);
-        const int32_t target_chunks = std::max(1, 2 * grid);
-        g->chunk_subs = std::max<int32_t>(1, (g->nsub + target_chunks - 1) / target_chunks);
-        if ((rc = build_chunk_table(g, g->chunk_subs, g->plan.h_chunks, s))) return rc;
+        // Sweep chunks: about kChunksPerWarp per resident warp so the queue balances.
+        const int64_t warps = std::max(1, sweep_resident_warps());
+        const int64_t per_warp = chunks_per_warp();
+        int64_t chunk_items = (total + warps * per_warp - 1) / (warps * per_warp);
+        chunk_items = std::max<int64_t>(kTileItems, (chunk_items + kTileItems - 1) / kTileItems * kTileItems);
+        if ((rc = build_sweep_tiles(g, chunk_items, s))) return rc;
     }
     cudaEventRecord(g->ev1, s);
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "preparation"))) return rc;
