@@ -305,7 +305,8 @@ static uint64_t bits_of(double x) {
 
 int64_t egpr_graph::device_bytes() const {
     return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes + sub_coord.bytes +
-                     tile_coord.bytes + plan.d_groups.bytes + plan.d_group_cnt.bytes + plan.d_group_part.bytes +
+                     tile_coord.bytes + hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_groups.bytes +
+                     plan.d_group_cnt.bytes + plan.d_group_part.bytes +
                      plan.d_span_list.bytes +
                      scale.bytes + tele.bytes + x0.bytes + x1.bytes + z0.bytes + z1.bytes + out.bytes + z64.bytes +
                      plan.d_chunks.bytes + plan.d_graphs.bytes + plan.d_states.bytes + plan.d_ndang.bytes +
@@ -325,7 +326,7 @@ static void destroy_graph_object(egpr_graph* g) {
     spmm_work_release(g);
     g->plan.release();
     for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord, &g->tile_coord,
-                      &g->scale, &g->tele,
+                      &g->hub_ids, &g->hub_slot, &g->hubz, &g->scale, &g->tele,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})
         b->release();
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -389,7 +390,8 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
     }
     const size_t nf = (size_t)n * sizeof(float), nd = (size_t)n * sizeof(double);
     if ((rc = g->scale.alloc(nf)) || (rc = g->tele.alloc(nf)) || (rc = g->x0.alloc(nf)) || (rc = g->x1.alloc(nf)) ||
-        (rc = g->z0.alloc(2 * nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd))) {
+        (rc = g->z0.alloc(2 * nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd)) ||
+        (rc = g->hubz.alloc(2 * (size_t)std::max(g->nhub, 4) * sizeof(float)))) {
         destroy_graph_object(g);
         return rc;
     }
@@ -434,7 +436,7 @@ int egpr_graph_export_inbound(const egpr_graph* gc, int32_t* in_row, int32_t* in
     if ((rc = check_device(g))) return rc;
     cudaStream_t s = g->stream;
     if ((rc = cuda_ok(cudaMemcpyAsync(in_row, g->in_row.p, ((size_t)g->n + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H")) ||
-        (g->nnz > 0 && (rc = cuda_ok(cudaMemcpyAsync(in_col, g->in_col.p, (size_t)g->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H"))) ||
+        (rc = export_in_col(g, in_col, s)) ||
         (rc = cuda_ok(cudaMemcpyAsync(dangling01, g->dangling01.p, (size_t)g->n * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H")) ||
         (rc = cuda_ok(cudaMemcpyAsync(out_weight_sum, g->outw.p, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H")))
         return rc;

@@ -41,14 +41,23 @@ struct Chunk {
     int32_t tail_tb;     // global chunk id where the tail row's span ends
     int32_t tail_row;    // vertex id of the tail row (span rows are finalised by row id)
     int32_t group;       // global reduction group (sweep chunks only)
+    int32_t nnz_begin;   // entries [nnz_begin, nnz_end) belong to the chunk
+    int32_t nnz_end;
+    int32_t row_end;     // rows [first finished row of tile 0, row_end) are finished by the chunk
+    int32_t pad;
 };
 
-// The sweep's warp tiles: kTileItems merge items per warp sub-tile, chunks of
+// The sweep's warp tiles: kTileItems inbound entries per warp tile (each lane
+// kLaneItems consecutive entries, tile starts aligned to 8 entries), chunks of
 // whole rows (cut only inside rows longer than a chunk), and reduction groups
 // of at most kGroupChunks consecutive chunks of one graph.
 constexpr int kLaneItems = 8;
 constexpr int kTileItems = 32 * kLaneItems;
 constexpr int kGroupChunks = 64;
+// Hub cache: the carried values of the kHubCap sources with the largest
+// out-degree are kept in shared memory by the sweep; inbound entries from a hub
+// store -(slot + 1) instead of the source id.
+constexpr int kHubCap = 32768;
 
 struct Group {
     int32_t chunk_begin;
@@ -70,6 +79,10 @@ struct GraphDev {
     float* z[2];             // x * scale: the value each out-edge carries
     double* out;             // n, FP64 result
     double* z64;             // n, FP64 carried values for the correction sweep
+    const int32_t* hub_ids;  // nhub source ids of the hub slots
+    const int32_t* hub_slot; // n, slot of each vertex or -1
+    float* hubz[2];          // nhub carried values of the hubs, double-buffered with z
+    int32_t nhub;
     int32_t n;
     int32_t chunk_begin;     // this graph's global chunk id range
     int32_t chunk_end;
@@ -77,7 +90,6 @@ struct GraphDev {
     int32_t group_end;
     int32_t span_begin;      // this graph's entries of the span list (span start chunks)
     int32_t span_end;
-    int32_t pad;
 };
 
 struct GraphState {
@@ -125,6 +137,7 @@ struct SweepParams {
     cudaGraphConditionalHandle cond;
     int32_t use_cond;
     int32_t total_warps;     // warps of the launch (exit accounting)
+    int32_t hub_smem;        // 1: one graph, its hub values are staged in shared memory
 };
 
 // ---- device buffers --------------------------------------------------------
@@ -181,7 +194,8 @@ struct egpr_graph {
     int32_t chunk_subs = 1;        // sub-tiles per chunk
     int32_t ntiles = 0;            // warp tiles of the sweep
     // prepared graph
-    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord, tile_coord;
+    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord, tile_coord, hub_ids, hub_slot, hubz;
+    int32_t nhub = 0;
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
     egpr::Plan plan;               // single-graph plan
@@ -207,6 +221,7 @@ double wall_seconds();
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
 int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
 int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s);
+int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
 int sweep_resident_warps();
 int chunks_per_warp();
 

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -176,18 +177,22 @@ __device__ __forceinline__ double sanitize_w(double w) {
 // FP64 out-weight sum per source in entry order (pagerank.cu:301-316).  For
 // unit weights the sum is a count, which is exact in any order.
 __global__ void k_out_weight(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
-                             const double* __restrict__ W, int32_t n, double* __restrict__ outw) {
+                             const double* __restrict__ W, int32_t n, double* __restrict__ outw,
+                             uint32_t* __restrict__ hub_key, uint32_t* __restrict__ hub_val) {
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
          u += (int64_t)gridDim.x * blockDim.x) {
         const int32_t b = V[u], e = V[u + 1];
         double s = 0.0;
+        int32_t c = 0;
         if (W) {
             for (int32_t p = b; p < e; ++p) {
                 const int32_t v = E[p];
-                if (v >= 0 && v < n) s += sanitize_w(W[p]);
+                if (v >= 0 && v < n) {
+                    s += sanitize_w(W[p]);
+                    ++c;
+                }
             }
         } else {
-            int32_t c = 0;
             for (int32_t p = b; p < e; ++p) {
                 const int32_t v = E[p];
                 c += (v >= 0 && v < n) ? 1 : 0;
@@ -195,6 +200,36 @@ __global__ void k_out_weight(const int32_t* __restrict__ V, const int32_t* __res
             s = (double)c;
         }
         outw[u] = s;
+        // hub ranking: descending out-degree, ascending id (stable sort of ~count)
+        hub_key[u] = ~(uint32_t)c;
+        hub_val[u] = (uint32_t)u;
+    }
+}
+
+__global__ void k_hub_slots(const uint32_t* __restrict__ ranked, int32_t nhub, int32_t* __restrict__ hub_ids,
+                            int32_t* __restrict__ hub_slot) {
+    for (int32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nhub; s += gridDim.x * blockDim.x) {
+        const int32_t v = (int32_t)ranked[s];
+        hub_ids[s] = v;
+        hub_slot[v] = s;
+    }
+}
+
+// Inbound entries from a hub store -(slot + 1).
+__global__ void k_encode_hubs(int32_t* __restrict__ in_col, int64_t nnz, const int32_t* __restrict__ hub_slot) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t s = hub_slot[in_col[i]];
+        if (s >= 0) in_col[i] = -(s + 1);
+    }
+}
+
+__global__ void k_decode_hubs(const int32_t* __restrict__ in_col, int64_t nnz, const int32_t* __restrict__ hub_ids,
+                              int32_t* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = in_col[i];
+        out[i] = c < 0 ? hub_ids[-c - 1] : c;
     }
 }
 
@@ -381,22 +416,32 @@ __global__ void k_ideal_bounds(const int32_t* __restrict__ in_row, int32_t n, in
         int64_t d = (int64_t)c * chunk_items;
         if (d > total) d = total;
         const int2 rc = merge_search(in_row, n, nnz, d);
-        out[c] = make_int4(rc.x, rc.y, rc.x < n ? in_row[rc.x] : (int32_t)nnz, 0);
+        out[c] = make_int4(rc.x, rc.y, rc.x < n ? in_row[rc.x] : (int32_t)nnz,
+                           rc.x < n ? in_row[rc.x + 1] : (int32_t)nnz);
     }
 }
 
-// Coordinates of every warp tile: chunk c owns slots [off_c, off_c + subs_c], slot s
-// at diagonal min(d_c + s * kTileItems, d_{c+1}).
-__global__ void k_tile_coords(const int32_t* __restrict__ in_row, int32_t n, int64_t nnz,
-                              const int64_t* __restrict__ chunk_d, const int32_t* __restrict__ chunk_off,
-                              int32_t nchunks, int2* __restrict__ coord) {
+// Warp tiles of chunk c (boundaries (r_c, k_c) .. (r_{c+1}, k_{c+1})): tile t covers
+// entries [T_t, T_t + kTileItems) with T_t = (k_c & ~7) + t * kTileItems and
+// finishes the rows r in [r_c, r_{c+1}) whose end in_row[r+1] lies in
+// (T_t, T_t + kTileItems] (tile 0 also those ending at or before T_0, the last
+// tile all remaining).  coord[off_c + t] = (T_t, first finished row).
+__global__ void k_tile_coords(const int32_t* __restrict__ in_row, const int4* __restrict__ chunk_rk,
+                              const int32_t* __restrict__ chunk_off, int32_t nchunks, int2* __restrict__ coord) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
-        const int64_t d0 = chunk_d[c], d1 = chunk_d[c + 1];
-        const int32_t off = chunk_off[c], subs = chunk_off[c + 1] - off - 1;
-        for (int32_t s = 0; s <= subs; ++s) {
-            int64_t d = d0 + (int64_t)s * kTileItems;
-            if (d > d1) d = d1;
-            coord[off + s] = merge_search(in_row, n, nnz, d);
+        const int4 a = chunk_rk[c], b = chunk_rk[c + 1];  // (row, entry, -, -)
+        const int32_t off = chunk_off[c], nt = chunk_off[c + 1] - off;
+        const int32_t t0 = a.y & ~7;
+        coord[off] = make_int2(t0, a.x);
+        for (int32_t t = 1; t < nt; ++t) {
+            const int32_t T = t0 + t * kTileItems;
+            int32_t lo = a.x, hi = b.x;  // first row in [a.x, b.x) with in_row[r+1] > T
+            while (lo < hi) {
+                const int32_t mid = lo + ((hi - lo) >> 1);
+                if (in_row[mid + 1] > T) hi = mid;
+                else lo = mid + 1;
+            }
+            coord[off + t] = make_int2(T, lo);
         }
     }
 }
@@ -432,34 +477,37 @@ int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s) {
     for (int32_t c = 1; c < ideal; ++c) {
         const int4 b = hb[(size_t)c];
         B snapped{b.x, b.z, b.z, (int64_t)b.x + b.z};
-        B cut{b.x, b.y, b.z, (int64_t)b.x + b.y};
+        // A cut keeps at least one entry of the row for the next chunk: a point
+        // after the row's last entry becomes the start of the following row.
+        B cut = b.y < b.w ? B{b.x, b.y, b.z, (int64_t)b.x + b.y}
+                          : B{b.x + 1, b.y, b.y, (int64_t)b.x + 1 + b.y};
         if (snapped.d > bs.back().d) bs.push_back(snapped);
         else if (cut.d > bs.back().d) bs.push_back(cut);
     }
     if (total > bs.back().d) bs.push_back(B{n, (int32_t)nnz, (int32_t)nnz, total});
     const int32_t nch = (int32_t)bs.size() - 1;
-    std::vector<int64_t> cd((size_t)nch + 1);
+    std::vector<int4> rk((size_t)nch + 1);
     std::vector<int32_t> off((size_t)nch + 1);
     off[0] = 0;
+    for (int32_t c = 0; c <= nch; ++c) rk[(size_t)c] = make_int4(bs[(size_t)c].r, bs[(size_t)c].k, 0, 0);
     for (int32_t c = 0; c < nch; ++c) {
-        cd[(size_t)c] = bs[(size_t)c].d;
-        const int64_t items = bs[(size_t)c + 1].d - bs[(size_t)c].d;
-        const int32_t subs = (int32_t)std::max<int64_t>(1, (items + kTileItems - 1) / kTileItems);
-        off[(size_t)c + 1] = off[(size_t)c] + subs + 1;
+        const int64_t t0 = bs[(size_t)c].k & ~7;
+        const int64_t span = (int64_t)bs[(size_t)c + 1].k - t0;
+        const int32_t nt = (int32_t)std::max<int64_t>(1, (span + kTileItems - 1) / kTileItems);
+        off[(size_t)c + 1] = off[(size_t)c] + nt;
     }
-    cd[(size_t)nch] = bs[(size_t)nch].d;
     const int32_t slots = off[(size_t)nch];
     if ((rc = g->tile_coord.alloc((size_t)slots * sizeof(int2)))) return rc;
-    int64_t* d_cd = nullptr;
+    int4* d_rk = nullptr;
     int32_t* d_off = nullptr;
-    if ((rc = cuda_ok(cudaMallocAsync(&d_cd, cd.size() * sizeof(int64_t), s), "cudaMallocAsync")) ||
+    if ((rc = cuda_ok(cudaMallocAsync(&d_rk, rk.size() * sizeof(int4), s), "cudaMallocAsync")) ||
         (rc = cuda_ok(cudaMallocAsync(&d_off, off.size() * sizeof(int32_t), s), "cudaMallocAsync")))
         return rc;
-    cudaMemcpyAsync(d_cd, cd.data(), cd.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_rk, rk.data(), rk.size() * sizeof(int4), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
-    k_tile_coords<<<grid_for(nch), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, nnz, d_cd, d_off, nch,
+    k_tile_coords<<<grid_for(nch), kThreads, 0, s>>>(g->in_row.as<int32_t>(), d_rk, d_off, nch,
                                                       g->tile_coord.as<int2>());
-    cudaFreeAsync(d_cd, s);
+    cudaFreeAsync(d_rk, s);
     cudaFreeAsync(d_off, s);
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "sweep tiles"))) return rc;
     // Chunk table (local ids), spans and groups.
@@ -470,7 +518,11 @@ int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s) {
         const B& a = bs[(size_t)c];
         const B& b = bs[(size_t)c + 1];
         k.sub_begin = off[(size_t)c];
-        k.sub_end = off[(size_t)c + 1] - 1;
+        k.sub_end = off[(size_t)c + 1];
+        k.nnz_begin = a.k;
+        k.nnz_end = b.k;
+        k.row_end = b.r;
+        k.pad = 0;
         k.graph = 0;
         const bool head = a.k > a.rs;
         const bool tail = b.r < n && b.k > b.rs;
@@ -497,7 +549,7 @@ int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s) {
     g->plan.h_groups.clear();
     for (int32_t c = 0; c < nch; c += kGroupChunks)
         g->plan.h_groups.push_back(Group{c, std::min(nch, c + kGroupChunks), 0, 0});
-    g->ntiles = slots - nch;
+    g->ntiles = slots;
     return EGPR_SUCC;
 }
 
@@ -564,6 +616,10 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         uint32_t* vals2 = tmp.get<uint32_t>((size_t)m, &rc);
         int32_t* src = tmp.get<int32_t>((size_t)m, &rc);
         unsigned long long* counts = tmp.get<unsigned long long>(2, &rc);
+        uint32_t* hkey = tmp.get<uint32_t>((size_t)n, &rc);
+        uint32_t* hval = tmp.get<uint32_t>((size_t)n, &rc);
+        uint32_t* hkey2 = tmp.get<uint32_t>((size_t)n, &rc);
+        uint32_t* hval2 = tmp.get<uint32_t>((size_t)n, &rc);
         if (rc) return rc;
         if ((rc = g->in_row.alloc(((size_t)n + 1) * sizeof(int32_t))) ||
             (rc = g->outw.alloc((size_t)n * sizeof(double))) ||
@@ -577,7 +633,7 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             return rc;
         cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * sizeof(uint32_t), s);
         cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s);
-        k_out_weight<<<grid_for(n), kThreads, 0, s>>>(dV, dE, dW, n, g->outw.as<double>());
+        k_out_weight<<<grid_for(n), kThreads, 0, s>>>(dV, dE, dW, n, g->outw.as<double>(), hkey, hval);
         if (m > 0) k_in_degree_keys<<<grid_for(m), kThreads, 0, s>>>(dE, m, n, indeg, keys, vals);
         if ((rc = exclusive_scan_u32(indeg, reinterpret_cast<uint32_t*>(g->in_row.as<int32_t>()), (int64_t)n + 1, s)))
             return rc;
@@ -587,9 +643,11 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             return rc;
         g->nnz = nnz32;
         const int64_t nnz = g->nnz;
-        if ((rc = g->in_col.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(int32_t) + 64)))
+        // Padding: a warp tile reads whole 8-entry groups up to kTileItems past the end.
+        const size_t pad = (size_t)(kTileItems + 16) * sizeof(int32_t);
+        if ((rc = g->in_col.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(int32_t) + pad)))
             return rc;
-        if (W && (rc = g->in_w.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(float) + 64)))
+        if (W && (rc = g->in_w.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(float) + pad)))
             return rc;
         if (m > 0) {
             int bits = 0;
@@ -601,6 +659,22 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             if (nnz > 0)
                 k_gather_inbound<<<grid_for(nnz), kThreads, 0, s>>>(sorted_ids, nnz, src, dW, g->in_col.as<int32_t>(),
                                                                    W ? g->in_w.as<float>() : nullptr);
+        }
+        // Hubs: the min(n, kHubCap) sources of largest out-degree (a multiple of 4,
+        // the granule of the shared-memory staging copy).
+        const char* hub_env = std::getenv("EGPR_HUBS");  // EGPR_HUBS=0: no hub cache
+        g->nhub = (hub_env && hub_env[0] == '0') ? 0 : (std::min<int32_t>(n, kHubCap) & ~3);
+        if ((rc = g->hub_slot.alloc((size_t)n * sizeof(int32_t))) ||
+            (rc = g->hub_ids.alloc((size_t)std::max(g->nhub, 4) * sizeof(int32_t))) ||
+            (rc = cuda_ok(cudaMemsetAsync(g->hub_slot.p, 0xff, (size_t)n * sizeof(int32_t), s), "memset")))
+            return rc;
+        if (g->nhub > 0) {
+            bool alt = false;
+            if ((rc = radix_sort_pairs(hkey, hval, hkey2, hval2, n, 32, s, tmp, &alt))) return rc;
+            k_hub_slots<<<grid_for(g->nhub), kThreads, 0, s>>>(alt ? hval2 : hval, g->nhub, g->hub_ids.as<int32_t>(),
+                                                               g->hub_slot.as<int32_t>());
+            if (nnz > 0)
+                k_encode_hubs<<<grid_for(nnz), kThreads, 0, s>>>(g->in_col.as<int32_t>(), nnz, g->hub_slot.as<int32_t>());
         }
         k_dangling<<<grid_for(n), kThreads, 0, s>>>(g->outw.as<double>(), n, g->dangling01.as<int32_t>(), counts);
         unsigned long long hc[2] = {0, 0};
@@ -629,6 +703,19 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
     g->prep_seconds = ms * 1e-3;
     (void)t0;
     return EGPR_SUCC;
+}
+
+// Copies in_col to the host with hub entries decoded back to source ids.
+int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s) {
+    if (g->nnz <= 0) return EGPR_SUCC;
+    int32_t* tmp = nullptr;
+    int rc = cuda_ok(cudaMallocAsync(&tmp, (size_t)g->nnz * sizeof(int32_t), s), "cudaMallocAsync (export)");
+    if (rc) return rc;
+    k_decode_hubs<<<grid_for(g->nnz), kThreads, 0, s>>>(g->in_col.as<int32_t>(), g->nnz, g->hub_ids.as<int32_t>(),
+                                                        tmp);
+    rc = cuda_ok(cudaMemcpyAsync(host, tmp, (size_t)g->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H in_col");
+    cudaFreeAsync(tmp, s);
+    return rc;
 }
 
 }  // namespace egpr

@@ -59,7 +59,8 @@ struct SpmmParams {
     int32_t n;
     int32_t max_iter;
     const int32_t* in_row;
-    const int32_t* in_col;
+    const int32_t* in_col;   // hub entries store -(slot + 1)
+    const int32_t* hub_ids;
     const float* in_w;
     const int2* sub_coord;
     const double* outw;
@@ -258,7 +259,8 @@ __device__ void process_unit(const SpmmParams& P, int32_t p, int32_t c, SpmmSmem
         const int32_t nnz_sub = b.y - a.y;
         const int32_t nrows = b.x - a.x;
         for (int32_t i = tid; i < nnz_sub; i += kThreads) {
-            const int32_t u = P.in_col[ka + i];
+            const int32_t cu = P.in_col[ka + i];
+            const int32_t u = cu >= 0 ? cu : P.hub_ids[-cu - 1];  // hub entries store -(slot + 1)
             S.col[i] = u;
             S.w[i] = P.in_w ? P.in_w[ka + i] : 1.0f;
             if constexpr (kFinal) S.outw[i] = P.outw[u];
@@ -660,6 +662,7 @@ int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, i
     P.max_iter = max_iter;
     P.in_row = g->in_row.as<int32_t>();
     P.in_col = g->in_col.as<int32_t>();
+    P.hub_ids = g->hub_ids.as<int32_t>();
     P.in_w = g->weighted ? g->in_w.as<float>() : nullptr;
     P.sub_coord = g->sub_coord.as<int2>();
     P.outw = g->outw.as<double>();

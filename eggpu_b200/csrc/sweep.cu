@@ -16,19 +16,28 @@
 // Sdot, two memsets, add_base_and_reduce, scale_vec and the two host round
 // trips (gpu_easygraph/functions/centrality/pagerank.cu:591-664).
 //
-// Work split (merge path, one warp per tile): the items of a graph's merge
-// path (one per row end, one per inbound entry) are cut into chunks of whole
-// rows, and chunks into warp tiles of kTileItems items.  Every warp is an
-// independent worker: it pulls chunks from a queue and, per tile, stages the
-// entries' products in its own shared memory with coalesced loads, lets each
-// lane walk kLaneItems consecutive items, joins rows split between lanes with
-// a shuffle segmented scan, and finishes the tile's rows with coalesced
-// stores.  No block-wide barrier exists, so the SM always has independent
-// warps to issue from.  Only rows longer than a chunk are cut between chunks;
-// the last chunk of such a row to finish combines its pieces in chunk order.
-// FP64 partial sums are reduced in a fixed order through groups of chunks and
-// then per graph, so every result is deterministic.  Nothing waits on another
-// warp.
+// Work split.  A graph's rows are cut into chunks of whole rows (only rows
+// longer than a chunk are cut, into "spans"), chunks into warp tiles of
+// kTileItems inbound entries starting on 8-entry boundaries.  One persistent
+// CTA of 32 independent warps runs per SM; warps pull chunks from a queue.
+// Per tile a warp
+//   1. loads its 256 entries' sources with two 16-byte loads per lane (lane l
+//      owns entries 8l..8l+7) and gathers their carried values: sources among
+//      the graph's hubs (the kHubCap largest out-degrees, encoded as -(slot+1))
+//      read the CTA's shared-memory copy of the hub values, staged once per
+//      launch by a TMA bulk copy; the rest read z from L2/HBM;
+//   2. marks the last entry of every row finished in the tile in a 256-bit
+//      mask (row ends come from in_row) and lists those rows in order; rows
+//      without entries are finished on the spot;
+//   3. sums each lane's 8 products segment by segment and joins rows that
+//      cross lanes with one shuffle segmented scan; a row still open at the
+//      tile's end carries into the next tile;
+//   4. finishes the listed rows (coalesced).
+// Rows cut between chunks are finished by whichever chunk arrives last, adding
+// the pieces in chunk order.  FP64 partial sums are reduced in a fixed order
+// through groups of chunks and then per graph, so every result is
+// deterministic.  Nothing waits on another warp; the only wait is on the TMA
+// copy, and it is bounded.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,16 +49,16 @@
 namespace egpr {
 namespace {
 
-constexpr int kCtaWarps = 4;                 // independent warps per CTA
+constexpr int kCtaWarps = 32;                 // independent warps per CTA, one CTA per SM
 constexpr int kCtaThreads = 32 * kCtaWarps;
-constexpr int kRowPre = 1;                   // row-data loads issued with the gathers (x 32 rows)
-constexpr int kMinCtasPerSm = 8;             // 32 warps per SM: registers capped at 64
 constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kCopyPiece = 32768;        // bytes per bulk copy instruction
+constexpr long long kWaitLimit = 1ll << 26;   // bounded wait on the hub staging copy
 
 template <typename Real>
-struct WarpSmem {
-    Real prod[kTileItems];
-    int32_t rowend[kTileItems + 1];
+struct WarpScratch {
+    uint32_t flags[kTileItems / 32];
+    int32_t list[kTileItems];
     Real rowval[kTileItems];
 };
 
@@ -62,49 +71,47 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;  // valid in lane 0
 }
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
 // Per-chunk view of one graph.
 struct SweepView {
     const float* xin;     // previous ranks
     const float* zsrc32;  // carried values (FP32 sweep)
     float* xout;
     float* zout;
+    const float* hub_in;  // hub values read by this sweep (global copy)
+    float* hub_out;       // hub values written for the next sweep
     double jump;          // (1-alpha)/n + dangling term (uniform teleport)
     double dmass;         // dangling term alone (personalised teleport)
     double one_minus_alpha;
     int32_t personalised;
 };
 
-// Row data the epilogue needs, loaded ahead of time.
-struct RowPre {
-    float xin;
-    float scale;
-    float tele;
-};
-
-__device__ __forceinline__ void load_row(const GraphDev& G, const SweepView& W, int32_t v, RowPre& p) {
-    p.xin = W.xin[v];
-    p.scale = G.scale[v];
-    p.tele = W.personalised ? G.tele[v] : 0.f;
-}
-
 // Finishes row v given its gathered sum; accumulates residual / dangling /
-// rank sums.  FP32 sweep: writes x_new and z_new; the residual compares the
-// stored FP32 iterates, so the loop can stop once they no longer change even
-// when tol*n is below FP32 resolution.  FP64 correction sweep: writes the FP64
-// result.
+// rank sums.  FP32 sweep: writes x_new, z_new (and the hub copy of z_new); the
+// residual compares the stored FP32 iterates, so the loop can stop once they no
+// longer change even when tol*n is below FP32 resolution.  FP64 correction
+// sweep: writes the FP64 result.
 template <typename Real>
 __device__ __forceinline__ void finish_row(const GraphDev& G, const SweepView& W, int32_t v, double acc,
-                                           const RowPre& p, double& err, double& dsum, double& xsum) {
+                                           double& err, double& dsum, double& xsum) {
+    const float xin = W.xin[v];
+    const float scale = G.scale[v];
     double val;
-    if (W.personalised) val = (acc + W.one_minus_alpha * (double)p.tele) + W.dmass;
+    if (W.personalised) val = (acc + W.one_minus_alpha * (double)G.tele[v]) + W.dmass;
     else val = acc + W.jump;
-    const double prev = (double)p.xin;
+    const double prev = (double)xin;
     if constexpr (std::is_same<Real, float>::value) {
         const float xo = (float)val;
         err += fabs((double)xo - prev);
         W.xout[v] = xo;
-        W.zout[v] = p.scale >= 0.f ? xo * p.scale : 0.f;
-        if (p.scale < 0.f) dsum += (double)xo;
+        const float zo = scale >= 0.f ? xo * scale : 0.f;
+        W.zout[v] = zo;
+        const int32_t hs = G.hub_slot[v];
+        if (hs >= 0) W.hub_out[hs] = zo;
+        if (scale < 0.f) dsum += (double)xo;
         xsum += (double)xo;
     } else {
         err += fabs(val - prev);
@@ -127,10 +134,8 @@ __device__ void span_arrive(const SweepParams& P, const GraphDev& G, const Sweep
     for (int32_t q = ta + 1; q < tb; ++q) sum += ldcg(&P.piece[2 * q + 1]);
     sum += ldcg(&P.piece[2 * tb]);
     P.span_cnt[ta] = 0u;
-    RowPre rp;
-    load_row(G, W, cta.tail_row, rp);
     double e = 0.0, d = 0.0, x = 0.0;
-    finish_row<Real>(G, W, cta.tail_row, sum, rp, e, d, x);
+    finish_row<Real>(G, W, cta.tail_row, sum, e, d, x);
     P.span_part[3 * ta] = e;
     P.span_part[3 * ta + 1] = d;
     P.span_part[3 * ta + 2] = x;
@@ -244,9 +249,10 @@ __device__ void chunk_finish(const SweepParams& P, int32_t c, const Chunk& ck, c
 }
 
 template <typename Real>
-__device__ void process_chunk(const SweepParams& P, int32_t c, WarpSmem<Real>& S) {
+__device__ void process_chunk(const SweepParams& P, int32_t c, WarpScratch<Real>& S, const float* hub_smem) {
     constexpr bool kFinal = std::is_same<Real, double>::value;
     const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
     const Chunk ck = P.chunks[c];
     const GraphDev& G = P.graphs[ck.graph];
     GraphState* st = P.states + ck.graph;
@@ -263,6 +269,8 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, WarpSmem<Real>& S
         W.zsrc32 = G.z[par];
         W.xout = G.x[par ^ 1];
         W.zout = G.z[par ^ 1];
+        W.hub_in = G.hubz[par];
+        W.hub_out = G.hubz[par ^ 1];
         W.dmass = ldcg(&st->dmass);
     } else {
         const int par = (iter - 1) & 1;  // x_{k-1}: the input of the last sweep
@@ -270,151 +278,199 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, WarpSmem<Real>& S
         W.zsrc32 = nullptr;
         W.xout = nullptr;
         W.zout = nullptr;
+        W.hub_in = nullptr;
+        W.hub_out = nullptr;
         W.dmass = ldcg(&st->dmass_prev);
     }
     W.jump = st->c1 + W.dmass;
-    const Real* __restrict__ gsrc;
-    if constexpr (kFinal) gsrc = G.z64;
-    else gsrc = W.zsrc32;
+    const float* __restrict__ hub = hub_smem ? hub_smem : W.hub_in;
     const int32_t* __restrict__ in_row = G.in_row;
-    const int32_t* __restrict__ in_col = G.in_col;
-    const float* __restrict__ in_w = G.in_w;
+    const int4* __restrict__ col4 = reinterpret_cast<const int4*>(G.in_col);
+    const float4* __restrict__ w4 = reinterpret_cast<const float4*>(G.in_w);
     const int2* __restrict__ coord = G.sub_coord;
 
     double err = 0.0, dsum = 0.0, xsum = 0.0;
-    Real carry = Real(0);  // partial of the row in progress from the previous tile
+    Real carry = Real(0);  // partial of the row still open at the end of the previous tile
     Real head_val = Real(0);
     bool head_pending = (ck.flags & kHasHead) != 0;
 
-    // Software pipeline: tile t+1's indices load while tile t is reduced.
-    int2 a = coord[ck.sub_begin];
-    int2 b = coord[ck.sub_begin + 1];
-    int32_t col[kLaneItems];
+    int2 tc = coord[ck.sub_begin];
+    int4 ca = __ldcs(col4 + (tc.x >> 2) + 2 * lane);
+    int4 cb = __ldcs(col4 + (tc.x >> 2) + 2 * lane + 1);
+    for (int32_t t = ck.sub_begin; t < ck.sub_end; ++t) {
+        const int32_t T = tc.x, fa = tc.y;
+        const bool has_next = t + 1 < ck.sub_end;
+        const int2 tn = has_next ? coord[t + 1] : make_int2(T, ck.row_end);
+        const int32_t fb = tn.y;
+        const int32_t lo = max(T, ck.nnz_begin), hi = min(T + kTileItems, ck.nnz_end);
+        // 1. gathers of this tile's entries
+        const int32_t cc[kLaneItems] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+        const int32_t p0 = T + kLaneItems * lane;
+        Real v[kLaneItems];
 #pragma unroll
-    for (int u = 0; u < kLaneItems; ++u) {
-        const int32_t i = lane + 32 * u;
-        col[u] = i < b.y - a.y ? __ldcs(in_col + a.y + i) : -1;
-    }
-    for (int32_t sidx = ck.sub_begin; sidx < ck.sub_end; ++sidx) {
-        const int32_t ra = a.x, ka = a.y;
-        const int32_t nnz_sub = b.y - a.y;
-        const int32_t nrows = b.x - a.x;
-        const bool has_next = sidx + 1 < ck.sub_end;
-        const int2 bn = has_next ? coord[sidx + 2] : b;
-        // Phase 1: gathers of this tile, next tile's indices, row data.
-        Real val[kLaneItems];
-#pragma unroll
-        for (int u = 0; u < kLaneItems; ++u) val[u] = col[u] >= 0 ? gsrc[col[u]] : Real(0);
-        if (in_w) {
-#pragma unroll
-            for (int u = 0; u < kLaneItems; ++u) {
-                const int32_t i = lane + 32 * u;
-                if (i < nnz_sub) val[u] *= (Real)__ldcs(in_w + ka + i);
+        for (int u = 0; u < kLaneItems; ++u) {
+            const int32_t p = p0 + u;
+            const int32_t cu = cc[u];
+            Real x = Real(0);
+            if (p >= lo && p < hi) {
+                if constexpr (kFinal) x = G.z64[cu >= 0 ? cu : G.hub_ids[-cu - 1]];
+                else x = cu >= 0 ? W.zsrc32[cu] : hub[-cu - 1];
             }
+            v[u] = x;
         }
-        const int32_t nnz_next = bn.y - b.y;
+        if (w4) {
+            const float4 wa = __ldcs(w4 + (T >> 2) + 2 * lane);
+            const float4 wb = __ldcs(w4 + (T >> 2) + 2 * lane + 1);
+            const float ww[kLaneItems] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
 #pragma unroll
-        for (int u = 0; u < kLaneItems; ++u) {
-            const int32_t i = lane + 32 * u;
-            col[u] = (has_next && i < nnz_next) ? __ldcs(in_col + b.y + i) : -1;
+            for (int u = 0; u < kLaneItems; ++u) v[u] *= (Real)ww[u];
         }
-        RowPre pre[kRowPre];
-#pragma unroll
-        for (int q = 0; q < kRowPre; ++q) {
-            const int32_t r = lane + 32 * q;
-            if (r < nrows) load_row(G, W, ra + r, pre[q]);
+        if (has_next) {
+            ca = __ldcs(col4 + (tn.x >> 2) + 2 * lane);
+            cb = __ldcs(col4 + (tn.x >> 2) + 2 * lane + 1);
         }
-        for (int32_t i = lane; i < nrows; i += 32) S.rowend[i] = in_row[ra + i + 1] - ka;
-#pragma unroll
-        for (int u = 0; u < kLaneItems; ++u) {
-            const int32_t i = lane + 32 * u;
-            if (i < nnz_sub) S.prod[i] = val[u];
+        // 2. rows finished in this tile: end marks for rows with entries, the
+        //    rest finished on the spot
+        if (lane < kTileItems / 32) S.flags[lane] = 0u;
+        __syncwarp();
+        int32_t nlist = 0;
+        for (int32_t r0 = fa; r0 < fb; r0 += 32) {
+            const int32_t r = r0 + lane;
+            const bool in = r < fb;
+            const int32_t s = in ? in_row[r] : 0;
+            int32_t e = __shfl_down_sync(kFull, s, 1);
+            if (lane == 31 && in) e = in_row[r + 1];
+            if (in && r + 1 == fb && lane != 31) e = in_row[r + 1];
+            const bool ne = in && e > s;
+            const unsigned bal = __ballot_sync(kFull, ne);
+            if (ne) {
+                S.list[nlist + __popc(bal & lt_mask)] = r;
+                const int32_t bit = e - 1 - T;  // in [0, kTileItems) by construction of the tiles
+                if ((unsigned)bit < (unsigned)kTileItems) atomicOr(&S.flags[bit >> 5], 1u << (bit & 31));
+            } else if (in) {
+                finish_row<Real>(G, W, r, 0.0, err, dsum, xsum);
+            }
+            nlist += __popc(bal);
         }
         __syncwarp();
-        // Phase 2: each lane walks kLaneItems consecutive items of the merge path.
-        const int32_t total = nrows + nnz_sub;
-        const int32_t diag = min(lane * kLaneItems, total);
-        const int32_t dend = min(diag + kLaneItems, total);
-        int32_t lo = max(diag - nnz_sub, 0), hi = min(diag, nrows);
-        while (lo < hi) {
-            const int32_t mid = (lo + hi) >> 1;
-            if (S.rowend[mid] <= diag - mid - 1) lo = mid + 1;
-            else hi = mid;
-        }
-        int32_t i = lo, j = diag - lo;
-        Real acc = Real(0);
-        int32_t first = -1;
-        for (int32_t d = diag; d < dend; ++d) {
-            if (i < nrows && j >= S.rowend[i]) {
-                S.rowval[i] = acc;
-                if (first < 0) first = i;
+        // 3. per-lane segmented sums, then lanes joined by a segmented scan
+        const uint32_t fw = S.flags[lane >> 2];
+        const int sh = (lane & 3) * 8;
+        const uint32_t mybits = (fw >> sh) & 0xffu;
+        int32_t k = __popc(fw & ((1u << sh) - 1u));
+        for (int w = 0; w < (lane >> 2); ++w) k += __popc(S.flags[w]);
+        Real acc = Real(0), head_part = Real(0);
+        int32_t first_close = -1;
+#pragma unroll
+        for (int u = 0; u < kLaneItems; ++u) {
+            acc += v[u];
+            if ((mybits >> u) & 1u) {
+                if (first_close < 0) {
+                    first_close = k;
+                    head_part = acc;
+                } else {
+                    S.rowval[k] = acc;
+                }
                 acc = Real(0);
-                ++i;
-            } else {
-                acc += S.prod[j];
-                ++j;
+                ++k;
             }
         }
-        // Phase 2b: segmented inclusive scan of the lanes' carries keyed by the
-        // row they stopped in (rows never decrease across lanes).  The carry
-        // from the previous tile belongs to local row 0: it joins lane 0's carry,
-        // or lane 0's first row if lane 0 completed row 0.
+        bool f = first_close >= 0;
         Real seg = acc;
-        if (lane == 0 && first != 0) seg += carry;
+        if (lane == 0 && !f) seg += carry;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const Real up = __shfl_up_sync(kFull, seg, o);
-            const int32_t rup = __shfl_up_sync(kFull, i, o);
-            if (lane >= o && rup == i) seg += up;
-        }
-        const Real prev_seg = __shfl_up_sync(kFull, seg, 1);
-        const int32_t prev_row = __shfl_up_sync(kFull, i, 1);
-        if (first >= 0) {
-            Real v = S.rowval[first];
-            if (lane == 0) v += carry;  // first == 0 here: lane 0 starts in row 0
-            else if (prev_row == first) v += prev_seg;
-            S.rowval[first] = v;
-        }
-        carry = __shfl_sync(kFull, seg, 31);  // lane 31 always stops in row nrows
-        __syncwarp();
-        // Phase 3: finish the rows that ended in this tile (coalesced).
-#pragma unroll
-        for (int q = 0; q < kRowPre; ++q) {
-            const int32_t r = lane + 32 * q;
-            if (r < nrows) {
-                const Real racc = S.rowval[r];
-                if (r == 0 && head_pending) head_val = racc;  // finished through its span
-                else finish_row<Real>(G, W, ra + r, (double)racc, pre[q], err, dsum, xsum);
+            const bool fup = __shfl_up_sync(kFull, (int)f, o) != 0;
+            if (lane >= o) {
+                if (!f) seg += up;
+                f = f || fup;
             }
         }
-        for (int32_t r = lane + 32 * kRowPre; r < nrows; r += 32) {
-            RowPre rp;
-            load_row(G, W, ra + r, rp);
-            finish_row<Real>(G, W, ra + r, (double)S.rowval[r], rp, err, dsum, xsum);
-        }
-        head_val = __shfl_sync(kFull, head_val, 0);
-        if (nrows > 0) head_pending = false;
+        const Real prev_seg = __shfl_up_sync(kFull, seg, 1);
+        if (first_close >= 0) S.rowval[first_close] = head_part + (lane == 0 ? carry : prev_seg);
+        carry = __shfl_sync(kFull, seg, 31);
         __syncwarp();
-        a = b;
-        b = bn;
+        // 4. finish the listed rows; the chunk's head row (cut before the chunk)
+        //    is the chunk's first listed row and becomes its span piece instead
+        int32_t jstart = 0;
+        if (head_pending && nlist > 0) {
+            head_val = S.rowval[0];
+            head_pending = false;
+            jstart = 1;
+        }
+        for (int32_t j = jstart + lane; j < nlist; j += 32)
+            finish_row<Real>(G, W, S.list[j], (double)S.rowval[j], err, dsum, xsum);
+        __syncwarp();
+        tc = tn;
     }
     chunk_finish<Real>(P, c, ck, G, W, st, err, dsum, xsum, (double)head_val, (double)carry);
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_sweep(SweepParams P) {
-    __shared__ WarpSmem<Real> smem[kCtaWarps];
+__global__ void __launch_bounds__(kCtaThreads, 1) k_sweep(SweepParams P) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ int32_t s_abort;
+    __shared__ int32_t s_idle;
     constexpr bool kFinal = std::is_same<Real, double>::value;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpSmem<Real>& S = smem[warp];
-    const bool idle = !kFinal && ldcg(&P.ctl->active) <= 0;
+    const bool stage = !kFinal && P.hub_smem;
+    const float* hub_smem = stage ? reinterpret_cast<const float*>(smem) : nullptr;
+    const size_t hub_bytes = stage ? (size_t)kHubCap * sizeof(float) : 0;
+    WarpScratch<Real>& S = reinterpret_cast<WarpScratch<Real>*>(smem + hub_bytes)[warp];
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        s_idle = (!kFinal && ldcg(&P.ctl->active) <= 0) ? 1 : 0;  // one reading for the whole CTA
+    }
+    __syncthreads();
+    bool idle = s_idle != 0;
+    if (stage && !idle) {
+        // Stage graph 0's hub values for this launch's parity.  A CTA that reads
+        // the next parity can only do so after every chunk was taken, so it gets
+        // no work.
+        const GraphDev& G = P.graphs[0];
+        const uint32_t bytes = (uint32_t)G.nhub * (uint32_t)sizeof(float);
+        if (threadIdx.x == 0 && bytes > 0) {
+            const float* src = G.hubz[ldcg(&P.states[0].iter) & 1];
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(bytes)
+                         : "memory");
+            for (uint32_t off = 0; off < bytes; off += kCopyPiece) {
+                const uint32_t piece = min(kCopyPiece, bytes - off);
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        smem_u32(smem + off)),
+                    "l"(reinterpret_cast<const unsigned char*>(src) + off), "r"(piece), "r"(smem_u32(&mbar))
+                    : "memory");
+            }
+        }
+        __syncthreads();
+        if (bytes > 0) {
+            uint32_t ok = 0;
+            for (long long i = 0; i < kWaitLimit && !ok; ++i) {
+                asm volatile(
+                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+                    : "=r"(ok)
+                    : "r"(smem_u32(&mbar))
+                    : "memory");
+            }
+            if (!ok) atomicExch(&s_abort, 1);
+        }
+        __syncthreads();
+        if (s_abort) {
+            if (threadIdx.x == 0) atomicExch(&P.ctl->error, EGPR_TIMEOUT);
+            idle = true;
+        }
+    }
     if (!idle) {
         for (;;) {
             int32_t c = 0;
             if (lane == 0) c = (int32_t)atomicAdd(&P.ctl->queue, 1u);
             c = __shfl_sync(kFull, c, 0);
             if (c >= P.nchunks) break;
-            process_chunk<Real>(P, c, S);
+            process_chunk<Real>(P, c, S, hub_smem);
         }
     }
     if (lane == 0) {
@@ -428,7 +484,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_sweep(SweepParam
                 const int32_t launches = P.ctl->launches + 1;
                 P.ctl->launches = launches;
                 const int32_t active = ldcg(&P.ctl->active);
-                const bool more = active > 0 && launches < P.ctl->cap;
+                const bool more = active > 0 && launches < P.ctl->cap && P.ctl->error == 0;
                 if (active > 0 && launches >= P.ctl->cap) P.ctl->error = EGPR_TIMEOUT;
                 if (P.use_cond) cudaGraphSetConditional(P.cond, more ? 1u : 0u);
             }
@@ -440,7 +496,7 @@ __global__ void __launch_bounds__(kCtaThreads, kMinCtasPerSm) k_sweep(SweepParam
 // ---- per-solve set-up and finishing kernels --------------------------------
 
 // scale = alpha / outw (FP32), -1 marks a dangling vertex (outw <= 1e-15,
-// pagerank.py:118); x0 = 1/n; z0 = x0 * scale.
+// pagerank.py:118); x0 = 1/n; z0 = x0 * scale; hub copy of z0.
 __global__ void k_init_vertices(const GraphDev* graphs, int32_t count, double alpha) {
     const int32_t gi = blockIdx.y;
     if (gi >= count) return;
@@ -453,7 +509,10 @@ __global__ void k_init_vertices(const GraphDev* graphs, int32_t count, double al
         const float sc = o <= 1e-15 ? -1.f : (float)(alpha / o);
         scale[v] = sc;
         G.x[0][v] = x0;
-        G.z[0][v] = sc >= 0.f ? x0 * sc : 0.f;
+        const float z = sc >= 0.f ? x0 * sc : 0.f;
+        G.z[0][v] = z;
+        const int32_t hs = G.hub_slot[v];
+        if (hs >= 0) G.hubz[0][hs] = z;
     }
 }
 
@@ -532,6 +591,11 @@ int g_cta_cache[2][64] = {};
 
 int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SUCC : set_cuda_error(e, what); }
 
+size_t sweep_smem_bytes(int mode, bool hub) {
+    if (mode == 0) return (hub ? (size_t)kHubCap * sizeof(float) : 0) + kCtaWarps * sizeof(WarpScratch<float>);
+    return kCtaWarps * sizeof(WarpScratch<double>);
+}
+
 SweepParams make_params(Plan& plan, int mode, int use_cond) {
     SweepParams P;
     P.chunks = plan.d_chunks.as<Chunk>();
@@ -551,6 +615,7 @@ SweepParams make_params(Plan& plan, int mode, int use_cond) {
     P.cond = plan.cond;
     P.use_cond = use_cond;
     P.total_warps = (mode ? plan.grid_final : plan.grid) * kCtaWarps;
+    P.hub_smem = (mode == 0 && plan.ngraphs == 1) ? 1 : 0;
     return P;
 }
 
@@ -579,7 +644,8 @@ cudaLaunchAttributeValue l2_window(const Plan& plan) {
     return v;
 }
 
-// Resident CTAs of a sweep kernel on the current device.
+// Resident CTAs of a sweep kernel on the current device (dynamic shared memory
+// sized for the hub cache).
 int sweep_ctas(int mode) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -588,10 +654,17 @@ int sweep_ctas(int mode) {
     if (cached > 0) return cached;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (mode == 0)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<float>, kCtaThreads, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<double>, kCtaThreads, 0);
+    if (mode == 0) {
+        cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sweep_smem_bytes(0, true));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<float>, kCtaThreads, sweep_smem_bytes(0, true));
+    } else {
+        cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sweep_smem_bytes(1, false));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<double>, kCtaThreads,
+                                                      sweep_smem_bytes(1, false));
+    }
+    cudaGetLastError();
     if (per_sm < 1) per_sm = 1;
     cached = sms * per_sm;
     return cached;
@@ -656,11 +729,15 @@ GraphDev graph_dev_view(const egpr_graph* g) {
     d.z[1] = g->z0.as<float>() + g->n;  // one allocation: both buffers under one L2 window
     d.out = g->out.as<double>();
     d.z64 = g->z64.as<double>();
+    d.hub_ids = g->hub_ids.as<int32_t>();
+    d.hub_slot = g->hub_slot.as<int32_t>();
+    d.hubz[0] = g->hubz.as<float>();
+    d.hubz[1] = g->hubz.as<float>() + std::max(g->nhub, 4);
+    d.nhub = g->nhub;
     d.n = g->n;
     d.chunk_begin = d.chunk_end = 0;
     d.group_begin = d.group_end = 0;
     d.span_begin = d.span_end = 0;
-    d.pad = 0;
     return d;
 }
 
@@ -762,7 +839,7 @@ int plan_capture_loop(Plan& plan, cudaStream_t stream) {
     kp.func = (void*)k_sweep<float>;
     kp.gridDim = dim3((unsigned)plan.grid);
     kp.blockDim = dim3(kCtaThreads);
-    kp.sharedMemBytes = 0;
+    kp.sharedMemBytes = (unsigned)sweep_smem_bytes(0, P.hub_smem != 0);
     kp.kernelParams = args;
     e = cudaGraphAddKernelNode(&knode, cp.conditional.phGraph_out[0], nullptr, 0, &kp);
     if (e != cudaSuccess) goto fail;
@@ -808,6 +885,7 @@ int launch_loop(Plan& plan, int32_t max_iter, cudaStream_t stream, int32_t* laun
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)plan.grid);
     cfg.blockDim = dim3(kCtaThreads);
+    cfg.dynamicSmemBytes = sweep_smem_bytes(0, P.hub_smem != 0);
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     if (plan.l2_bytes > 0) {
@@ -832,7 +910,7 @@ int launch_finish(Plan& plan, bool correction, cudaStream_t stream, int32_t* lau
                                                   plan.ngraphs);
         // The loop's last warp left the queue reset; the control block keeps the sweep count.
         SweepParams P = make_params(plan, 1, 0);
-        k_sweep<double><<<plan.grid_final, kCtaThreads, 0, stream>>>(P);
+        k_sweep<double><<<plan.grid_final, kCtaThreads, sweep_smem_bytes(1, false), stream>>>(P);
         l += 2;
     }
     k_normalize<<<grid, kThreads, 0, stream>>>(plan.d_graphs.as<GraphDev>(), plan.d_states.as<GraphState>(),
