@@ -82,16 +82,11 @@ void Plan::release() {
     d_graphs.release();
     d_states.release();
     d_ndang.release();
-    d_chunk_part.release();
-    d_piece.release();
-    d_span_cnt.release();
-    d_span_part.release();
     d_ctl.release();
-    d_groups.release();
-    d_group_cnt.release();
-    d_group_part.release();
+    d_acc.release();
+    d_span_acc.release();
     d_span_list.release();
-    ngraphs = nchunks = grid = grid_final = max_n = ngroups = 0;
+    ngraphs = nchunks = grid = any_weighted = max_n = nspans = nacc = 0;
 }
 
 int check_device(const egpr_graph* g) {
@@ -305,12 +300,10 @@ static uint64_t bits_of(double x) {
 
 int64_t egpr_graph::device_bytes() const {
     return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes + sub_coord.bytes +
-                     tile_coord.bytes + hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_groups.bytes +
-                     plan.d_group_cnt.bytes + plan.d_group_part.bytes +
+                     hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_acc.bytes + plan.d_span_acc.bytes +
                      plan.d_span_list.bytes +
                      scale.bytes + tele.bytes + x0.bytes + x1.bytes + z0.bytes + z1.bytes + out.bytes + z64.bytes +
                      plan.d_chunks.bytes + plan.d_graphs.bytes + plan.d_states.bytes + plan.d_ndang.bytes +
-                     plan.d_chunk_part.bytes + plan.d_piece.bytes + plan.d_span_cnt.bytes + plan.d_span_part.bytes +
                      plan.d_ctl.bytes);
 }
 
@@ -325,7 +318,7 @@ static void destroy_graph_object(egpr_graph* g) {
     if (g->own_stream) cudaStreamSynchronize(g->own_stream);
     spmm_work_release(g);
     g->plan.release();
-    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord, &g->tile_coord,
+    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord,
                       &g->hub_ids, &g->hub_slot, &g->hubz, &g->scale, &g->tele,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})
         b->release();
@@ -388,7 +381,8 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
         destroy_graph_object(g);
         return rc;
     }
-    const size_t nf = (size_t)n * sizeof(float), nd = (size_t)n * sizeof(double);
+    // Row arrays are read by 16-byte bulk copies that may run up to 3 elements past n.
+    const size_t nf = ((size_t)n + 8) * sizeof(float), nd = (size_t)n * sizeof(double);
     if ((rc = g->scale.alloc(nf)) || (rc = g->tele.alloc(nf)) || (rc = g->x0.alloc(nf)) || (rc = g->x1.alloc(nf)) ||
         (rc = g->z0.alloc(2 * nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd)) ||
         (rc = g->hubz.alloc(2 * (size_t)std::max(g->nhub, 4) * sizeof(float)))) {

@@ -33,45 +33,40 @@ constexpr int32_t kHasTail = 2;    // the chunk's last row continues into a late
 constexpr int32_t kInterior = 4;   // the chunk lies inside one row (head and tail are that row)
 
 struct Chunk {
-    int32_t sub_begin;   // first sub-tile (index into the graph's tile-coordinate table)
-    int32_t sub_end;     // one past the last sub-tile (coordinate sub_end closes the chunk)
+    int32_t sub_begin;   // SpMM: first sub-tile; sweep stage: first row touched
+    int32_t sub_end;     // SpMM: one past the last sub-tile; sweep stage: one past the last row touched
     int32_t graph;       // slot in the plan's graph table
     int32_t flags;
     int32_t head_ta;     // global chunk id where the head row's span starts
     int32_t tail_tb;     // global chunk id where the tail row's span ends
     int32_t tail_row;    // vertex id of the tail row (span rows are finalised by row id)
-    int32_t group;       // global reduction group (sweep chunks only)
+    int32_t pad2;
     int32_t nnz_begin;   // entries [nnz_begin, nnz_end) belong to the chunk
     int32_t nnz_end;
-    int32_t row_end;     // rows [first finished row of tile 0, row_end) are finished by the chunk
+    int32_t row_end;     // sweep stage: rows before row_end are finished by the stage
     int32_t pad;
 };
 
-// The sweep's warp tiles: kTileItems inbound entries per warp tile (each lane
-// kLaneItems consecutive entries, tile starts aligned to 8 entries), chunks of
-// whole rows (cut only inside rows longer than a chunk), and reduction groups
-// of at most kGroupChunks consecutive chunks of one graph.
-constexpr int kLaneItems = 8;
-constexpr int kTileItems = 32 * kLaneItems;
-constexpr int kGroupChunks = 64;
+// The sweep's stages: runs of consecutive rows with at most kStageMaxEntries
+// inbound entries and kStageMaxRows rows (only a row longer than a stage is
+// cut), staged whole in shared memory.  The buffers hold kStageEntries /
+// kStageRows elements because bulk copies start on 16-byte boundaries (up to 3
+// elements early) and the row offsets need one element past the last row.
+constexpr int kLaneItems = 8;                       // entries per consumer thread
+constexpr int kStageEntries = 2048;
+constexpr int kStageRows = 512;
+constexpr int kStageMaxEntries = kStageEntries - 8;
+constexpr int kStageMaxRows = kStageRows - 8;
 // Hub cache: the carried values of the kHubCap sources with the largest
 // out-degree are kept in shared memory by the sweep; inbound entries from a hub
 // store -(slot + 1) instead of the source id.
 constexpr int kHubCap = 32768;
-
-struct Group {
-    int32_t chunk_begin;
-    int32_t chunk_end;
-    int32_t graph;
-    int32_t pad;
-};
 
 // Per-graph device view used by the sweep kernels.
 struct GraphDev {
     const int32_t* in_row;   // n+1
     const int32_t* in_col;   // nnz
     const float* in_w;       // nnz, NULL = unit weights
-    const int2* sub_coord;   // merge-path coordinates (row, entry) of the sweep's warp tiles
     const double* outw;      // n, FP64 out-weight sums
     const float* scale;      // n, alpha/outw (FP32) or -1 for dangling vertices
     const float* tele;       // n, personalisation (NULL = uniform)
@@ -86,9 +81,7 @@ struct GraphDev {
     int32_t n;
     int32_t chunk_begin;     // this graph's global chunk id range
     int32_t chunk_end;
-    int32_t group_begin;     // this graph's global reduction groups
-    int32_t group_end;
-    int32_t span_begin;      // this graph's entries of the span list (span start chunks)
+    int32_t span_begin;      // this graph's entries of the span list (span start stages)
     int32_t span_end;
 };
 
@@ -119,25 +112,45 @@ struct Ctl {
     int32_t error;
 };
 
+// Shared-memory layout of the sweep: the staged hub values, then `slots` stage
+// buffers of slot_bytes each (byte offsets inside a buffer below).
+struct StageLayout {
+    int32_t slots;
+    int32_t slot_bytes;
+    int32_t hub_bytes;    // offset of the first stage buffer
+    int32_t hub_count;    // hub values staged (0: hubs read from global memory)
+    int32_t off_col;      // int32 sources; FP32 sweep: gathered values in place
+    int32_t off_val64;    // FP64 sweep: gathered values
+    int32_t off_w;        // FP32 weights (weighted graphs)
+    int32_t off_mark;     // u8 row-end marks
+    int32_t off_rowptr;   // in_row of the rows touched
+    int32_t off_xin;      // previous ranks of those rows
+    int32_t off_scale;    // FP32 sweep: alpha / out-weight
+    int32_t off_hslot;    // FP32 sweep: hub slot
+    int32_t dyn_bytes;    // dynamic shared memory of the launch
+};
+
+constexpr int kAccWords = 8;  // words per accumulator slot (6 used; 64-byte slots)
+
 struct SweepParams {
     const Chunk* chunks;
     int32_t nchunks;
     int32_t mode;            // 0 = FP32 sweep, 1 = FP64 correction sweep
     const GraphDev* graphs;
     GraphState* states;
-    double* chunk_part;      // 3 per chunk: err, dsum, xsum of rows finalised by the chunk
-    double* piece;           // 2 per chunk: head piece, tail piece
-    uint32_t* span_cnt;      // per chunk (span start)
-    double* span_part;       // 3 per chunk (span start): err, dsum, xsum of span rows
-    const Group* groups;
-    uint32_t* group_cnt;     // chunk arrivals per group
-    double* group_part;      // 3 per group
-    const int32_t* span_list;  // span start chunks, per graph ranges
+    // FP64 sums are accumulated as two's-complement fixed point (2 words: units
+    // of 2^-32 and of 2^-64) with integer atomics, so their order does not
+    // change the result.
+    unsigned long long* acc;       // kAccWords per slot: err, dangling, rank sums
+    unsigned long long* span_acc;  // 2 per stage (span start stage): the cut row's sum
+    const int32_t* span_list;  // span start stages
+    int32_t nspans;
+    int32_t acc_sub;           // accumulator slots per graph
     Ctl* ctl;
     cudaGraphConditionalHandle cond;
     int32_t use_cond;
-    int32_t total_warps;     // warps of the launch (exit accounting)
-    int32_t hub_smem;        // 1: one graph, its hub values are staged in shared memory
+    int32_t ngraphs;
+    StageLayout lay;
 };
 
 // ---- device buffers --------------------------------------------------------
@@ -154,16 +167,16 @@ struct DevBuf {
 struct Plan {
     int32_t ngraphs = 0;
     int32_t nchunks = 0;
-    int32_t grid = 0;        // CTAs of an FP32 sweep
-    int32_t grid_final = 0;  // CTAs of the FP64 correction sweep
+    int32_t grid = 0;        // CTAs of a sweep
+    int32_t any_weighted = 0;
+    int32_t hub_count = 0;   // hubs of the plan's graph (one-graph plans)
     int32_t max_n = 0;
-    DevBuf d_chunks, d_graphs, d_states, d_ndang, d_chunk_part, d_piece, d_span_cnt, d_span_part, d_ctl,
-        d_groups, d_group_cnt, d_group_part, d_span_list;
+    DevBuf d_chunks, d_graphs, d_states, d_ndang, d_ctl, d_span_list, d_acc, d_span_acc;
     std::vector<Chunk> h_chunks;      // a graph's own chunk table (local ids)
-    std::vector<Group> h_groups;      // a graph's own groups (local ids)
     std::vector<int32_t> h_spans;     // a graph's span start chunks (local ids)
     std::vector<Chunk> h_chunks_all;  // the plan's table (global ids)
-    int32_t ngroups = 0;
+    int32_t nspans = 0;
+    int32_t nacc = 0;                 // accumulator slots
     cudaGraph_t cg = nullptr;
     cudaGraphExec_t cg_exec = nullptr;
     cudaGraphConditionalHandle cond = 0;
@@ -190,11 +203,10 @@ struct egpr_graph {
     int32_t n_dangling = 0;        // out-weight <= 0 (reference mask)
     int32_t n_dangling_solve = 0;  // out-weight <= 1e-15 (EasyGraph CPU rule)
     double prep_seconds = 0.0;
-    int32_t nsub = 0;              // sub-tiles
-    int32_t chunk_subs = 1;        // sub-tiles per chunk
-    int32_t ntiles = 0;            // warp tiles of the sweep
+    int32_t nsub = 0;              // SpMM merge-path sub-tiles
+    int32_t chunk_subs = 1;        // sub-tiles per SpMM chunk
     // prepared graph
-    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord, tile_coord, hub_ids, hub_slot, hubz;
+    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord, hub_ids, hub_slot, hubz;
     int32_t nhub = 0;
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
@@ -220,13 +232,11 @@ double wall_seconds();
 // Preparation (prep.cu).
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
 int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
-int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s);
+int build_stage_table(egpr_graph* g, cudaStream_t s);
 int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
-int sweep_resident_warps();
-int chunks_per_warp();
 
 // Plans and sweeps (sweep.cu).
-int sweep_occupancy_grid(int mode);
+int sweep_grid();
 int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_t stream);
 int plan_capture_loop(Plan& plan, cudaStream_t stream);
 void plan_set_l2_window(Plan& plan, void* base, size_t bytes);

@@ -408,133 +408,81 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, cudaStrea
 
 namespace {
 
-// (row, entry, start of that row, diagonal) at ideal chunk boundaries d = c * chunk_items.
-__global__ void k_ideal_bounds(const int32_t* __restrict__ in_row, int32_t n, int64_t nnz, int64_t chunk_items,
-                               int32_t count, int4* __restrict__ out) {
-    const int64_t total = (int64_t)n + nnz;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= count; c += gridDim.x * blockDim.x) {
-        int64_t d = (int64_t)c * chunk_items;
-        if (d > total) d = total;
-        const int2 rc = merge_search(in_row, n, nnz, d);
-        out[c] = make_int4(rc.x, rc.y, rc.x < n ? in_row[rc.x] : (int32_t)nnz,
-                           rc.x < n ? in_row[rc.x + 1] : (int32_t)nnz);
-    }
-}
-
-// Warp tiles of chunk c (boundaries (r_c, k_c) .. (r_{c+1}, k_{c+1})): tile t covers
-// entries [T_t, T_t + kTileItems) with T_t = (k_c & ~7) + t * kTileItems and
-// finishes the rows r in [r_c, r_{c+1}) whose end in_row[r+1] lies in
-// (T_t, T_t + kTileItems] (tile 0 also those ending at or before T_0, the last
-// tile all remaining).  coord[off_c + t] = (T_t, first finished row).
-__global__ void k_tile_coords(const int32_t* __restrict__ in_row, const int4* __restrict__ chunk_rk,
-                              const int32_t* __restrict__ chunk_off, int32_t nchunks, int2* __restrict__ coord) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
-        const int4 a = chunk_rk[c], b = chunk_rk[c + 1];  // (row, entry, -, -)
-        const int32_t off = chunk_off[c], nt = chunk_off[c + 1] - off;
-        const int32_t t0 = a.y & ~7;
-        coord[off] = make_int2(t0, a.x);
-        for (int32_t t = 1; t < nt; ++t) {
-            const int32_t T = t0 + t * kTileItems;
-            int32_t lo = a.x, hi = b.x;  // first row in [a.x, b.x) with in_row[r+1] > T
-            while (lo < hi) {
-                const int32_t mid = lo + ((hi - lo) >> 1);
-                if (in_row[mid + 1] > T) hi = mid;
-                else lo = mid + 1;
-            }
-            coord[off + t] = make_int2(T, lo);
-        }
-    }
+int stage_entry_cap() {
+    static const int v = [] {
+        const char* e = std::getenv("EGPR_STAGE_ENTRIES");  // tuning: entries per stage
+        const int x = e ? std::atoi(e) : kStageMaxEntries;
+        return x >= 64 && x <= kStageMaxEntries ? x : kStageMaxEntries;
+    }();
+    return v;
 }
 
 }  // namespace
 
-// The sweep's work decomposition.  Chunk boundaries start at ideal diagonals
-// c * chunk_items and are moved back to the start of the row they fall in, so
-// a chunk holds whole rows; only a row longer than a chunk is cut (a span).
-// Chunks are cut into warp tiles of kTileItems items and grouped by
-// kGroupChunks for the reduction tree.
-int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s) {
+// The sweep's stages, by one host pass over in_row: consecutive rows are packed
+// while a stage holds at most stage_entry_cap() entries and kStageMaxRows rows.
+// A row that does not fit an empty stage is cut, filling the current stage
+// first; every cut leaves at least one entry of the row on each side.  A cut
+// row is a span: its stages add their pieces to the span's accumulator and the
+// sweep finishes the row once every stage of the launch is done.
+int build_stage_table(egpr_graph* g, cudaStream_t s) {
     const int32_t n = g->n;
     const int64_t nnz = g->nnz;
-    const int64_t total = (int64_t)n + nnz;
-    const int32_t ideal = (int32_t)std::max<int64_t>(1, (total + chunk_items - 1) / chunk_items);
-    int4* bounds = nullptr;
-    int rc = cuda_ok(cudaMallocAsync(&bounds, ((size_t)ideal + 1) * sizeof(int4), s), "cudaMallocAsync (bounds)");
-    if (rc) return rc;
-    k_ideal_bounds<<<grid_for((int64_t)ideal + 1), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, nnz, chunk_items,
-                                                                     ideal, bounds);
-    std::vector<int4> hb((size_t)ideal + 1);
-    rc = cuda_ok(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int4), cudaMemcpyDeviceToHost, s), "D2H bounds");
-    cudaFreeAsync(bounds, s);
-    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "sweep tiles"))) return rc;
-    // Snap: (row, entry, row start) per boundary.
+    const int32_t cap_e = stage_entry_cap(), cap_r = kStageMaxRows;
+    std::vector<int32_t> row((size_t)n + 1);
+    int rc = cuda_ok(cudaMemcpyAsync(row.data(), g->in_row.p, row.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
+                     "D2H in_row");
+    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "stage table"))) return rc;
     struct B {
-        int32_t r, k, rs;
-        int64_t d;
+        int32_t r, k;  // stage start: row, entry
     };
     std::vector<B> bs;
-    bs.push_back(B{0, 0, 0, 0});
-    for (int32_t c = 1; c < ideal; ++c) {
-        const int4 b = hb[(size_t)c];
-        B snapped{b.x, b.z, b.z, (int64_t)b.x + b.z};
-        // A cut keeps at least one entry of the row for the next chunk: a point
-        // after the row's last entry becomes the start of the following row.
-        B cut = b.y < b.w ? B{b.x, b.y, b.z, (int64_t)b.x + b.y}
-                          : B{b.x + 1, b.y, b.y, (int64_t)b.x + 1 + b.y};
-        if (snapped.d > bs.back().d) bs.push_back(snapped);
-        else if (cut.d > bs.back().d) bs.push_back(cut);
+    bs.push_back(B{0, 0});
+    int32_t ent = 0, rows = 0, r = 0, pos = 0;
+    while (r < n) {
+        const int32_t rem = row[(size_t)r + 1] - pos;
+        if (rows < cap_r && ent + rem <= cap_e) {
+            ++rows;
+            ent += rem;
+            pos = row[(size_t)r + 1];
+            ++r;
+            continue;
+        }
+        if ((rows > 0 && rem <= cap_e) || rows >= cap_r || ent >= cap_e) {
+            bs.push_back(B{r, pos});  // close the stage before row r (or its rest)
+            ent = rows = 0;
+            continue;
+        }
+        pos += cap_e - ent;  // cut: row r continues in the next stage
+        bs.push_back(B{r, pos});
+        ent = rows = 0;
     }
-    if (total > bs.back().d) bs.push_back(B{n, (int32_t)nnz, (int32_t)nnz, total});
+    if (bs.back().r != n || bs.back().k != (int32_t)nnz || bs.size() == 1) bs.push_back(B{n, (int32_t)nnz});
     const int32_t nch = (int32_t)bs.size() - 1;
-    std::vector<int4> rk((size_t)nch + 1);
-    std::vector<int32_t> off((size_t)nch + 1);
-    off[0] = 0;
-    for (int32_t c = 0; c <= nch; ++c) rk[(size_t)c] = make_int4(bs[(size_t)c].r, bs[(size_t)c].k, 0, 0);
-    for (int32_t c = 0; c < nch; ++c) {
-        const int64_t t0 = bs[(size_t)c].k & ~7;
-        const int64_t span = (int64_t)bs[(size_t)c + 1].k - t0;
-        const int32_t nt = (int32_t)std::max<int64_t>(1, (span + kTileItems - 1) / kTileItems);
-        off[(size_t)c + 1] = off[(size_t)c] + nt;
-    }
-    const int32_t slots = off[(size_t)nch];
-    if ((rc = g->tile_coord.alloc((size_t)slots * sizeof(int2)))) return rc;
-    int4* d_rk = nullptr;
-    int32_t* d_off = nullptr;
-    if ((rc = cuda_ok(cudaMallocAsync(&d_rk, rk.size() * sizeof(int4), s), "cudaMallocAsync")) ||
-        (rc = cuda_ok(cudaMallocAsync(&d_off, off.size() * sizeof(int32_t), s), "cudaMallocAsync")))
-        return rc;
-    cudaMemcpyAsync(d_rk, rk.data(), rk.size() * sizeof(int4), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
-    k_tile_coords<<<grid_for(nch), kThreads, 0, s>>>(g->in_row.as<int32_t>(), d_rk, d_off, nch,
-                                                      g->tile_coord.as<int2>());
-    cudaFreeAsync(d_rk, s);
-    cudaFreeAsync(d_off, s);
-    if ((rc = cuda_ok(cudaStreamSynchronize(s), "sweep tiles"))) return rc;
-    // Chunk table (local ids), spans and groups.
     std::vector<Chunk>& ch = g->plan.h_chunks;
     ch.assign((size_t)nch, Chunk{});
     for (int32_t c = 0; c < nch; ++c) {
         Chunk& k = ch[(size_t)c];
         const B& a = bs[(size_t)c];
         const B& b = bs[(size_t)c + 1];
-        k.sub_begin = off[(size_t)c];
-        k.sub_end = off[(size_t)c + 1];
-        k.nnz_begin = a.k;
-        k.nnz_end = b.k;
-        k.row_end = b.r;
-        k.pad = 0;
-        k.graph = 0;
-        const bool head = a.k > a.rs;
-        const bool tail = b.r < n && b.k > b.rs;
+        const bool head = a.r < n && a.k > row[(size_t)a.r];
+        const bool tail = b.r < n && b.k > row[(size_t)b.r];
         int32_t f = 0;
         if (head) f |= kHasHead;
         if (tail) f |= kHasTail;
         if (head && tail && a.r == b.r) f |= kInterior;
         k.flags = f;
+        k.sub_begin = a.r;
+        k.sub_end = b.r + (tail ? 1 : 0);
+        k.nnz_begin = a.k;
+        k.nnz_end = b.k;
+        k.row_end = b.r;
+        k.pad = 0;
+        k.graph = 0;
         k.tail_row = tail ? b.r : -1;
         k.head_ta = -1;
         k.tail_tb = -1;
-        k.group = c / kGroupChunks;
+        k.pad2 = 0;
     }
     g->plan.h_spans.clear();
     for (int32_t c = 0; c < nch; ++c) {
@@ -546,10 +494,6 @@ int build_sweep_tiles(egpr_graph* g, int64_t chunk_items, cudaStream_t s) {
         Chunk& k = ch[(size_t)c];
         if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
     }
-    g->plan.h_groups.clear();
-    for (int32_t c = 0; c < nch; c += kGroupChunks)
-        g->plan.h_groups.push_back(Group{c, std::min(nch, c + kGroupChunks), 0, 0});
-    g->ntiles = slots;
     return EGPR_SUCC;
 }
 
@@ -584,7 +528,7 @@ int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& ch,
         k.tail_row = tail ? b.x : -1;
         k.head_ta = -1;
         k.tail_tb = -1;
-        k.group = 0;
+        k.pad2 = 0;
     }
     for (int32_t c = 0; c < nch; ++c) {
         Chunk& k = ch[(size_t)c];
@@ -621,7 +565,8 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         uint32_t* hkey2 = tmp.get<uint32_t>((size_t)n, &rc);
         uint32_t* hval2 = tmp.get<uint32_t>((size_t)n, &rc);
         if (rc) return rc;
-        if ((rc = g->in_row.alloc(((size_t)n + 1) * sizeof(int32_t))) ||
+        // in_row, hub_slot: bulk copies of a stage's rows may read up to 3 elements past the end.
+        if ((rc = g->in_row.alloc(((size_t)n + 8) * sizeof(int32_t))) ||
             (rc = g->outw.alloc((size_t)n * sizeof(double))) ||
             (rc = g->dangling01.alloc((size_t)n * sizeof(int32_t))))
             return rc;
@@ -643,8 +588,8 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             return rc;
         g->nnz = nnz32;
         const int64_t nnz = g->nnz;
-        // Padding: a warp tile reads whole 8-entry groups up to kTileItems past the end.
-        const size_t pad = (size_t)(kTileItems + 16) * sizeof(int32_t);
+        // Padding: a stage's bulk copy reads up to 3 entries past the end.
+        const size_t pad = 16 * sizeof(int32_t);
         if ((rc = g->in_col.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(int32_t) + pad)))
             return rc;
         if (W && (rc = g->in_w.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(float) + pad)))
@@ -664,9 +609,9 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         // the granule of the shared-memory staging copy).
         const char* hub_env = std::getenv("EGPR_HUBS");  // EGPR_HUBS=0: no hub cache
         g->nhub = (hub_env && hub_env[0] == '0') ? 0 : (std::min<int32_t>(n, kHubCap) & ~3);
-        if ((rc = g->hub_slot.alloc((size_t)n * sizeof(int32_t))) ||
+        if ((rc = g->hub_slot.alloc(((size_t)n + 8) * sizeof(int32_t))) ||
             (rc = g->hub_ids.alloc((size_t)std::max(g->nhub, 4) * sizeof(int32_t))) ||
-            (rc = cuda_ok(cudaMemsetAsync(g->hub_slot.p, 0xff, (size_t)n * sizeof(int32_t), s), "memset")))
+            (rc = cuda_ok(cudaMemsetAsync(g->hub_slot.p, 0xff, ((size_t)n + 8) * sizeof(int32_t), s), "memset")))
             return rc;
         if (g->nhub > 0) {
             bool alt = false;
@@ -689,12 +634,7 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                                                                        g->sub_coord.as<int2>());
         g->n_dangling = (int32_t)hc[0];
         g->n_dangling_solve = (int32_t)hc[1];
-        // Sweep chunks: about kChunksPerWarp per resident warp so the queue balances.
-        const int64_t warps = std::max(1, sweep_resident_warps());
-        const int64_t per_warp = chunks_per_warp();
-        int64_t chunk_items = (total + warps * per_warp - 1) / (warps * per_warp);
-        chunk_items = std::max<int64_t>(kTileItems, (chunk_items + kTileItems - 1) / kTileItems * kTileItems);
-        if ((rc = build_sweep_tiles(g, chunk_items, s))) return rc;
+        if ((rc = build_stage_table(g, s))) return rc;
     }
     cudaEventRecord(g->ev1, s);
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "preparation"))) return rc;

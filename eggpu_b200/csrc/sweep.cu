@@ -16,28 +16,27 @@
 // Sdot, two memsets, add_base_and_reduce, scale_vec and the two host round
 // trips (gpu_easygraph/functions/centrality/pagerank.cu:591-664).
 //
-// Work split.  A graph's rows are cut into chunks of whole rows (only rows
-// longer than a chunk are cut, into "spans"), chunks into warp tiles of
-// kTileItems inbound entries starting on 8-entry boundaries.  One persistent
-// CTA of 32 independent warps runs per SM; warps pull chunks from a queue.
-// Per tile a warp
-//   1. loads its 256 entries' sources with two 16-byte loads per lane (lane l
-//      owns entries 8l..8l+7) and gathers their carried values: sources among
-//      the graph's hubs (the kHubCap largest out-degrees, encoded as -(slot+1))
-//      read the CTA's shared-memory copy of the hub values, staged once per
-//      launch by a TMA bulk copy; the rest read z from L2/HBM;
-//   2. marks the last entry of every row finished in the tile in a 256-bit
-//      mask (row ends come from in_row) and lists those rows in order; rows
-//      without entries are finished on the spot;
-//   3. sums each lane's 8 products segment by segment and joins rows that
-//      cross lanes with one shuffle segmented scan; a row still open at the
-//      tile's end carries into the next tile;
-//   4. finishes the listed rows (coalesced).
-// Rows cut between chunks are finished by whichever chunk arrives last, adding
-// the pieces in chunk order.  FP64 partial sums are reduced in a fixed order
-// through groups of chunks and then per graph, so every result is
-// deterministic.  Nothing waits on another warp; the only wait is on the TMA
-// copy, and it is bounded.
+// Work split.  A graph's rows are packed into stages of at most
+// kStageMaxEntries inbound entries and kStageMaxRows rows (only a row longer
+// than a stage is cut).  One persistent CTA runs per SM with three roles that
+// meet at a ring of stage buffers in shared memory, each guarded by mbarriers:
+//   * a producer warp claims stages from a global queue (a batch ahead) and
+//     moves each stage's sources, weights, row offsets, previous ranks, scales
+//     and hub slots into a free buffer with bulk copies (TMA);
+//   * gatherer warps replace every source by its carried value: hubs (the
+//     kHubCap largest out-degrees, encoded -(slot+1)) from the CTA's copy of
+//     the hub values, staged once per launch, the rest with asynchronous 4-byte
+//     copies from z (cp.async, tracked by the buffer's mbarrier), so a warp has
+//     no register tied to a load in flight and many stages gather at once;
+//   * two groups of eight consumer warps take alternate stages and work from
+//     shared memory only: row ends are marked, each thread sums its 8 entries
+//     segment by segment, a segmented scan over the group joins rows that cross
+//     threads, and the rows are finished with coalesced stores.
+// Rows cut between stages are finished by whichever stage arrives last, adding
+// the pieces in stage order.  FP64 partial sums are reduced in a fixed order
+// through groups of stages and then per graph, so every result is
+// deterministic.  No CTA waits on another; every wait inside a CTA is bounded
+// by the global timer and ends the launch with EGPR_TIMEOUT.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,17 +48,30 @@
 namespace egpr {
 namespace {
 
-constexpr int kCtaWarps = 32;                 // independent warps per CTA, one CTA per SM
+constexpr int kGatherWarps = 4;
+constexpr int kGroupWarps = kStageEntries / (32 * kLaneItems);  // consumer warps per group
+constexpr int kConsumerGroups = 2;
+constexpr int kCtaWarps = 1 + kGatherWarps + kConsumerGroups * kGroupWarps;
 constexpr int kCtaThreads = 32 * kCtaWarps;
+constexpr int kGatherThreads = 32 * kGatherWarps;
+constexpr int kGroupThreads = 32 * kGroupWarps;
+constexpr int kMaxSlots = 8;          // stage buffers at most
+constexpr int kClaim = 4;             // stages claimed from the queue at a time
+constexpr int kGatherLag = 2;         // stages a gatherer keeps in flight before signalling the oldest
+constexpr int kSmemGraphs = 256;      // graph states mirrored in shared memory
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kCopyPiece = 32768;        // bytes per bulk copy instruction
-constexpr long long kWaitLimit = 1ll << 26;   // bounded wait on the hub staging copy
+constexpr uint32_t kCopyPiece = 32768;             // bytes per hub staging copy
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every wait (2 s)
 
-template <typename Real>
-struct WarpScratch {
-    uint32_t flags[kTileItems / 32];
-    int32_t list[kTileItems];
-    Real rowval[kTileItems];
+static_assert(kGroupWarps * 32 * kLaneItems == kStageEntries, "a group covers one stage buffer");
+static_assert(kStageEntries % kGatherThreads == 0, "gatherers cover one stage buffer");
+static_assert(kGatherLag >= 1 && kGatherLag < kMaxSlots, "the ring must hold the stages a gatherer keeps in flight");
+
+struct StageInfo {
+    Chunk ck;
+    int32_t c;     // global stage id; -1: no more stages
+    int32_t iter;  // sweeps done by the stage's graph
+    int32_t pad[2];
 };
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
@@ -71,425 +83,735 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;  // valid in lane 0
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
+// ---- PTX wrappers ------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Generic-proxy writes to a stage buffer are ordered before the next bulk copy into it.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void group_sync(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kGroupThreads) : "memory");
+}
+// Barrier of one consumer group that also ORs a predicate over its threads.
+__device__ __forceinline__ bool group_any(int id, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{ .reg .pred p, q; setp.ne.u32 p, %1, 0; bar.red.or.pred q, %2, %3, p; selp.u32 %0, 1, 0, q; }"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(kGroupThreads)
+        : "memory");
+    return r != 0;
 }
 
-// Per-chunk view of one graph.
+// Bounded wait for the completion of phase `parity` of b.  Gives up when another
+// role of the CTA has given up or after kWaitNs, and then flags the launch.
+__device__ bool wait_bar(uint64_t* b, uint32_t parity, volatile int32_t* abort_flag, Ctl* ctl) {
+    if (mbar_try(b, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (uint32_t i = 1;; ++i) {
+        if (mbar_try(b, parity)) return true;
+        if ((i & 31u) == 0u) {
+            if (*abort_flag) return false;
+            if (global_ns() - t0 > kWaitNs) {
+                *abort_flag = 1;
+                atomicExch(&ctl->error, EGPR_TIMEOUT);
+                return false;
+            }
+        }
+    }
+}
+
+// ---- per-graph view ------------------------------------------------------------
 struct SweepView {
-    const float* xin;     // previous ranks
-    const float* zsrc32;  // carried values (FP32 sweep)
+    const float* xin;       // previous ranks (global; rows of cut spans)
     float* xout;
     float* zout;
-    const float* hub_in;  // hub values read by this sweep (global copy)
-    float* hub_out;       // hub values written for the next sweep
-    double jump;          // (1-alpha)/n + dangling term (uniform teleport)
-    double dmass;         // dangling term alone (personalised teleport)
+    float* hub_out;         // hub values written for the next sweep
+    const float* scale;
+    const int32_t* hub_slot;
+    const float* tele;
+    double* out;
+    double jump;            // (1-alpha)/n + dangling term (uniform teleport)
+    double dmass;           // dangling term alone (personalised teleport)
     double one_minus_alpha;
     int32_t personalised;
+    int32_t weighted;
 };
+
+template <bool kFinal>
+__device__ SweepView make_view(const GraphDev& G, GraphState* st, int32_t iter) {
+    SweepView W;
+    W.one_minus_alpha = 1.0 - st->alpha;
+    W.personalised = st->personalised;
+    W.weighted = G.in_w != nullptr;
+    W.scale = G.scale;
+    W.hub_slot = G.hub_slot;
+    W.tele = G.tele;
+    W.out = G.out;
+    if (!kFinal) {
+        const int par = iter & 1;
+        W.xin = G.x[par];
+        W.xout = G.x[par ^ 1];
+        W.zout = G.z[par ^ 1];
+        W.hub_out = G.hubz[par ^ 1];
+        W.dmass = ldcg(&st->dmass);
+    } else {
+        W.xin = G.x[(iter - 1) & 1];  // x_{k-1}: the input of the last sweep
+        W.xout = nullptr;
+        W.zout = nullptr;
+        W.hub_out = nullptr;
+        W.dmass = ldcg(&st->dmass_prev);
+    }
+    W.jump = st->c1 + W.dmass;
+    return W;
+}
 
 // Finishes row v given its gathered sum; accumulates residual / dangling /
 // rank sums.  FP32 sweep: writes x_new, z_new (and the hub copy of z_new); the
 // residual compares the stored FP32 iterates, so the loop can stop once they no
 // longer change even when tol*n is below FP32 resolution.  FP64 correction
 // sweep: writes the FP64 result.
-template <typename Real>
-__device__ __forceinline__ void finish_row(const GraphDev& G, const SweepView& W, int32_t v, double acc,
-                                           double& err, double& dsum, double& xsum) {
-    const float xin = W.xin[v];
-    const float scale = G.scale[v];
+template <bool kFinal>
+__device__ __forceinline__ void finish_row(const SweepView& W, int32_t v, double acc, float xin, float scale,
+                                           int32_t hs, double& err, double& dsum, double& xsum) {
     double val;
-    if (W.personalised) val = (acc + W.one_minus_alpha * (double)G.tele[v]) + W.dmass;
+    if (W.personalised) val = (acc + W.one_minus_alpha * (double)__ldg(W.tele + v)) + W.dmass;
     else val = acc + W.jump;
-    const double prev = (double)xin;
-    if constexpr (std::is_same<Real, float>::value) {
+    if (!kFinal) {
         const float xo = (float)val;
-        err += fabs((double)xo - prev);
+        err += fabs((double)xo - (double)xin);
         W.xout[v] = xo;
         const float zo = scale >= 0.f ? xo * scale : 0.f;
         W.zout[v] = zo;
-        const int32_t hs = G.hub_slot[v];
         if (hs >= 0) W.hub_out[hs] = zo;
         if (scale < 0.f) dsum += (double)xo;
         xsum += (double)xo;
     } else {
-        err += fabs(val - prev);
-        G.out[v] = val;
+        err += fabs(val - (double)xin);
+        W.out[v] = val;
         xsum += val;
     }
 }
 
-// Span arrival (lane 0 only).  The last participant adds the pieces in chunk
-// order and finishes the row; its contribution goes to the span's own slot.
-template <typename Real>
-__device__ void span_arrive(const SweepParams& P, const GraphDev& G, const SweepView& W, int32_t ta,
-                            int32_t participants) {
-    const uint32_t prev = atomicAdd(&P.span_cnt[ta], 1u);
-    if (prev != (uint32_t)(participants - 1)) return;
-    __threadfence();
-    const Chunk cta = P.chunks[ta];
-    const int32_t tb = cta.tail_tb;
-    double sum = ldcg(&P.piece[2 * ta + 1]);
-    for (int32_t q = ta + 1; q < tb; ++q) sum += ldcg(&P.piece[2 * q + 1]);
-    sum += ldcg(&P.piece[2 * tb]);
-    P.span_cnt[ta] = 0u;
-    double e = 0.0, d = 0.0, x = 0.0;
-    finish_row<Real>(G, W, cta.tail_row, sum, e, d, x);
-    P.span_part[3 * ta] = e;
-    P.span_part[3 * ta + 1] = d;
-    P.span_part[3 * ta + 2] = x;
-    __threadfence();
+// ---- order-free FP64 sums ---------------------------------------------------------
+// A value is split into two's-complement words in units of 2^-32 and of 2^-64
+// (the remainder, truncated) and added with integer atomics, so the total does
+// not depend on the order in which stages finish.  Partial sums here are far
+// below 2^31 and there are far fewer than 2^21 terms, so no word overflows and
+// both convert to double exactly.
+__device__ __forceinline__ void fx_add(unsigned long long* a, double v) {
+    const double t = v * 4294967296.0;  // exact
+    const double f = floor(t);
+    const unsigned long long hi = (unsigned long long)(long long)f;
+    const unsigned long long lo = (unsigned long long)((t - f) * 4294967296.0);
+    atomicAdd(a, hi);  // results unused: issued as reductions
+    atomicAdd(a + 1, lo);
 }
 
-// The last group of a graph (whole warp): reduce the graph's group partials
-// and span slots in a fixed order and advance the graph's state.
-template <typename Real>
-__device__ void graph_reduce(const SweepParams& P, const GraphDev& G, GraphState* st) {
-    const int lane = threadIdx.x & 31;
-    __threadfence();
-    double e = 0.0, d = 0.0, x = 0.0;
-    for (int32_t q = G.group_begin + lane; q < G.group_end; q += 32) {
-        e += ldcg(&P.group_part[3 * q]);
-        d += ldcg(&P.group_part[3 * q + 1]);
-        x += ldcg(&P.group_part[3 * q + 2]);
-    }
-    for (int32_t q = G.span_begin + lane; q < G.span_end; q += 32) {
-        const int32_t ta = P.span_list[q];
-        e += ldcg(&P.span_part[3 * ta]);
-        d += ldcg(&P.span_part[3 * ta + 1]);
-        x += ldcg(&P.span_part[3 * ta + 2]);
-        P.span_part[3 * ta] = 0.0;
-        P.span_part[3 * ta + 1] = 0.0;
-        P.span_part[3 * ta + 2] = 0.0;
-    }
-    e = warp_sum(e);
-    d = warp_sum(d);
-    x = warp_sum(x);
-    if (lane == 0) {
-        if constexpr (std::is_same<Real, float>::value) {
-            st->residual = e;
-            st->dsum = d;
-            st->xsum = x;
-            st->dmass_prev = st->dmass;
-            st->dmass = st->alpha * d / (double)G.n;
-            const int32_t it = st->iter + 1;
-            st->iter = it;
-            const bool conv = e < st->tol_n;
-            if (conv || it >= st->max_iter) {
-                st->done = 1;
-                st->converged = conv ? 1 : 0;
-                atomicSub(&P.ctl->active, 1);
-            }
-        } else {
-            st->residual64 = e;
-            st->xsum = x;
-        }
-        st->arrive = 0u;
-        __threadfence();
-    }
-    __syncwarp();
+__device__ __forceinline__ double fx_join(unsigned long long hi, unsigned long long lo) {
+    return (double)(long long)hi * (1.0 / 4294967296.0) + (double)lo * (1.0 / 18446744073709551616.0);
 }
 
-// Chunk done (whole warp): chunk partials, spans, group and graph arrival.
-template <typename Real>
-__device__ void chunk_finish(const SweepParams& P, int32_t c, const Chunk& ck, const GraphDev& G,
-                             const SweepView& W, GraphState* st, double err, double dsum, double xsum,
-                             double head_val, double tail_val) {
-    const int lane = threadIdx.x & 31;
-    err = warp_sum(err);
-    dsum = warp_sum(dsum);
-    xsum = warp_sum(xsum);
-    int32_t last_group = 0;
-    if (lane == 0) {
-        P.chunk_part[3 * c] = err;
-        P.chunk_part[3 * c + 1] = dsum;
-        P.chunk_part[3 * c + 2] = xsum;
-        const int32_t f = ck.flags;
-        if ((f & kHasHead) && !(f & kInterior)) P.piece[2 * c] = head_val;
-        if (f & kHasTail) P.piece[2 * c + 1] = tail_val;
-        __threadfence();
-        if (f & kInterior) {
-            span_arrive<Real>(P, G, W, ck.head_ta, ck.tail_tb - ck.head_ta + 1);
-        } else {
-            if (f & kHasHead) span_arrive<Real>(P, G, W, ck.head_ta, c - ck.head_ta + 1);
-            if (f & kHasTail) span_arrive<Real>(P, G, W, c, ck.tail_tb - c + 1);
-        }
-        __threadfence();
-        const Group gr = P.groups[ck.group];
-        const uint32_t prev = atomicAdd(&P.group_cnt[ck.group], 1u);
-        last_group = prev == (uint32_t)(gr.chunk_end - gr.chunk_begin - 1) ? 1 : 0;
-    }
-    last_group = __shfl_sync(kFull, last_group, 0);
-    if (!last_group) return;
-    // Last chunk of its group: fixed-order reduction of the group's chunks.
-    __threadfence();
-    const Group gr = P.groups[ck.group];
-    double e = 0.0, d = 0.0, x = 0.0;
-    for (int32_t q = gr.chunk_begin + lane; q < gr.chunk_end; q += 32) {
-        e += ldcg(&P.chunk_part[3 * q]);
-        d += ldcg(&P.chunk_part[3 * q + 1]);
-        x += ldcg(&P.chunk_part[3 * q + 2]);
-    }
-    e = warp_sum(e);
-    d = warp_sum(d);
-    x = warp_sum(x);
-    int32_t last_graph = 0;
-    if (lane == 0) {
-        P.group_part[3 * ck.group] = e;
-        P.group_part[3 * ck.group + 1] = d;
-        P.group_part[3 * ck.group + 2] = x;
-        P.group_cnt[ck.group] = 0u;
-        __threadfence();
-        const uint32_t prev = atomicAdd(&st->arrive, 1u);
-        last_graph = prev == (uint32_t)(G.group_end - G.group_begin - 1) ? 1 : 0;
-    }
-    last_graph = __shfl_sync(kFull, last_graph, 0);
-    if (last_graph) graph_reduce<Real>(P, G, st);
+__device__ __forceinline__ unsigned long long ldcg_u64(const unsigned long long* p) { return __ldcg(p); }
+
+// Accumulator slot of (graph, CTA, consumer group): each graph has acc_sub
+// slots so that concurrent stages rarely add to the same address.
+__device__ __forceinline__ unsigned long long* acc_slot(const SweepParams& P, int32_t gi, int32_t k) {
+    return P.acc + (size_t)kAccWords * ((size_t)gi * (size_t)P.acc_sub + (size_t)(k % P.acc_sub));
 }
 
-template <typename Real>
-__device__ void process_chunk(const SweepParams& P, int32_t c, WarpScratch<Real>& S, const float* hub_smem) {
-    constexpr bool kFinal = std::is_same<Real, double>::value;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    const Chunk ck = P.chunks[c];
-    const GraphDev& G = P.graphs[ck.graph];
-    GraphState* st = P.states + ck.graph;
-    const int32_t iter = ldcg(&st->iter);
-    if (!kFinal && ldcg(&st->done)) return;  // frozen graph (same answer for the whole warp)
-
-    SweepView W;
-    const double alpha = st->alpha;
-    W.one_minus_alpha = 1.0 - alpha;
-    W.personalised = st->personalised;
-    if (!kFinal) {
-        const int par = iter & 1;
-        W.xin = G.x[par];
-        W.zsrc32 = G.z[par];
-        W.xout = G.x[par ^ 1];
-        W.zout = G.z[par ^ 1];
-        W.hub_in = G.hubz[par];
-        W.hub_out = G.hubz[par ^ 1];
-        W.dmass = ldcg(&st->dmass);
+// Stage done (lane 0 of a consumer group's first warp): the stage's sums, and
+// the pieces of rows cut between stages, go to the accumulators.
+__device__ __forceinline__ void stage_accumulate(const SweepParams& P, int32_t c, const Chunk& ck, int32_t k,
+                                                 double err, double dsum, double xsum, double head_val,
+                                                 double tail_val) {
+    unsigned long long* a = acc_slot(P, ck.graph, k);
+    fx_add(a, err);
+    fx_add(a + 2, dsum);
+    fx_add(a + 4, xsum);
+    const int32_t f = ck.flags;
+    if (f & kInterior) {
+        fx_add(P.span_acc + 2 * ck.head_ta, tail_val);
     } else {
-        const int par = (iter - 1) & 1;  // x_{k-1}: the input of the last sweep
-        W.xin = G.x[par];
-        W.zsrc32 = nullptr;
-        W.xout = nullptr;
-        W.zout = nullptr;
-        W.hub_in = nullptr;
-        W.hub_out = nullptr;
-        W.dmass = ldcg(&st->dmass_prev);
+        if (f & kHasHead) fx_add(P.span_acc + 2 * ck.head_ta, head_val);
+        if (f & kHasTail) fx_add(P.span_acc + 2 * c, tail_val);
     }
-    W.jump = st->c1 + W.dmass;
-    const float* __restrict__ hub = hub_smem ? hub_smem : W.hub_in;
-    const int32_t* __restrict__ in_row = G.in_row;
-    const int4* __restrict__ col4 = reinterpret_cast<const int4*>(G.in_col);
-    const float4* __restrict__ w4 = reinterpret_cast<const float4*>(G.in_w);
-    const int2* __restrict__ coord = G.sub_coord;
+}
 
-    double err = 0.0, dsum = 0.0, xsum = 0.0;
-    Real carry = Real(0);  // partial of the row still open at the end of the previous tile
-    Real head_val = Real(0);
-    bool head_pending = (ck.flags & kHasHead) != 0;
+// End of a launch, run by the whole last CTA to leave the queue: finishes the
+// rows cut between stages, then per graph turns the accumulators into the
+// residual, dangling mass and rank sum, clears them, and advances the graph's
+// state (pagerank.py:117-131).
+template <bool kFinal>
+__device__ void launch_tail(const SweepParams& P) {
+    const int tid = threadIdx.x;
+    for (int32_t q = tid; q < P.nspans; q += blockDim.x) {
+        const int32_t ta = P.span_list[q];
+        const int32_t gi = __ldg(&P.chunks[ta].graph);
+        const int32_t v = __ldg(&P.chunks[ta].tail_row);
+        GraphState* st = P.states + gi;
+        if (!kFinal && ldcg(&st->done)) continue;
+        unsigned long long* sa = P.span_acc + 2 * ta;
+        const double sum = fx_join(ldcg_u64(sa), ldcg_u64(sa + 1));
+        sa[0] = 0ull;
+        sa[1] = 0ull;
+        const SweepView W = make_view<kFinal>(P.graphs[gi], st, ldcg(&st->iter));
+        double e = 0.0, d = 0.0, x = 0.0;
+        finish_row<kFinal>(W, v, sum, W.xin[v], kFinal ? 0.f : W.scale[v], kFinal ? -1 : W.hub_slot[v], e, d, x);
+        unsigned long long* a = acc_slot(P, gi, tid);
+        fx_add(a, e);
+        fx_add(a + 2, d);
+        fx_add(a + 4, x);
+    }
+    __threadfence();
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int32_t gi = warp; gi < P.ngraphs; gi += (int32_t)(blockDim.x >> 5)) {
+        GraphState* st = P.states + gi;
+        if (!kFinal && ldcg(&st->done)) continue;
+        unsigned long long w[6] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+        for (int32_t k = lane; k < P.acc_sub; k += 32) {
+            unsigned long long* a = P.acc + (size_t)kAccWords * ((size_t)gi * (size_t)P.acc_sub + (size_t)k);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                w[i] += ldcg_u64(a + i);
+                a[i] = 0ull;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w[i] += __shfl_down_sync(kFull, w[i], o);
+        if (lane == 0) {
+            const double e = fx_join(w[0], w[1]), d = fx_join(w[2], w[3]), x = fx_join(w[4], w[5]);
+            if (!kFinal) {
+                st->residual = e;
+                st->dsum = d;
+                st->xsum = x;
+                st->dmass_prev = st->dmass;
+                st->dmass = st->alpha * d / (double)P.graphs[gi].n;
+                const int32_t it = st->iter + 1;
+                st->iter = it;
+                const bool conv = e < st->tol_n;
+                if (conv || it >= st->max_iter) {
+                    st->done = 1;
+                    st->converged = conv ? 1 : 0;
+                    atomicSub(&P.ctl->active, 1);
+                }
+            } else {
+                st->residual64 = e;
+                st->xsum = x;
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+}
 
-    int2 tc = coord[ck.sub_begin];
-    int4 ca = __ldcs(col4 + (tc.x >> 2) + 2 * lane);
-    int4 cb = __ldcs(col4 + (tc.x >> 2) + 2 * lane + 1);
-    for (int32_t t = ck.sub_begin; t < ck.sub_end; ++t) {
-        const int32_t T = tc.x, fa = tc.y;
-        const bool has_next = t + 1 < ck.sub_end;
-        const int2 tn = has_next ? coord[t + 1] : make_int2(T, ck.row_end);
-        const int32_t fb = tn.y;
-        const int32_t lo = max(T, ck.nnz_begin), hi = min(T + kTileItems, ck.nnz_end);
-        // 1. gathers of this tile's entries
-        const int32_t cc[kLaneItems] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
-        const int32_t p0 = T + kLaneItems * lane;
+// ---- the three roles -------------------------------------------------------------
+struct CtaShared {
+    uint64_t bar_full[kMaxSlots];   // bulk copies of the stage landed (1 arrival + bytes)
+    uint64_t bar_gath[kMaxSlots];   // gathered values in place (1 arrival per gatherer thread)
+    uint64_t bar_empty[kMaxSlots];  // the consumers are done with the buffer (1 per consumer warp)
+    uint64_t bar_hub;               // hub values staged
+    StageInfo info[kMaxSlots];
+    double red[kConsumerGroups][kGroupWarps][3];
+    double scan_d[kConsumerGroups][kGroupWarps];
+    float scan_f[kConsumerGroups][kGroupWarps];
+    int32_t scan_flag[kConsumerGroups][kGroupWarps];
+    int32_t giter[kSmemGraphs];
+    int32_t gdone[kSmemGraphs];
+    int32_t abort_flag;
+    int32_t idle;
+    int32_t last;
+};
+
+__device__ __forceinline__ Chunk shfl_chunk(const Chunk& a, int src) {
+    Chunk b;
+    const int32_t* pa = reinterpret_cast<const int32_t*>(&a);
+    int32_t* pb = reinterpret_cast<int32_t*>(&b);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(Chunk) / 4); ++i) pb[i] = __shfl_sync(kFull, pa[i], src);
+    return b;
+}
+
+__device__ __forceinline__ Chunk load_chunk(const Chunk* p) {
+    const int4* q = reinterpret_cast<const int4*>(p);
+    Chunk c;
+    int4* d = reinterpret_cast<int4*>(&c);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(Chunk) / 16); ++i) d[i] = __ldg(q + i);
+    return c;
+}
+
+template <bool kFinal>
+__device__ void run_producer(const SweepParams& P, CtaShared& S, unsigned char* stages, float* hub_smem) {
+    const int lane = threadIdx.x & 31;
+    const StageLayout& L = P.lay;
+    const uint32_t nslots = (uint32_t)L.slots;
+    volatile int32_t* abort_flag = &S.abort_flag;
+    if (L.hub_count > 0 && lane == 0) {
+        const uint32_t bytes = (uint32_t)L.hub_count * (uint32_t)sizeof(float);
+        const float* src = P.graphs[0].hubz[S.giter[0] & 1];
+        mbar_arrive_tx(&S.bar_hub, bytes);
+        for (uint32_t off = 0; off < bytes; off += kCopyPiece)
+            bulk_load(reinterpret_cast<unsigned char*>(hub_smem) + off, reinterpret_cast<const unsigned char*>(src) + off,
+                      min(kCopyPiece, bytes - off), &S.bar_hub);
+    }
+    // Claims run one batch ahead: the queue position of the next batch and its
+    // stage records are in flight while the current batch is issued.
+    int32_t base_next = 0, base_after = P.nchunks;
+    if (lane == 0) base_next = (int32_t)atomicAdd(&P.ctl->queue, (uint32_t)kClaim);
+    base_next = __shfl_sync(kFull, base_next, 0);
+    if (lane == 0 && base_next < P.nchunks) base_after = (int32_t)atomicAdd(&P.ctl->queue, (uint32_t)kClaim);
+    Chunk nk{};
+    if (lane < kClaim && base_next + lane < P.nchunks) nk = load_chunk(P.chunks + base_next + lane);
+    uint32_t q = 0;
+    bool abort = false;
+    // lane 0's cache of the current graph's arrays
+    int32_t cg = -1, citer = -1;
+    const int32_t* in_col = nullptr;
+    const float* in_w = nullptr;
+    const int32_t* in_row = nullptr;
+    const float* xin = nullptr;
+    const float* scale = nullptr;
+    const int32_t* hslot = nullptr;
+    while (!abort) {
+        const int32_t base = base_next;
+        if (base >= P.nchunks) break;
+        const Chunk cur = nk;
+        base_next = __shfl_sync(kFull, base_after, 0);
+        if (lane == 0)
+            base_after = base_next < P.nchunks ? (int32_t)atomicAdd(&P.ctl->queue, (uint32_t)kClaim) : P.nchunks;
+        if (lane < kClaim && base_next + lane < P.nchunks) nk = load_chunk(P.chunks + base_next + lane);
+        for (int i = 0; i < kClaim; ++i) {
+            const int32_t c = base + i;
+            if (c >= P.nchunks) break;
+            const Chunk ck = shfl_chunk(cur, i);
+            const int32_t gi = ck.graph;
+            const int32_t iter = gi < kSmemGraphs ? S.giter[gi] : ldcg(&P.states[gi].iter);
+            if (!kFinal && (gi < kSmemGraphs ? S.gdone[gi] : ldcg(&P.states[gi].done))) continue;
+            const uint32_t slot = q % nslots, round = q / nslots;
+            if (round > 0 && !wait_bar(&S.bar_empty[slot], (round - 1) & 1u, abort_flag, P.ctl)) {
+                abort = true;
+                break;
+            }
+            if (lane == 0) {
+                if (gi != cg || iter != citer) {
+                    const GraphDev& G = P.graphs[gi];
+                    in_col = G.in_col;
+                    in_w = G.in_w;
+                    in_row = G.in_row;
+                    xin = kFinal ? G.x[(iter - 1) & 1] : G.x[iter & 1];
+                    scale = G.scale;
+                    hslot = G.hub_slot;
+                    cg = gi;
+                    citer = iter;
+                }
+                StageInfo& in = S.info[slot];
+                in.ck = ck;
+                in.c = c;
+                in.iter = iter;
+                unsigned char* sp = stages + (size_t)slot * (size_t)L.slot_bytes;
+                const int32_t e0 = ck.nnz_begin, e1 = ck.nnz_end;
+                const int32_t eb = e0 & ~3;
+                const uint32_t ebytes = e1 > e0 ? (uint32_t)(((e1 + 3) & ~3) - eb) * 4u : 0u;
+                const int32_t ra = ck.sub_begin, nr = ck.sub_end - ck.sub_begin;
+                const int32_t rb = ra & ~3;
+                const uint32_t pbytes = nr > 0 ? (uint32_t)(((ra + nr + 1 + 3) & ~3) - rb) * 4u : 0u;
+                const uint32_t xbytes = nr > 0 ? (uint32_t)(((ra + nr + 3) & ~3) - rb) * 4u : 0u;
+                const uint32_t tx = ebytes * (in_w ? 2u : 1u) + pbytes + xbytes * (kFinal ? 1u : 3u);
+                mbar_arrive_tx(&S.bar_full[slot], tx);
+                if (ebytes) {
+                    bulk_load(sp + L.off_col, in_col + eb, ebytes, &S.bar_full[slot]);
+                    if (in_w) bulk_load(sp + L.off_w, in_w + eb, ebytes, &S.bar_full[slot]);
+                }
+                if (nr > 0) {
+                    bulk_load(sp + L.off_rowptr, in_row + rb, pbytes, &S.bar_full[slot]);
+                    bulk_load(sp + L.off_xin, xin + rb, xbytes, &S.bar_full[slot]);
+                    if (!kFinal) {
+                        bulk_load(sp + L.off_scale, scale + rb, xbytes, &S.bar_full[slot]);
+                        bulk_load(sp + L.off_hslot, hslot + rb, xbytes, &S.bar_full[slot]);
+                    }
+                }
+            }
+            __syncwarp();
+            ++q;
+        }
+    }
+    // One end marker per consumer group (the gatherers stop at the first).
+    for (int k = 0; k < kConsumerGroups && !abort; ++k) {
+        const uint32_t slot = q % nslots, round = q / nslots;
+        if (round > 0 && !wait_bar(&S.bar_empty[slot], (round - 1) & 1u, abort_flag, P.ctl)) {
+            abort = true;
+            break;
+        }
+        if (lane == 0) {
+            S.info[slot].c = -1;
+            mbar_arrive(&S.bar_full[slot]);
+        }
+        __syncwarp();
+        ++q;
+    }
+    if (abort && lane == 0) {
+        // Leave no bulk copy in flight into this CTA's shared memory.
+        const uint32_t first = q > nslots ? q - nslots : 0u;
+        for (uint32_t k = first; k < q; ++k) {
+            const unsigned long long t0 = global_ns();
+            while (!mbar_try(&S.bar_full[k % nslots], (k / nslots) & 1u) && global_ns() - t0 < kWaitNs) {
+            }
+        }
+        if (L.hub_count > 0) {
+            const unsigned long long t0 = global_ns();
+            while (!mbar_try(&S.bar_hub, 0u) && global_ns() - t0 < kWaitNs) {
+            }
+        }
+    }
+}
+
+template <bool kFinal>
+__device__ void run_gatherer(const SweepParams& P, CtaShared& S, unsigned char* stages, const float* hub_smem) {
+    constexpr int kPer = kStageEntries / kGatherThreads;  // entries per gatherer thread and stage
+    const int j = threadIdx.x - 32;                       // 0 .. kGatherThreads-1
+    const StageLayout& L = P.lay;
+    const uint32_t nslots = (uint32_t)L.slots;
+    volatile int32_t* abort_flag = &S.abort_flag;
+    bool ok = L.hub_count > 0 ? wait_bar(&S.bar_hub, 0u, abort_flag, P.ctl) : true;
+    int32_t cg = -1, citer = -1;
+    const float* zsrc = nullptr;
+    const float* hub_g = nullptr;
+    const double* z64 = nullptr;
+    const int32_t* hub_ids = nullptr;
+    uint32_t q = 0;
+    for (; ok; ++q) {
+        const uint32_t slot = q % nslots, round = q / nslots;
+        if (!wait_bar(&S.bar_full[slot], round & 1u, abort_flag, P.ctl)) break;
+        const StageInfo& in = S.info[slot];
+        if (in.c < 0) break;
+        const int32_t gi = in.ck.graph, iter = in.iter;
+        if (gi != cg || iter != citer) {
+            const GraphDev& G = P.graphs[gi];
+            zsrc = G.z[iter & 1];
+            hub_g = G.hubz[iter & 1];
+            z64 = G.z64;
+            hub_ids = G.hub_ids;
+            cg = gi;
+            citer = iter;
+        }
+        unsigned char* sp = stages + (size_t)slot * (size_t)L.slot_bytes;
+        int32_t* col = reinterpret_cast<int32_t*>(sp + L.off_col);
+        double* v64 = reinterpret_cast<double*>(sp + L.off_val64);
+        const int32_t eb = in.ck.nnz_begin & ~3;
+        const int32_t lo = in.ck.nnz_begin - eb, hi = in.ck.nnz_end - eb;
+        // Consecutive threads take consecutive entries: conflict-free shared
+        // memory on both the source read and the value write.
+        int32_t cv[kPer];
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) cv[i] = col[j + i * kGatherThreads];
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const int k = j + i * kGatherThreads;
+            if (k < lo || k >= hi) continue;
+            const int32_t s = cv[i];
+            if (!kFinal) {
+                if (s >= 0) {
+                    cp_async4(col + k, zsrc + s);
+                } else {
+                    const int32_t h = -s - 1;
+                    if (h < L.hub_count) reinterpret_cast<float*>(col)[k] = hub_smem[h];
+                    else cp_async4(col + k, hub_g + h);
+                }
+            } else {
+                const int32_t idx = s >= 0 ? s : __ldg(hub_ids + (-s - 1));
+                cp_async8(v64 + k, z64 + idx);
+            }
+        }
+        cp_async_commit();
+        // Stage q - kGatherLag has landed: hand it to the consumers.
+        if (q >= (uint32_t)kGatherLag) {
+            cp_async_wait_group<kGatherLag>();
+            mbar_arrive(&S.bar_gath[(q - kGatherLag) % nslots]);
+        }
+    }
+    cp_async_wait_all();
+    for (uint32_t p = q > (uint32_t)kGatherLag ? q - kGatherLag : 0u; p < q; ++p) mbar_arrive(&S.bar_gath[p % nslots]);
+}
+
+template <typename Real>
+__device__ __forceinline__ void scan_store(CtaShared& S, int g, int w, Real v);
+template <>
+__device__ __forceinline__ void scan_store<float>(CtaShared& S, int g, int w, float v) { S.scan_f[g][w] = v; }
+template <>
+__device__ __forceinline__ void scan_store<double>(CtaShared& S, int g, int w, double v) { S.scan_d[g][w] = v; }
+template <typename Real>
+__device__ __forceinline__ Real scan_load(const CtaShared& S, int g, int w);
+template <>
+__device__ __forceinline__ float scan_load<float>(const CtaShared& S, int g, int w) { return S.scan_f[g][w]; }
+template <>
+__device__ __forceinline__ double scan_load<double>(const CtaShared& S, int g, int w) { return S.scan_d[g][w]; }
+
+template <typename Real>
+__device__ void run_consumer(const SweepParams& P, CtaShared& S, unsigned char* stages) {
+    constexpr bool kFinal = std::is_same<Real, double>::value;
+    const int gt = threadIdx.x - 32 * (1 + kGatherWarps);
+    const int g = gt / kGroupThreads, t = gt % kGroupThreads;
+    const int w = t >> 5, lane = t & 31;
+    const int bar_id = 1 + g;
+    const StageLayout& L = P.lay;
+    const uint32_t nslots = (uint32_t)L.slots;
+    volatile int32_t* abort_flag = &S.abort_flag;
+    int32_t cg = -1, citer = -1;
+    SweepView W{};
+    const int k0 = kLaneItems * t;
+    for (uint32_t q = (uint32_t)g;; q += kConsumerGroups) {
+        const uint32_t slot = q % nslots, round = q / nslots;
+        const bool ok = wait_bar(&S.bar_full[slot], round & 1u, abort_flag, P.ctl);
+        StageInfo in;
+        in.c = -1;
+        if (ok) in = S.info[slot];
+        if (group_any(bar_id, !ok || in.c < 0)) break;
+        if (in.ck.graph != cg || in.iter != citer) {
+            cg = in.ck.graph;
+            citer = in.iter;
+            W = make_view<kFinal>(P.graphs[cg], P.states + cg, citer);
+        }
+        unsigned char* sp = stages + (size_t)slot * (size_t)L.slot_bytes;
+        const int32_t e0 = in.ck.nnz_begin, e1 = in.ck.nnz_end;
+        const int32_t eb = e0 & ~3, lo = e0 - eb, hi = e1 - eb;
+        const int32_t ra = in.ck.sub_begin, nr = in.ck.sub_end - in.ck.sub_begin, ro = ra & 3;
+        const int32_t* rowp = reinterpret_cast<const int32_t*>(sp + L.off_rowptr) + ro;
+        uint8_t* mark = sp + L.off_mark;
+        // 1. mark the last entry of every row that ends in this stage
+        for (int j = t; j < nr; j += kGroupThreads) {
+            const int32_t rs = rowp[j], re = rowp[j + 1];
+            if (re <= e1 && re > max(rs, e0)) mark[re - 1 - eb] = 1;
+        }
+        const bool ok2 = wait_bar(&S.bar_gath[slot], round & 1u, abort_flag, P.ctl);
+        if (group_any(bar_id, !ok2)) break;
+        // 2. per-thread segmented sums over entries k0 .. k0+7; row sums are
+        //    written in place at the row's last entry
+        Real* rsum = kFinal ? reinterpret_cast<Real*>(sp + L.off_val64) : reinterpret_cast<Real*>(sp + L.off_col);
         Real v[kLaneItems];
+        if (!kFinal) {
+            const float4 a = *reinterpret_cast<const float4*>(sp + L.off_col + 4 * k0);
+            const float4 b = *reinterpret_cast<const float4*>(sp + L.off_col + 4 * k0 + 16);
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+            v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        } else {
 #pragma unroll
-        for (int u = 0; u < kLaneItems; ++u) {
-            const int32_t p = p0 + u;
-            const int32_t cu = cc[u];
-            Real x = Real(0);
-            if (p >= lo && p < hi) {
-                if constexpr (kFinal) x = G.z64[cu >= 0 ? cu : G.hub_ids[-cu - 1]];
-                else x = cu >= 0 ? W.zsrc32[cu] : hub[-cu - 1];
+            for (int u = 0; u < kLaneItems; u += 2) {
+                const double2 d = *reinterpret_cast<const double2*>(sp + L.off_val64 + 8 * (k0 + u));
+                v[u] = (Real)d.x;
+                v[u + 1] = (Real)d.y;
             }
-            v[u] = x;
         }
-        if (w4) {
-            const float4 wa = __ldcs(w4 + (T >> 2) + 2 * lane);
-            const float4 wb = __ldcs(w4 + (T >> 2) + 2 * lane + 1);
-            const float ww[kLaneItems] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
-#pragma unroll
-            for (int u = 0; u < kLaneItems; ++u) v[u] *= (Real)ww[u];
+        if (W.weighted) {
+            const float4 a = *reinterpret_cast<const float4*>(sp + L.off_w + 4 * k0);
+            const float4 b = *reinterpret_cast<const float4*>(sp + L.off_w + 4 * k0 + 16);
+            v[0] *= (Real)a.x; v[1] *= (Real)a.y; v[2] *= (Real)a.z; v[3] *= (Real)a.w;
+            v[4] *= (Real)b.x; v[5] *= (Real)b.y; v[6] *= (Real)b.z; v[7] *= (Real)b.w;
         }
-        if (has_next) {
-            ca = __ldcs(col4 + (tn.x >> 2) + 2 * lane);
-            cb = __ldcs(col4 + (tn.x >> 2) + 2 * lane + 1);
-        }
-        // 2. rows finished in this tile: end marks for rows with entries, the
-        //    rest finished on the spot
-        if (lane < kTileItems / 32) S.flags[lane] = 0u;
-        __syncwarp();
-        int32_t nlist = 0;
-        for (int32_t r0 = fa; r0 < fb; r0 += 32) {
-            const int32_t r = r0 + lane;
-            const bool in = r < fb;
-            const int32_t s = in ? in_row[r] : 0;
-            int32_t e = __shfl_down_sync(kFull, s, 1);
-            if (lane == 31 && in) e = in_row[r + 1];
-            if (in && r + 1 == fb && lane != 31) e = in_row[r + 1];
-            const bool ne = in && e > s;
-            const unsigned bal = __ballot_sync(kFull, ne);
-            if (ne) {
-                S.list[nlist + __popc(bal & lt_mask)] = r;
-                const int32_t bit = e - 1 - T;  // in [0, kTileItems) by construction of the tiles
-                if ((unsigned)bit < (unsigned)kTileItems) atomicOr(&S.flags[bit >> 5], 1u << (bit & 31));
-            } else if (in) {
-                finish_row<Real>(G, W, r, 0.0, err, dsum, xsum);
-            }
-            nlist += __popc(bal);
-        }
-        __syncwarp();
-        // 3. per-lane segmented sums, then lanes joined by a segmented scan
-        const uint32_t fw = S.flags[lane >> 2];
-        const int sh = (lane & 3) * 8;
-        const uint32_t mybits = (fw >> sh) & 0xffu;
-        int32_t k = __popc(fw & ((1u << sh) - 1u));
-        for (int w = 0; w < (lane >> 2); ++w) k += __popc(S.flags[w]);
+        const uint2 mk = *reinterpret_cast<const uint2*>(mark + k0);
         Real acc = Real(0), head_part = Real(0);
-        int32_t first_close = -1;
+        int first = -1;
 #pragma unroll
         for (int u = 0; u < kLaneItems; ++u) {
-            acc += v[u];
-            if ((mybits >> u) & 1u) {
-                if (first_close < 0) {
-                    first_close = k;
+            const int k = k0 + u;
+            if (k >= lo && k < hi) acc += v[u];
+            const uint32_t m = ((u < 4 ? mk.x : mk.y) >> (8 * (u & 3))) & 1u;
+            if (m) {
+                if (first < 0) {
+                    first = u;
                     head_part = acc;
                 } else {
-                    S.rowval[k] = acc;
+                    rsum[k] = acc;
                 }
                 acc = Real(0);
-                ++k;
             }
         }
-        bool f = first_close >= 0;
-        Real seg = acc;
-        if (lane == 0 && !f) seg += carry;
+        // 3. segmented scan over the group: (open sum, has a row end)
+        Real sa = acc;
+        int fa = first >= 0 ? 1 : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const Real up = __shfl_up_sync(kFull, seg, o);
-            const bool fup = __shfl_up_sync(kFull, (int)f, o) != 0;
+            const Real us = __shfl_up_sync(kFull, sa, o);
+            const int uf = __shfl_up_sync(kFull, fa, o);
             if (lane >= o) {
-                if (!f) seg += up;
-                f = f || fup;
+                if (!fa) sa += us;
+                fa |= uf;
             }
         }
-        const Real prev_seg = __shfl_up_sync(kFull, seg, 1);
-        if (first_close >= 0) S.rowval[first_close] = head_part + (lane == 0 ? carry : prev_seg);
-        carry = __shfl_sync(kFull, seg, 31);
-        __syncwarp();
-        // 4. finish the listed rows; the chunk's head row (cut before the chunk)
-        //    is the chunk's first listed row and becomes its span piece instead
-        int32_t jstart = 0;
-        if (head_pending && nlist > 0) {
-            head_val = S.rowval[0];
-            head_pending = false;
-            jstart = 1;
+        Real ex = __shfl_up_sync(kFull, sa, 1);
+        int exf = __shfl_up_sync(kFull, fa, 1);
+        if (lane == 0) {
+            ex = Real(0);
+            exf = 0;
         }
-        for (int32_t j = jstart + lane; j < nlist; j += 32)
-            finish_row<Real>(G, W, S.list[j], (double)S.rowval[j], err, dsum, xsum);
+        if (lane == 31) {
+            scan_store<Real>(S, g, w, sa);
+            S.scan_flag[g][w] = fa;
+        }
+        group_sync(bar_id);
+        Real cw = Real(0);
+        if (!exf) {
+            for (int w2 = w - 1; w2 >= 0; --w2) {
+                cw += scan_load<Real>(S, g, w2);
+                if (S.scan_flag[g][w2]) break;
+            }
+        }
+        Real tail_val = Real(0);  // the row still open at the end of the stage
+        if (t == 0) {
+            for (int w2 = kGroupWarps - 1; w2 >= 0; --w2) {
+                tail_val += scan_load<Real>(S, g, w2);
+                if (S.scan_flag[g][w2]) break;
+            }
+        }
+        if (first >= 0) rsum[k0 + first] = (exf ? ex : cw + ex) + head_part;
+        group_sync(bar_id);
+        // 4. finish the rows of the stage (not its head row begun in an earlier
+        //    stage, nor its tail row that continues)
+        const int32_t flags = in.ck.flags;
+        const int j_lo = (flags & kHasHead) ? 1 : 0;
+        const int j_hi = nr - ((flags & kHasTail) ? 1 : 0);
+        const float* xin_s = reinterpret_cast<const float*>(sp + L.off_xin) + ro;
+        const float* sc_s = reinterpret_cast<const float*>(sp + L.off_scale) + ro;
+        const int32_t* hs_s = reinterpret_cast<const int32_t*>(sp + L.off_hslot) + ro;
+        double err = 0.0, dsum = 0.0, xsum = 0.0;
+        for (int j = j_lo + t; j < j_hi; j += kGroupThreads) {
+            const int32_t rs = rowp[j], re = rowp[j + 1];
+            const Real sum = re > rs ? rsum[re - 1 - eb] : Real(0);
+            finish_row<kFinal>(W, ra + j, (double)sum, xin_s[j], kFinal ? 0.f : sc_s[j], kFinal ? -1 : hs_s[j], err,
+                               dsum, xsum);
+        }
+        Real head_val = Real(0);
+        if (t == 0 && (flags & kHasHead) && !(flags & kInterior)) head_val = rsum[rowp[1] - 1 - eb];
+        *reinterpret_cast<uint2*>(mark + k0) = make_uint2(0u, 0u);
+        err = warp_sum(err);
+        dsum = warp_sum(dsum);
+        xsum = warp_sum(xsum);
+        if (lane == 0) {
+            S.red[g][w][0] = err;
+            S.red[g][w][1] = dsum;
+            S.red[g][w][2] = xsum;
+        }
+        fence_proxy_async();
         __syncwarp();
-        tc = tn;
+        if (lane == 0) mbar_arrive(&S.bar_empty[slot]);
+        group_sync(bar_id);
+        if (w == 0) {
+            double e = 0.0, d = 0.0, x = 0.0;
+            if (lane < kGroupWarps) {
+                e = S.red[g][lane][0];
+                d = S.red[g][lane][1];
+                x = S.red[g][lane][2];
+            }
+            e = warp_sum(e);
+            d = warp_sum(d);
+            x = warp_sum(x);
+            if (lane == 0)
+                stage_accumulate(P, in.c, in.ck, 2 * (int32_t)blockIdx.x + g, e, d, x, (double)head_val,
+                                 (double)tail_val);
+        }
     }
-    chunk_finish<Real>(P, c, ck, G, W, st, err, dsum, xsum, (double)head_val, (double)carry);
 }
 
 template <typename Real>
 __global__ void __launch_bounds__(kCtaThreads, 1) k_sweep(SweepParams P) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long mbar;
-    __shared__ int32_t s_abort;
-    __shared__ int32_t s_idle;
     constexpr bool kFinal = std::is_same<Real, double>::value;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool stage = !kFinal && P.hub_smem;
-    const float* hub_smem = stage ? reinterpret_cast<const float*>(smem) : nullptr;
-    const size_t hub_bytes = stage ? (size_t)kHubCap * sizeof(float) : 0;
-    WarpScratch<Real>& S = reinterpret_cast<WarpScratch<Real>*>(smem + hub_bytes)[warp];
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(16) CtaShared S;
+    float* hub_smem = reinterpret_cast<float*>(smem);
+    unsigned char* stages = smem + P.lay.hub_bytes;
+    const int warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
-        s_abort = 0;
-        s_idle = (!kFinal && ldcg(&P.ctl->active) <= 0) ? 1 : 0;  // one reading for the whole CTA
+        S.abort_flag = 0;
+        S.idle = (!kFinal && ldcg(&P.ctl->active) <= 0) ? 1 : 0;  // one reading for the whole CTA
+        for (int i = 0; i < P.lay.slots; ++i) {
+            mbar_init(&S.bar_full[i], 1);
+            mbar_init(&S.bar_gath[i], kGatherThreads);
+            mbar_init(&S.bar_empty[i], kGroupWarps);
+        }
+        mbar_init(&S.bar_hub, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < min(P.ngraphs, kSmemGraphs); i += kCtaThreads) {
+        S.giter[i] = ldcg(&P.states[i].iter);
+        S.gdone[i] = ldcg(&P.states[i].done);
+    }
+    for (int i = threadIdx.x; i < P.lay.slots * (kStageEntries / 16); i += kCtaThreads) {
+        const int slot = i / (kStageEntries / 16), piece = i % (kStageEntries / 16);
+        *reinterpret_cast<uint4*>(stages + (size_t)slot * P.lay.slot_bytes + P.lay.off_mark + 16 * piece) =
+            make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
-    bool idle = s_idle != 0;
-    if (stage && !idle) {
-        // Stage graph 0's hub values for this launch's parity.  A CTA that reads
-        // the next parity can only do so after every chunk was taken, so it gets
-        // no work.
-        const GraphDev& G = P.graphs[0];
-        const uint32_t bytes = (uint32_t)G.nhub * (uint32_t)sizeof(float);
-        if (threadIdx.x == 0 && bytes > 0) {
-            const float* src = G.hubz[ldcg(&P.states[0].iter) & 1];
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(bytes)
-                         : "memory");
-            for (uint32_t off = 0; off < bytes; off += kCopyPiece) {
-                const uint32_t piece = min(kCopyPiece, bytes - off);
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        smem_u32(smem + off)),
-                    "l"(reinterpret_cast<const unsigned char*>(src) + off), "r"(piece), "r"(smem_u32(&mbar))
-                    : "memory");
-            }
-        }
-        __syncthreads();
-        if (bytes > 0) {
-            uint32_t ok = 0;
-            for (long long i = 0; i < kWaitLimit && !ok; ++i) {
-                asm volatile(
-                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-                    : "=r"(ok)
-                    : "r"(smem_u32(&mbar))
-                    : "memory");
-            }
-            if (!ok) atomicExch(&s_abort, 1);
-        }
-        __syncthreads();
-        if (s_abort) {
-            if (threadIdx.x == 0) atomicExch(&P.ctl->error, EGPR_TIMEOUT);
-            idle = true;
-        }
+    if (!S.idle) {
+        if (warp == 0) run_producer<kFinal>(P, S, stages, hub_smem);
+        else if (warp <= kGatherWarps) run_gatherer<kFinal>(P, S, stages, hub_smem);
+        else run_consumer<Real>(P, S, stages);
     }
-    if (!idle) {
-        for (;;) {
-            int32_t c = 0;
-            if (lane == 0) c = (int32_t)atomicAdd(&P.ctl->queue, 1u);
-            c = __shfl_sync(kFull, c, 0);
-            if (c >= P.nchunks) break;
-            process_chunk<Real>(P, c, S, hub_smem);
-        }
-    }
-    if (lane == 0) {
-        __threadfence();
+    __threadfence();  // this CTA's accumulator updates before its exit is counted
+    __syncthreads();
+    if (threadIdx.x == 0) {
         const uint32_t prev = atomicAdd(&P.ctl->exited, 1u);
-        if (prev == (uint32_t)(P.total_warps - 1)) {
-            // Last warp out: every chunk of this launch is done.
-            P.ctl->queue = 0u;
-            P.ctl->exited = 0u;
-            if (!kFinal) {
-                const int32_t launches = P.ctl->launches + 1;
-                P.ctl->launches = launches;
-                const int32_t active = ldcg(&P.ctl->active);
-                const bool more = active > 0 && launches < P.ctl->cap && P.ctl->error == 0;
-                if (active > 0 && launches >= P.ctl->cap) P.ctl->error = EGPR_TIMEOUT;
-                if (P.use_cond) cudaGraphSetConditional(P.cond, more ? 1u : 0u);
-            }
-            __threadfence();
+        S.last = prev == gridDim.x - 1 ? 1 : 0;
+    }
+    __syncthreads();
+    if (!S.last) return;
+    // Last CTA out: every stage of this launch is done.
+    __threadfence();
+    launch_tail<kFinal>(P);
+    if (threadIdx.x == 0) {
+        P.ctl->queue = 0u;
+        P.ctl->exited = 0u;
+        if (!kFinal) {
+            const int32_t launches = P.ctl->launches + 1;
+            P.ctl->launches = launches;
+            const int32_t active = ldcg(&P.ctl->active);
+            const bool more = active > 0 && launches < P.ctl->cap && P.ctl->error == 0;
+            if (active > 0 && launches >= P.ctl->cap) P.ctl->error = EGPR_TIMEOUT;
+            if (P.use_cond) cudaGraphSetConditional(P.cond, more ? 1u : 0u);
         }
+        __threadfence();
     }
 }
 
@@ -587,13 +909,76 @@ __global__ void k_normalize(const GraphDev* graphs, const GraphState* states, in
     }
 }
 
-int g_cta_cache[2][64] = {};
-
 int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SUCC : set_cuda_error(e, what); }
 
-size_t sweep_smem_bytes(int mode, bool hub) {
-    if (mode == 0) return (hub ? (size_t)kHubCap * sizeof(float) : 0) + kCtaWarps * sizeof(WarpScratch<float>);
-    return kCtaWarps * sizeof(WarpScratch<double>);
+int env_int(const char* name, int dflt, int lo, int hi) {
+    const char* e = std::getenv(name);
+    if (!e) return dflt;
+    const int x = std::atoi(e);
+    return x >= lo && x <= hi ? x : dflt;
+}
+
+// Dynamic shared memory a sweep launch may use on the current device (and the
+// kernel's opt-in to it).
+int smem_budget(int mode) {
+    static int cache[2][64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    int& c = cache[mode ? 1 : 0][dev];
+    if (c > 0) return c;
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa = {};
+    if (mode == 0) cudaFuncGetAttributes(&fa, k_sweep<float>);
+    else cudaFuncGetAttributes(&fa, k_sweep<double>);
+    cudaGetLastError();
+    if (optin <= 0) optin = 232448;
+    const int b = optin - (int)fa.sharedSizeBytes - 1024;
+    if (mode == 0) cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    else cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaGetLastError();
+    c = b;
+    return c;
+}
+
+// Stage buffer layout and ring depth.  FP32 sweeps of one graph stage up to
+// kHubCap hub values; the ring keeps EGPR_SLOTS buffers (default 4) and the hub
+// copy takes what is left.
+StageLayout make_layout(int mode, bool weighted, int32_t nhub) {
+    StageLayout L = {};
+    int off = 0;
+    auto take = [&](int bytes) {
+        const int o = off;
+        off += (bytes + 127) & ~127;
+        return o;
+    };
+    L.off_col = take(kStageEntries * 4);
+    L.off_val64 = mode ? take(kStageEntries * 8) : 0;
+    L.off_w = weighted ? take(kStageEntries * 4) : 0;
+    L.off_mark = take(kStageEntries);
+    L.off_rowptr = take(kStageRows * 4);
+    L.off_xin = take(kStageRows * 4);
+    L.off_scale = mode ? 0 : take(kStageRows * 4);
+    L.off_hslot = mode ? 0 : take(kStageRows * 4);
+    L.slot_bytes = off;
+    const int budget = smem_budget(mode);
+    // A gatherer signals stage q only after issuing stage q + kGatherLag, so the
+    // ring holds at least kGatherLag + 1 buffers.
+    const int min_slots = kGatherLag + 1;
+    const int max_slots = std::max(min_slots, std::min(kMaxSlots, budget / L.slot_bytes));
+    L.slots = std::max(min_slots, std::min(max_slots, env_int("EGPR_SLOTS", mode == 0 && nhub > 0 ? 4 : max_slots,
+                                                                 2, kMaxSlots)));
+    int32_t hubs = 0;
+    if (mode == 0 && nhub > 0) {
+        const int left = budget - L.slots * L.slot_bytes;
+        hubs = std::min<int32_t>(nhub, std::max(0, left) / 4) & ~31;
+        hubs = std::min<int32_t>(hubs, env_int("EGPR_HUB_SMEM", kHubCap, 0, kHubCap) & ~31);
+    }
+    L.hub_count = hubs;
+    L.hub_bytes = (hubs * 4 + 127) & ~127;
+    L.dyn_bytes = L.hub_bytes + L.slots * L.slot_bytes;
+    return L;
 }
 
 SweepParams make_params(Plan& plan, int mode, int use_cond) {
@@ -603,19 +988,16 @@ SweepParams make_params(Plan& plan, int mode, int use_cond) {
     P.mode = mode;
     P.graphs = plan.d_graphs.as<GraphDev>();
     P.states = plan.d_states.as<GraphState>();
-    P.chunk_part = plan.d_chunk_part.as<double>();
-    P.piece = plan.d_piece.as<double>();
-    P.span_cnt = plan.d_span_cnt.as<uint32_t>();
-    P.span_part = plan.d_span_part.as<double>();
-    P.groups = plan.d_groups.as<Group>();
-    P.group_cnt = plan.d_group_cnt.as<uint32_t>();
-    P.group_part = plan.d_group_part.as<double>();
+    P.acc = plan.d_acc.as<unsigned long long>();
+    P.span_acc = plan.d_span_acc.as<unsigned long long>();
+    P.acc_sub = plan.nacc / std::max(1, plan.ngraphs);
     P.span_list = plan.d_span_list.as<int32_t>();
+    P.nspans = plan.nspans;
     P.ctl = plan.d_ctl.as<Ctl>();
     P.cond = plan.cond;
     P.use_cond = use_cond;
-    P.total_warps = (mode ? plan.grid_final : plan.grid) * kCtaWarps;
-    P.hub_smem = (mode == 0 && plan.ngraphs == 1) ? 1 : 0;
+    P.ngraphs = plan.ngraphs;
+    P.lay = make_layout(mode, plan.any_weighted != 0, plan.ngraphs == 1 ? plan.hub_count : 0);
     return P;
 }
 
@@ -644,45 +1026,20 @@ cudaLaunchAttributeValue l2_window(const Plan& plan) {
     return v;
 }
 
-// Resident CTAs of a sweep kernel on the current device (dynamic shared memory
-// sized for the hub cache).
-int sweep_ctas(int mode) {
+}  // namespace
+
+// One persistent CTA per SM.
+int sweep_grid() {
+    static int cache[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    int& cached = g_cta_cache[mode ? 1 : 0][dev];
-    if (cached > 0) return cached;
-    int sms = 148, per_sm = 1;
+    if (cache[dev] > 0) return cache[dev];
+    int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (mode == 0) {
-        cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sweep_smem_bytes(0, true));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<float>, kCtaThreads, sweep_smem_bytes(0, true));
-    } else {
-        cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sweep_smem_bytes(1, false));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<double>, kCtaThreads,
-                                                      sweep_smem_bytes(1, false));
-    }
     cudaGetLastError();
-    if (per_sm < 1) per_sm = 1;
-    cached = sms * per_sm;
-    return cached;
-}
-
-}  // namespace
-
-int sweep_resident_warps() { return sweep_ctas(0) * kCtaWarps; }
-
-int sweep_occupancy_grid(int mode) { return sweep_ctas(mode); }
-
-int chunks_per_warp() {
-    static const int v = [] {
-        const char* e = std::getenv("EGPR_CHUNKS_PER_WARP");
-        const int x = e ? std::atoi(e) : 4;
-        return x >= 1 && x <= 64 ? x : 4;
-    }();
-    return v;
+    cache[dev] = std::max(1, sms);
+    return cache[dev];
 }
 
 // The FP32 carried values z (both buffers, contiguous) are gathered once per
@@ -719,7 +1076,6 @@ GraphDev graph_dev_view(const egpr_graph* g) {
     d.in_row = g->in_row.as<int32_t>();
     d.in_col = g->in_col.as<int32_t>();
     d.in_w = g->weighted ? g->in_w.as<float>() : nullptr;
-    d.sub_coord = g->tile_coord.as<int2>();
     d.outw = g->outw.as<double>();
     d.scale = g->scale.as<float>();
     d.tele = g->tele.as<float>();
@@ -736,7 +1092,6 @@ GraphDev graph_dev_view(const egpr_graph* g) {
     d.nhub = g->nhub;
     d.n = g->n;
     d.chunk_begin = d.chunk_end = 0;
-    d.group_begin = d.group_end = 0;
     d.span_begin = d.span_end = 0;
     return d;
 }
@@ -744,44 +1099,41 @@ GraphDev graph_dev_view(const egpr_graph* g) {
 int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_t stream) {
     plan.release();
     std::vector<Chunk> all;
-    std::vector<Group> groups;
     std::vector<int32_t> spans;
     std::vector<GraphDev> views((size_t)count);
     std::vector<int32_t> ndang((size_t)count);
-    int32_t max_n = 0;
+    int32_t max_n = 0, any_w = 0;
     for (int32_t gi = 0; gi < count; ++gi) {
         const egpr_graph* g = graphs[gi];
         const int32_t off = (int32_t)all.size();
-        const int32_t goff = (int32_t)groups.size();
         GraphDev v = graph_dev_view(g);
         v.chunk_begin = off;
-        v.group_begin = goff;
         v.span_begin = (int32_t)spans.size();
         for (const Chunk& c0 : g->plan.h_chunks) {
             Chunk c = c0;
             c.graph = gi;
             if (c.head_ta >= 0) c.head_ta += off;
             if (c.tail_tb >= 0) c.tail_tb += off;
-            c.group += goff;
             all.push_back(c);
         }
-        for (const Group& g0 : g->plan.h_groups)
-            groups.push_back(Group{g0.chunk_begin + off, g0.chunk_end + off, gi, 0});
         for (int32_t sp : g->plan.h_spans) spans.push_back(sp + off);
         v.chunk_end = (int32_t)all.size();
-        v.group_end = (int32_t)groups.size();
         v.span_end = (int32_t)spans.size();
         views[(size_t)gi] = v;
         ndang[(size_t)gi] = g->n_dangling_solve;
         max_n = std::max(max_n, g->n);
+        if (g->weighted) any_w = 1;
     }
     plan.ngraphs = count;
     plan.nchunks = (int32_t)all.size();
-    plan.ngroups = (int32_t)groups.size();
+    plan.nspans = (int32_t)spans.size();
     plan.max_n = max_n;
-    const int32_t chunk_ctas = std::max(1, (plan.nchunks + kCtaWarps - 1) / kCtaWarps);
-    plan.grid = std::max(1, std::min(chunk_ctas, sweep_ctas(0)));
-    plan.grid_final = std::max(1, std::min(chunk_ctas, sweep_ctas(1)));
+    plan.any_weighted = any_w;
+    plan.hub_count = count == 1 ? graphs[0]->nhub : 0;
+    plan.grid = std::max(1, std::min(plan.nchunks, sweep_grid()));
+    // accumulator slots: up to one per (CTA, consumer group) for each graph
+    const int32_t per_graph = std::max(1, std::min(2 * plan.grid, 8192 / std::max(1, count)));
+    plan.nacc = per_graph * count;
     plan.h_chunks_all = all;
     if (spans.empty()) spans.push_back(0);
     int rc;
@@ -789,23 +1141,14 @@ int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_
         (rc = plan.d_graphs.alloc(views.size() * sizeof(GraphDev))) ||
         (rc = plan.d_states.alloc((size_t)count * sizeof(GraphState))) ||
         (rc = plan.d_ndang.alloc((size_t)count * sizeof(int32_t))) ||
-        (rc = plan.d_chunk_part.alloc(all.size() * 3 * sizeof(double))) ||
-        (rc = plan.d_piece.alloc(all.size() * 2 * sizeof(double))) ||
-        (rc = plan.d_span_cnt.alloc(all.size() * sizeof(uint32_t))) ||
-        (rc = plan.d_span_part.alloc(all.size() * 3 * sizeof(double))) ||
-        (rc = plan.d_groups.alloc(groups.size() * sizeof(Group))) ||
-        (rc = plan.d_group_cnt.alloc(groups.size() * sizeof(uint32_t))) ||
-        (rc = plan.d_group_part.alloc(groups.size() * 3 * sizeof(double))) ||
+        (rc = plan.d_acc.alloc((size_t)plan.nacc * kAccWords * sizeof(unsigned long long))) ||
+        (rc = plan.d_span_acc.alloc(all.size() * 2 * sizeof(unsigned long long))) ||
         (rc = plan.d_span_list.alloc(spans.size() * sizeof(int32_t))) || (rc = plan.d_ctl.alloc(sizeof(Ctl))))
         return rc;
     if ((rc = cuda_ok(cudaMemcpyAsync(plan.d_chunks.p, all.data(), all.size() * sizeof(Chunk), cudaMemcpyHostToDevice, stream), "H2D chunks")) ||
         (rc = cuda_ok(cudaMemcpyAsync(plan.d_graphs.p, views.data(), views.size() * sizeof(GraphDev), cudaMemcpyHostToDevice, stream), "H2D graph table")) ||
         (rc = cuda_ok(cudaMemcpyAsync(plan.d_ndang.p, ndang.data(), ndang.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream), "H2D counts")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(plan.d_groups.p, groups.data(), groups.size() * sizeof(Group), cudaMemcpyHostToDevice, stream), "H2D groups")) ||
         (rc = cuda_ok(cudaMemcpyAsync(plan.d_span_list.p, spans.data(), spans.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream), "H2D spans")) ||
-        (rc = cuda_ok(cudaMemsetAsync(plan.d_span_cnt.p, 0, all.size() * sizeof(uint32_t), stream), "memset")) ||
-        (rc = cuda_ok(cudaMemsetAsync(plan.d_span_part.p, 0, all.size() * 3 * sizeof(double), stream), "memset")) ||
-        (rc = cuda_ok(cudaMemsetAsync(plan.d_group_cnt.p, 0, groups.size() * sizeof(uint32_t), stream), "memset")) ||
         (rc = cuda_ok(cudaStreamSynchronize(stream), "plan upload")))
         return rc;
     return EGPR_SUCC;
@@ -839,7 +1182,7 @@ int plan_capture_loop(Plan& plan, cudaStream_t stream) {
     kp.func = (void*)k_sweep<float>;
     kp.gridDim = dim3((unsigned)plan.grid);
     kp.blockDim = dim3(kCtaThreads);
-    kp.sharedMemBytes = (unsigned)sweep_smem_bytes(0, P.hub_smem != 0);
+    kp.sharedMemBytes = (unsigned)P.lay.dyn_bytes;
     kp.kernelParams = args;
     e = cudaGraphAddKernelNode(&knode, cp.conditional.phGraph_out[0], nullptr, 0, &kp);
     if (e != cudaSuccess) goto fail;
@@ -870,6 +1213,8 @@ int launch_init(Plan& plan, double alpha, int32_t max_iter, double tol, bool per
                                                                  plan.d_ndang.as<int32_t>(), plan.ngraphs,
                                                                  alpha, tol, max_iter, personalised ? 1 : 0);
     k_init_ctl<<<1, 1, 0, stream>>>(plan.d_ctl.as<Ctl>(), plan.ngraphs, max_iter + 1);
+    cudaMemsetAsync(plan.d_acc.p, 0, plan.d_acc.bytes, stream);
+    cudaMemsetAsync(plan.d_span_acc.p, 0, plan.d_span_acc.bytes, stream);
     return cuda_ok(cudaGetLastError(), "init launch");
 }
 
@@ -885,7 +1230,7 @@ int launch_loop(Plan& plan, int32_t max_iter, cudaStream_t stream, int32_t* laun
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)plan.grid);
     cfg.blockDim = dim3(kCtaThreads);
-    cfg.dynamicSmemBytes = sweep_smem_bytes(0, P.hub_smem != 0);
+    cfg.dynamicSmemBytes = (size_t)P.lay.dyn_bytes;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     if (plan.l2_bytes > 0) {
@@ -908,9 +1253,9 @@ int launch_finish(Plan& plan, bool correction, cudaStream_t stream, int32_t* lau
     if (correction) {
         k_prep_z64<<<grid, kThreads, 0, stream>>>(plan.d_graphs.as<GraphDev>(), plan.d_states.as<GraphState>(),
                                                   plan.ngraphs);
-        // The loop's last warp left the queue reset; the control block keeps the sweep count.
+        // The loop's last CTA left the queue reset; the control block keeps the sweep count.
         SweepParams P = make_params(plan, 1, 0);
-        k_sweep<double><<<plan.grid_final, kCtaThreads, sweep_smem_bytes(1, false), stream>>>(P);
+        k_sweep<double><<<plan.grid, kCtaThreads, (size_t)P.lay.dyn_bytes, stream>>>(P);
         l += 2;
     }
     k_normalize<<<grid, kThreads, 0, stream>>>(plan.d_graphs.as<GraphDev>(), plan.d_states.as<GraphState>(),
