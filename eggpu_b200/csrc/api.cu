@@ -300,6 +300,7 @@ static uint64_t bits_of(double x) {
 
 int64_t egpr_graph::device_bytes() const {
     return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes + sub_coord.bytes +
+                     sw_row.bytes + sw_col.bytes + sw_w.bytes + tile_bits.bytes + tile_row.bytes +
                      hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_acc.bytes + plan.d_span_acc.bytes +
                      plan.d_span_list.bytes +
                      scale.bytes + tele.bytes + x0.bytes + x1.bytes + z0.bytes + z1.bytes + out.bytes + z64.bytes +
@@ -318,7 +319,8 @@ static void destroy_graph_object(egpr_graph* g) {
     if (g->own_stream) cudaStreamSynchronize(g->own_stream);
     spmm_work_release(g);
     g->plan.release();
-    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord,
+    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord, &g->sw_row,
+                      &g->sw_col, &g->sw_w, &g->tile_bits, &g->tile_row,
                       &g->hub_ids, &g->hub_slot, &g->hubz, &g->scale, &g->tele,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})
         b->release();
@@ -384,8 +386,13 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
     // Row arrays are read by 16-byte bulk copies that may run up to 3 elements past n.
     const size_t nf = ((size_t)n + 8) * sizeof(float), nd = (size_t)n * sizeof(double);
     if ((rc = g->scale.alloc(nf)) || (rc = g->tele.alloc(nf)) || (rc = g->x0.alloc(nf)) || (rc = g->x1.alloc(nf)) ||
-        (rc = g->z0.alloc(2 * nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd)) ||
-        (rc = g->hubz.alloc(2 * (size_t)std::max(g->nhub, 4) * sizeof(float)))) {
+        (rc = g->z0.alloc(2 * nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd + sizeof(double))) ||
+        (rc = g->hubz.alloc(2 * (size_t)hub_stride(g->nhub) * sizeof(float))) ||
+        // zero slots: hubz[.][nhub] and z64[n] are read by placeholder entries
+        (rc = (cudaMemsetAsync(g->hubz.p, 0, g->hubz.bytes, g->own_stream) == cudaSuccess &&
+               cudaMemsetAsync(g->z64.p, 0, g->z64.bytes, g->own_stream) == cudaSuccess)
+                  ? EGPR_SUCC
+                  : set_cuda_error(cudaGetLastError(), "memset"))) {
         destroy_graph_object(g);
         return rc;
     }

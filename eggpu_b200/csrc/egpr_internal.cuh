@@ -47,26 +47,21 @@ struct Chunk {
     int32_t pad;
 };
 
-// The sweep's stages: runs of consecutive rows with at most kStageMaxEntries
-// inbound entries and kStageMaxRows rows (only a row longer than a stage is
-// cut), staged whole in shared memory.  The buffers hold kStageEntries /
-// kStageRows elements because bulk copies start on 16-byte boundaries (up to 3
-// elements early) and the row offsets need one element past the last row.
-constexpr int kLaneItems = 8;                       // entries per consumer thread
-constexpr int kStageEntries = 2048;
-constexpr int kStageRows = 512;
-constexpr int kStageMaxEntries = kStageEntries - 8;
-constexpr int kStageMaxRows = kStageRows - 8;
-// Hub cache: the carried values of the kHubCap sources with the largest
-// out-degree are kept in shared memory by the sweep; inbound entries from a hub
-// store -(slot + 1) instead of the source id.
+// The sweep's warp tiles: kTileItems entries, lane l owning entries 8l..8l+7.
+constexpr int kLaneItems = 8;
+constexpr int kTileItems = 32 * kLaneItems;
+// Hub cache: the carried values of the (up to kHubCap - 32) sources with the
+// largest out-degree are kept in shared memory by the sweep; inbound entries
+// from a hub store -(slot + 1) instead of the source id.  Slot nhub holds 0 and
+// is read by the placeholder entry of every row without entries.
 constexpr int kHubCap = 32768;
 
 // Per-graph device view used by the sweep kernels.
 struct GraphDev {
-    const int32_t* in_row;   // n+1
-    const int32_t* in_col;   // nnz
-    const float* in_w;       // nnz, NULL = unit weights
+    const int32_t* cols;        // sweep entries: hub-encoded sources, a placeholder in every empty row
+    const float* w;             // their weights, NULL = unit weights
+    const uint32_t* tile_bits;  // per warp tile: kTileItems bits, set on entries that end a row
+    const int32_t* tile_row;    // per warp tile: the row its first mark ends
     const double* outw;      // n, FP64 out-weight sums
     const float* scale;      // n, alpha/outw (FP32) or -1 for dangling vertices
     const float* tele;       // n, personalisation (NULL = uniform)
@@ -112,24 +107,6 @@ struct Ctl {
     int32_t error;
 };
 
-// Shared-memory layout of the sweep: the staged hub values, then `slots` stage
-// buffers of slot_bytes each (byte offsets inside a buffer below).
-struct StageLayout {
-    int32_t slots;
-    int32_t slot_bytes;
-    int32_t hub_bytes;    // offset of the first stage buffer
-    int32_t hub_count;    // hub values staged (0: hubs read from global memory)
-    int32_t off_col;      // int32 sources; FP32 sweep: gathered values in place
-    int32_t off_val64;    // FP64 sweep: gathered values
-    int32_t off_w;        // FP32 weights (weighted graphs)
-    int32_t off_mark;     // u8 row-end marks
-    int32_t off_rowptr;   // in_row of the rows touched
-    int32_t off_xin;      // previous ranks of those rows
-    int32_t off_scale;    // FP32 sweep: alpha / out-weight
-    int32_t off_hslot;    // FP32 sweep: hub slot
-    int32_t dyn_bytes;    // dynamic shared memory of the launch
-};
-
 constexpr int kAccWords = 8;  // words per accumulator slot (6 used; 64-byte slots)
 
 struct SweepParams {
@@ -150,7 +127,7 @@ struct SweepParams {
     cudaGraphConditionalHandle cond;
     int32_t use_cond;
     int32_t ngraphs;
-    StageLayout lay;
+    int32_t hub_count;       // hub slots staged in shared memory (0: hubs read from global memory)
 };
 
 // ---- device buffers --------------------------------------------------------
@@ -207,6 +184,10 @@ struct egpr_graph {
     int32_t chunk_subs = 1;        // sub-tiles per SpMM chunk
     // prepared graph
     egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord, hub_ids, hub_slot, hubz;
+    // the sweep's layout (see build_sweep_layout)
+    egpr::DevBuf sw_row, sw_col, sw_w, tile_bits, tile_row;
+    int64_t sw_nnz = 0;
+    int32_t ntiles = 0;
     int32_t nhub = 0;
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
@@ -232,11 +213,13 @@ double wall_seconds();
 // Preparation (prep.cu).
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
 int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
-int build_stage_table(egpr_graph* g, cudaStream_t s);
+int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s);
 int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
 
 // Plans and sweeps (sweep.cu).
 int sweep_grid();
+int sweep_resident_warps();
+int32_t hub_stride(int32_t nhub);  // floats per parity of the hub copy (zero slot included)
 int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_t stream);
 int plan_capture_loop(Plan& plan, cudaStream_t stream);
 void plan_set_l2_window(Plan& plan, void* base, size_t bytes);

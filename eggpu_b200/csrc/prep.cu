@@ -406,74 +406,121 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, cudaStrea
     return rc;
 }
 
+// The sweep's copy of the inbound CSR: every row keeps its entries (hub-encoded,
+// in the order of in_col) and a row without entries gets one placeholder entry
+// that reads a carried value of 0 (hub slot nhub).  One warp per row.
+__global__ void k_build_sweep_cols(const int32_t* __restrict__ in_row, const int32_t* __restrict__ in_col,
+                                   const float* __restrict__ in_w, int32_t n, const int32_t* __restrict__ sw_row,
+                                   int32_t* __restrict__ sw_col, float* __restrict__ sw_w, int32_t zero_code) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = warp; r < n; r += nwarps) {
+        const int32_t b = in_row[r], e = in_row[r + 1], o = sw_row[r];
+        if (e == b) {
+            if (lane == 0) {
+                sw_col[o] = zero_code;
+                if (sw_w) sw_w[o] = 0.f;
+            }
+            continue;
+        }
+        for (int32_t p = lane; p < e - b; p += 32) {
+            sw_col[o + p] = in_col[b + p];
+            if (sw_w) sw_w[o + p] = in_w[b + p];
+        }
+    }
+}
+
 namespace {
 
-int stage_entry_cap() {
+int chunks_per_warp() {
     static const int v = [] {
-        const char* e = std::getenv("EGPR_STAGE_ENTRIES");  // tuning: entries per stage
-        const int x = e ? std::atoi(e) : kStageMaxEntries;
-        return x >= 64 && x <= kStageMaxEntries ? x : kStageMaxEntries;
+        const char* e = std::getenv("EGPR_CHUNKS_PER_WARP");  // tuning: queue granularity
+        const int x = e ? std::atoi(e) : 4;
+        return x >= 1 && x <= 64 ? x : 4;
     }();
     return v;
 }
 
 }  // namespace
 
-// The sweep's stages, by one host pass over in_row: consecutive rows are packed
-// while a stage holds at most stage_entry_cap() entries and kStageMaxRows rows.
-// A row that does not fit an empty stage is cut, filling the current stage
-// first; every cut leaves at least one entry of the row on each side.  A cut
-// row is a span: its stages add their pieces to the span's accumulator and the
-// sweep finishes the row once every stage of the launch is done.
-int build_stage_table(egpr_graph* g, cudaStream_t s) {
+// The sweep's work layout, by one host pass over in_row.
+//   * sw_row / sw_col / sw_w: the inbound CSR with a placeholder entry in every
+//     empty row, so that every row ends on an entry of its own;
+//   * chunks: consecutive rows packed while a chunk holds at most chunk_items
+//     entries; a longer row is cut (a span: its chunks add pieces to the span's
+//     accumulator and the sweep finishes the row when the launch ends), and
+//     every cut leaves at least one entry of the row on each side;
+//   * warp tiles: chunk c covers tiles of kTileItems entries from
+//     (start & ~7); per tile a 256-bit mask of the entries that end a row
+//     finished by the chunk, and the first such row (the k-th mark of a tile
+//     ends row tile_row + k, since every row has an entry).
+int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     const int32_t n = g->n;
-    const int64_t nnz = g->nnz;
-    const int32_t cap_e = stage_entry_cap(), cap_r = kStageMaxRows;
     std::vector<int32_t> row((size_t)n + 1);
     int rc = cuda_ok(cudaMemcpyAsync(row.data(), g->in_row.p, row.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
                      "D2H in_row");
-    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "stage table"))) return rc;
+    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "sweep layout"))) return rc;
+    std::vector<int32_t> sw((size_t)n + 8);
+    int64_t acc = 0;
+    for (int32_t r = 0; r < n; ++r) {
+        sw[(size_t)r] = (int32_t)acc;
+        acc += std::max(1, row[(size_t)r + 1] - row[(size_t)r]);
+    }
+    if (acc > (int64_t)INT32_MAX - 4096) return EGPR_UNSUPPORTED_GRAPH;
+    for (size_t r = (size_t)n; r < sw.size(); ++r) sw[r] = (int32_t)acc;
+    const int32_t nnz = (int32_t)acc;
+    g->sw_nnz = nnz;
+    // chunks
+    const int64_t warps = std::max(1, resident_warps);
+    int64_t target = ((int64_t)nnz + warps * chunks_per_warp() - 1) / (warps * chunks_per_warp());
+    target = std::max<int64_t>(kTileItems, (target + kTileItems - 1) / kTileItems * kTileItems);
+    const int32_t cap_e = (int32_t)std::min<int64_t>(target, 1 << 24);
     struct B {
-        int32_t r, k;  // stage start: row, entry
+        int32_t r, k;  // chunk start: row, entry
     };
     std::vector<B> bs;
     bs.push_back(B{0, 0});
     int32_t ent = 0, rows = 0, r = 0, pos = 0;
     while (r < n) {
-        const int32_t rem = row[(size_t)r + 1] - pos;
-        if (rows < cap_r && ent + rem <= cap_e) {
+        const int32_t rem = sw[(size_t)r + 1] - pos;
+        if (ent + rem <= cap_e) {
             ++rows;
             ent += rem;
-            pos = row[(size_t)r + 1];
+            pos = sw[(size_t)r + 1];
             ++r;
             continue;
         }
-        if ((rows > 0 && rem <= cap_e) || rows >= cap_r || ent >= cap_e) {
-            bs.push_back(B{r, pos});  // close the stage before row r (or its rest)
+        if ((rows > 0 && rem <= cap_e) || ent >= cap_e) {
+            bs.push_back(B{r, pos});  // close the chunk before row r (or its rest)
             ent = rows = 0;
             continue;
         }
-        pos += cap_e - ent;  // cut: row r continues in the next stage
+        pos += cap_e - ent;  // cut: row r continues in the next chunk
         bs.push_back(B{r, pos});
         ent = rows = 0;
     }
-    if (bs.back().r != n || bs.back().k != (int32_t)nnz || bs.size() == 1) bs.push_back(B{n, (int32_t)nnz});
+    if (bs.back().r != n || bs.back().k != nnz || bs.size() == 1) bs.push_back(B{n, nnz});
     const int32_t nch = (int32_t)bs.size() - 1;
     std::vector<Chunk>& ch = g->plan.h_chunks;
     ch.assign((size_t)nch, Chunk{});
+    std::vector<int32_t> first_row((size_t)nch);
+    int64_t ntiles = 0;
     for (int32_t c = 0; c < nch; ++c) {
-        Chunk& k = ch[(size_t)c];
         const B& a = bs[(size_t)c];
         const B& b = bs[(size_t)c + 1];
-        const bool head = a.r < n && a.k > row[(size_t)a.r];
-        const bool tail = b.r < n && b.k > row[(size_t)b.r];
+        const int32_t t0 = a.k & ~7;
+        const int32_t nt = std::max<int32_t>(1, (b.k - t0 + kTileItems - 1) / kTileItems);
+        Chunk& k = ch[(size_t)c];
+        const bool head = a.r < n && a.k > sw[(size_t)a.r];
+        const bool tail = b.r < n && b.k > sw[(size_t)b.r];
         int32_t f = 0;
         if (head) f |= kHasHead;
         if (tail) f |= kHasTail;
         if (head && tail && a.r == b.r) f |= kInterior;
         k.flags = f;
-        k.sub_begin = a.r;
-        k.sub_end = b.r + (tail ? 1 : 0);
+        k.sub_begin = (int32_t)ntiles;
+        k.sub_end = (int32_t)(ntiles + nt);
         k.nnz_begin = a.k;
         k.nnz_end = b.k;
         k.row_end = b.r;
@@ -483,6 +530,29 @@ int build_stage_table(egpr_graph* g, cudaStream_t s) {
         k.head_ta = -1;
         k.tail_tb = -1;
         k.pad2 = 0;
+        first_row[(size_t)c] = a.r;
+        ntiles += nt;
+    }
+    if (ntiles > INT32_MAX / 2) return EGPR_UNSUPPORTED_GRAPH;
+    g->ntiles = (int32_t)ntiles;
+    std::vector<uint32_t> bits((size_t)ntiles * (kTileItems / 32), 0u);
+    std::vector<int32_t> trow((size_t)ntiles, -1);
+    for (int32_t c = 0; c < nch; ++c) {
+        const Chunk& k = ch[(size_t)c];
+        const int32_t t0 = k.nnz_begin & ~7;
+        // rows finished by the chunk: [first row, row_end); each ends on an entry in (begin, end]
+        for (int32_t rr = first_row[(size_t)c]; rr < k.row_end; ++rr) {
+            const int32_t p = sw[(size_t)rr + 1] - 1 - t0;
+            const int32_t t = k.sub_begin + p / kTileItems, i = p % kTileItems;
+            bits[(size_t)t * (kTileItems / 32) + (size_t)(i >> 5)] |= 1u << (i & 31);
+            if (trow[(size_t)t] < 0) trow[(size_t)t] = rr;
+        }
+        // a tile without a mark: the row its next mark would end
+        int32_t next = k.row_end;
+        for (int32_t t = k.sub_end - 1; t >= k.sub_begin; --t) {
+            if (trow[(size_t)t] < 0) trow[(size_t)t] = next;
+            else next = trow[(size_t)t];
+        }
     }
     g->plan.h_spans.clear();
     for (int32_t c = 0; c < nch; ++c) {
@@ -494,7 +564,25 @@ int build_stage_table(egpr_graph* g, cudaStream_t s) {
         Chunk& k = ch[(size_t)c];
         if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
     }
-    return EGPR_SUCC;
+    // device arrays (a tile reads up to kTileItems + 8 entries past a chunk's start)
+    const size_t pad = (size_t)(kTileItems + 16) * sizeof(int32_t);
+    if ((rc = g->sw_row.alloc(sw.size() * sizeof(int32_t))) ||
+        (rc = g->sw_col.alloc((size_t)nnz * sizeof(int32_t) + pad)) ||
+        (g->weighted && (rc = g->sw_w.alloc((size_t)nnz * sizeof(float) + pad))) ||
+        (rc = g->tile_bits.alloc(bits.size() * sizeof(uint32_t))) ||
+        (rc = g->tile_row.alloc(trow.size() * sizeof(int32_t))))
+        return rc;
+    if ((rc = cuda_ok(cudaMemcpyAsync(g->sw_row.p, sw.data(), sw.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D sweep rows")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(g->tile_bits.p, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "H2D tile masks")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(g->tile_row.p, trow.data(), trow.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D tile rows")) ||
+        (rc = cuda_ok(cudaMemsetAsync(g->sw_col.p, 0, g->sw_col.bytes, s), "memset")))
+        return rc;
+    if (g->weighted && (rc = cuda_ok(cudaMemsetAsync(g->sw_w.p, 0, g->sw_w.bytes, s), "memset"))) return rc;
+    k_build_sweep_cols<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(
+        g->in_row.as<int32_t>(), g->in_col.as<int32_t>(), g->weighted ? g->in_w.as<float>() : nullptr, n,
+        g->sw_row.as<int32_t>(), g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr,
+        -(g->nhub + 1));
+    return cuda_ok(cudaStreamSynchronize(s), "sweep layout");
 }
 
 // Chunk table over a graph's sub-tiles: runs of chunk_subs sub-tiles, with the
@@ -608,9 +696,10 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         // Hubs: the min(n, kHubCap) sources of largest out-degree (a multiple of 4,
         // the granule of the shared-memory staging copy).
         const char* hub_env = std::getenv("EGPR_HUBS");  // EGPR_HUBS=0: no hub cache
-        g->nhub = (hub_env && hub_env[0] == '0') ? 0 : (std::min<int32_t>(n, kHubCap) & ~3);
+        // (kHubCap - 32 leaves room for the zero slot nhub in a kHubCap-value copy)
+        g->nhub = (hub_env && hub_env[0] == '0') ? 0 : (std::min<int32_t>(n, kHubCap - 32) & ~3);
         if ((rc = g->hub_slot.alloc(((size_t)n + 8) * sizeof(int32_t))) ||
-            (rc = g->hub_ids.alloc((size_t)std::max(g->nhub, 4) * sizeof(int32_t))) ||
+            (rc = g->hub_ids.alloc((size_t)std::max(g->nhub + 1, 4) * sizeof(int32_t))) ||
             (rc = cuda_ok(cudaMemsetAsync(g->hub_slot.p, 0xff, ((size_t)n + 8) * sizeof(int32_t), s), "memset")))
             return rc;
         if (g->nhub > 0) {
@@ -621,6 +710,11 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             if (nnz > 0)
                 k_encode_hubs<<<grid_for(nnz), kThreads, 0, s>>>(g->in_col.as<int32_t>(), nnz, g->hub_slot.as<int32_t>());
         }
+        // hub slot nhub is the zero slot of placeholder entries; in the FP64
+        // correction sweep it reads z64[n] = 0
+        if ((rc = cuda_ok(cudaMemcpyAsync(g->hub_ids.as<int32_t>() + g->nhub, &g->n, sizeof(int32_t),
+                                          cudaMemcpyHostToDevice, s), "H2D zero slot")))
+            return rc;
         k_dangling<<<grid_for(n), kThreads, 0, s>>>(g->outw.as<double>(), n, g->dangling01.as<int32_t>(), counts);
         unsigned long long hc[2] = {0, 0};
         if ((rc = cuda_ok(cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s), "D2H counts")))
@@ -634,7 +728,7 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                                                                        g->sub_coord.as<int2>());
         g->n_dangling = (int32_t)hc[0];
         g->n_dangling_solve = (int32_t)hc[1];
-        if ((rc = build_stage_table(g, s))) return rc;
+        if ((rc = build_sweep_layout(g, sweep_resident_warps(), s))) return rc;
     }
     cudaEventRecord(g->ev1, s);
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "preparation"))) return rc;

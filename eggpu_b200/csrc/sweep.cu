@@ -16,27 +16,29 @@
 // Sdot, two memsets, add_base_and_reduce, scale_vec and the two host round
 // trips (gpu_easygraph/functions/centrality/pagerank.cu:591-664).
 //
-// Work split.  A graph's rows are packed into stages of at most
-// kStageMaxEntries inbound entries and kStageMaxRows rows (only a row longer
-// than a stage is cut).  One persistent CTA runs per SM with three roles that
-// meet at a ring of stage buffers in shared memory, each guarded by mbarriers:
-//   * a producer warp claims stages from a global queue (a batch ahead) and
-//     moves each stage's sources, weights, row offsets, previous ranks, scales
-//     and hub slots into a free buffer with bulk copies (TMA);
-//   * gatherer warps replace every source by its carried value: hubs (the
-//     kHubCap largest out-degrees, encoded -(slot+1)) from the CTA's copy of
-//     the hub values, staged once per launch, the rest with asynchronous 4-byte
-//     copies from z (cp.async, tracked by the buffer's mbarrier), so a warp has
-//     no register tied to a load in flight and many stages gather at once;
-//   * two groups of eight consumer warps take alternate stages and work from
-//     shared memory only: row ends are marked, each thread sums its 8 entries
-//     segment by segment, a segmented scan over the group joins rows that cross
-//     threads, and the rows are finished with coalesced stores.
-// Rows cut between stages are finished by whichever stage arrives last, adding
-// the pieces in stage order.  FP64 partial sums are reduced in a fixed order
-// through groups of stages and then per graph, so every result is
-// deterministic.  No CTA waits on another; every wait inside a CTA is bounded
-// by the global timer and ends the launch with EGPR_TIMEOUT.
+// Work split.  The sweep reads its own copy of the inbound CSR in which every
+// row ends on an entry of its own (an empty row holds one placeholder entry
+// whose carried value is 0).  Rows are packed into chunks (only a row longer
+// than a chunk is cut); a chunk is walked in warp tiles of kTileItems entries,
+// lane l owning entries 8l..8l+7.  For every tile the layout holds a 256-bit
+// mask of the entries that end a row and the row the first of them ends, so
+// the k-th mark of a tile ends row tile_row + k.  One persistent CTA per SM
+// runs independent warps that pull chunks from a queue; per tile a warp
+//   1. gathers the carried values of its 256 entries: hubs (the largest
+//      out-degrees, encoded -(slot+1)) from the CTA's shared-memory copy of
+//      the hub values, staged once per launch by a TMA bulk copy; the rest
+//      from z in L2/HBM.  The next tile's sources and mask are already loaded,
+//      and the previous ranks, scales and hub slots of the tile's rows are
+//      requested before the gathers return;
+//   2. sums each lane's entries segment by segment and joins the segments
+//      that cross lanes with a five-step shuffle scan bounded by the marked
+//      lanes; a row still open at the tile's end carries into the next tile;
+//   3. finishes the tile's rows with coalesced stores.
+// FP64 sums (residual, dangling mass, rank sum) are added as fixed-point
+// integers, so their total does not depend on the order in which chunks
+// finish; rows cut between chunks are finished by the last CTA to leave the
+// launch, which also advances every graph's state.  No warp waits on another;
+// the only wait is on the hub staging copy, and it is bounded.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,34 +50,15 @@
 namespace egpr {
 namespace {
 
-constexpr int kGatherWarps = 4;
-constexpr int kGroupWarps = kStageEntries / (32 * kLaneItems);  // consumer warps per group
-constexpr int kConsumerGroups = 2;
-constexpr int kCtaWarps = 1 + kGatherWarps + kConsumerGroups * kGroupWarps;
+constexpr int kCtaWarps = 24;         // independent warps per CTA, one CTA per SM
 constexpr int kCtaThreads = 32 * kCtaWarps;
-constexpr int kGatherThreads = 32 * kGatherWarps;
-constexpr int kGroupThreads = 32 * kGroupWarps;
-constexpr int kMaxSlots = 8;          // stage buffers at most
-constexpr int kClaim = 4;             // stages claimed from the queue at a time
-constexpr int kGatherLag = 2;         // stages a gatherer keeps in flight before signalling the oldest
-constexpr int kSmemGraphs = 256;      // graph states mirrored in shared memory
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kCopyPiece = 32768;             // bytes per hub staging copy
-constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every wait (2 s)
-
-static_assert(kGroupWarps * 32 * kLaneItems == kStageEntries, "a group covers one stage buffer");
-static_assert(kStageEntries % kGatherThreads == 0, "gatherers cover one stage buffer");
-static_assert(kGatherLag >= 1 && kGatherLag < kMaxSlots, "the ring must hold the stages a gatherer keeps in flight");
-
-struct StageInfo {
-    Chunk ck;
-    int32_t c;     // global stage id; -1: no more stages
-    int32_t iter;  // sweeps done by the stage's graph
-    int32_t pad[2];
-};
+constexpr uint32_t kCopyPiece = 32768;                 // bytes per hub staging copy
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of the staging wait (2 s)
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned long long ldcg_u64(const unsigned long long* p) { return __ldcg(p); }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -88,9 +71,6 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)_
 
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
@@ -110,60 +90,15 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-// Generic-proxy writes to a stage buffer are ordered before the next bulk copy into it.
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-__device__ __forceinline__ void group_sync(int id) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kGroupThreads) : "memory");
-}
-// Barrier of one consumer group that also ORs a predicate over its threads.
-__device__ __forceinline__ bool group_any(int id, bool pred) {
-    uint32_t r;
-    asm volatile(
-        "{ .reg .pred p, q; setp.ne.u32 p, %1, 0; bar.red.or.pred q, %2, %3, p; selp.u32 %0, 1, 0, q; }"
-        : "=r"(r)
-        : "r"((uint32_t)pred), "r"(id), "r"(kGroupThreads)
-        : "memory");
-    return r != 0;
-}
-
-// Bounded wait for the completion of phase `parity` of b.  Gives up when another
-// role of the CTA has given up or after kWaitNs, and then flags the launch.
-__device__ bool wait_bar(uint64_t* b, uint32_t parity, volatile int32_t* abort_flag, Ctl* ctl) {
-    if (mbar_try(b, parity)) return true;
-    const unsigned long long t0 = global_ns();
-    for (uint32_t i = 1;; ++i) {
-        if (mbar_try(b, parity)) return true;
-        if ((i & 31u) == 0u) {
-            if (*abort_flag) return false;
-            if (global_ns() - t0 > kWaitNs) {
-                *abort_flag = 1;
-                atomicExch(&ctl->error, EGPR_TIMEOUT);
-                return false;
-            }
-        }
-    }
-}
 
 // ---- per-graph view ------------------------------------------------------------
 struct SweepView {
-    const float* xin;       // previous ranks (global; rows of cut spans)
+    const float* xin;       // previous ranks
     float* xout;
     float* zout;
     float* hub_out;         // hub values written for the next sweep
@@ -175,7 +110,6 @@ struct SweepView {
     double dmass;           // dangling term alone (personalised teleport)
     double one_minus_alpha;
     int32_t personalised;
-    int32_t weighted;
 };
 
 template <bool kFinal>
@@ -183,7 +117,6 @@ __device__ SweepView make_view(const GraphDev& G, GraphState* st, int32_t iter) 
     SweepView W;
     W.one_minus_alpha = 1.0 - st->alpha;
     W.personalised = st->personalised;
-    W.weighted = G.in_w != nullptr;
     W.scale = G.scale;
     W.hub_slot = G.hub_slot;
     W.tele = G.tele;
@@ -235,15 +168,15 @@ __device__ __forceinline__ void finish_row(const SweepView& W, int32_t v, double
 
 // ---- order-free FP64 sums ---------------------------------------------------------
 // A value is split into two's-complement words in units of 2^-32 and of 2^-64
-// (the remainder, truncated) and added with integer atomics, so the total does
-// not depend on the order in which stages finish.  Partial sums here are far
-// below 2^31 and there are far fewer than 2^21 terms, so no word overflows and
-// both convert to double exactly.
+// (the remainder, rounded) and added with integer atomics, so the total does
+// not depend on the order in which chunks finish.  Partial sums here are far
+// below 2^31 and there are far fewer than 2^20 terms per word, so no word
+// overflows and both convert to double exactly.
 __device__ __forceinline__ void fx_add(unsigned long long* a, double v) {
     const double t = v * 4294967296.0;  // exact
     const double f = floor(t);
     const unsigned long long hi = (unsigned long long)(long long)f;
-    const unsigned long long lo = (unsigned long long)((t - f) * 4294967296.0);
+    const unsigned long long lo = (unsigned long long)rint((t - f) * 4294967296.0);
     atomicAdd(a, hi);  // results unused: issued as reductions
     atomicAdd(a + 1, lo);
 }
@@ -252,34 +185,14 @@ __device__ __forceinline__ double fx_join(unsigned long long hi, unsigned long l
     return (double)(long long)hi * (1.0 / 4294967296.0) + (double)lo * (1.0 / 18446744073709551616.0);
 }
 
-__device__ __forceinline__ unsigned long long ldcg_u64(const unsigned long long* p) { return __ldcg(p); }
-
-// Accumulator slot of (graph, CTA, consumer group): each graph has acc_sub
-// slots so that concurrent stages rarely add to the same address.
+// Accumulator slot of (graph, k): each graph has acc_sub slots so that
+// concurrent chunks rarely add to the same address.
 __device__ __forceinline__ unsigned long long* acc_slot(const SweepParams& P, int32_t gi, int32_t k) {
     return P.acc + (size_t)kAccWords * ((size_t)gi * (size_t)P.acc_sub + (size_t)(k % P.acc_sub));
 }
 
-// Stage done (lane 0 of a consumer group's first warp): the stage's sums, and
-// the pieces of rows cut between stages, go to the accumulators.
-__device__ __forceinline__ void stage_accumulate(const SweepParams& P, int32_t c, const Chunk& ck, int32_t k,
-                                                 double err, double dsum, double xsum, double head_val,
-                                                 double tail_val) {
-    unsigned long long* a = acc_slot(P, ck.graph, k);
-    fx_add(a, err);
-    fx_add(a + 2, dsum);
-    fx_add(a + 4, xsum);
-    const int32_t f = ck.flags;
-    if (f & kInterior) {
-        fx_add(P.span_acc + 2 * ck.head_ta, tail_val);
-    } else {
-        if (f & kHasHead) fx_add(P.span_acc + 2 * ck.head_ta, head_val);
-        if (f & kHasTail) fx_add(P.span_acc + 2 * c, tail_val);
-    }
-}
-
 // End of a launch, run by the whole last CTA to leave the queue: finishes the
-// rows cut between stages, then per graph turns the accumulators into the
+// rows cut between chunks, then per graph turns the accumulators into the
 // residual, dangling mass and rank sum, clears them, and advances the graph's
 // state (pagerank.py:117-131).
 template <bool kFinal>
@@ -348,32 +261,22 @@ __device__ void launch_tail(const SweepParams& P) {
     __syncthreads();
 }
 
-// ---- the three roles -------------------------------------------------------------
-struct CtaShared {
-    uint64_t bar_full[kMaxSlots];   // bulk copies of the stage landed (1 arrival + bytes)
-    uint64_t bar_gath[kMaxSlots];   // gathered values in place (1 arrival per gatherer thread)
-    uint64_t bar_empty[kMaxSlots];  // the consumers are done with the buffer (1 per consumer warp)
-    uint64_t bar_hub;               // hub values staged
-    StageInfo info[kMaxSlots];
-    double red[kConsumerGroups][kGroupWarps][3];
-    double scan_d[kConsumerGroups][kGroupWarps];
-    float scan_f[kConsumerGroups][kGroupWarps];
-    int32_t scan_flag[kConsumerGroups][kGroupWarps];
-    int32_t giter[kSmemGraphs];
-    int32_t gdone[kSmemGraphs];
-    int32_t abort_flag;
-    int32_t idle;
-    int32_t last;
+// ---- the sweep kernel ---------------------------------------------------------------
+// What a warp needs of the graph it works on; kept in shared memory so that the
+// tile loop keeps its registers for data in flight.
+struct WarpCtx {
+    SweepView W;
+    const int32_t* cols;
+    const float* w;
+    const uint32_t* tile_bits;
+    const int32_t* tile_row;
+    const float* zsrc;      // carried values read by this sweep
+    const float* hub_g;     // their hub copy (global)
+    const double* z64;
+    const int32_t* hub_ids;
+    int32_t graph;
+    int32_t iter;
 };
-
-__device__ __forceinline__ Chunk shfl_chunk(const Chunk& a, int src) {
-    Chunk b;
-    const int32_t* pa = reinterpret_cast<const int32_t*>(&a);
-    int32_t* pb = reinterpret_cast<int32_t*>(&b);
-#pragma unroll
-    for (int i = 0; i < (int)(sizeof(Chunk) / 4); ++i) pb[i] = __shfl_sync(kFull, pa[i], src);
-    return b;
-}
 
 __device__ __forceinline__ Chunk load_chunk(const Chunk* p) {
     const int4* q = reinterpret_cast<const int4*>(p);
@@ -384,373 +287,150 @@ __device__ __forceinline__ Chunk load_chunk(const Chunk* p) {
     return c;
 }
 
-template <bool kFinal>
-__device__ void run_producer(const SweepParams& P, CtaShared& S, unsigned char* stages, float* hub_smem) {
-    const int lane = threadIdx.x & 31;
-    const StageLayout& L = P.lay;
-    const uint32_t nslots = (uint32_t)L.slots;
-    volatile int32_t* abort_flag = &S.abort_flag;
-    if (L.hub_count > 0 && lane == 0) {
-        const uint32_t bytes = (uint32_t)L.hub_count * (uint32_t)sizeof(float);
-        const float* src = P.graphs[0].hubz[S.giter[0] & 1];
-        mbar_arrive_tx(&S.bar_hub, bytes);
-        for (uint32_t off = 0; off < bytes; off += kCopyPiece)
-            bulk_load(reinterpret_cast<unsigned char*>(hub_smem) + off, reinterpret_cast<const unsigned char*>(src) + off,
-                      min(kCopyPiece, bytes - off), &S.bar_hub);
-    }
-    // Claims run one batch ahead: the queue position of the next batch and its
-    // stage records are in flight while the current batch is issued.
-    int32_t base_next = 0, base_after = P.nchunks;
-    if (lane == 0) base_next = (int32_t)atomicAdd(&P.ctl->queue, (uint32_t)kClaim);
-    base_next = __shfl_sync(kFull, base_next, 0);
-    if (lane == 0 && base_next < P.nchunks) base_after = (int32_t)atomicAdd(&P.ctl->queue, (uint32_t)kClaim);
-    Chunk nk{};
-    if (lane < kClaim && base_next + lane < P.nchunks) nk = load_chunk(P.chunks + base_next + lane);
-    uint32_t q = 0;
-    bool abort = false;
-    // lane 0's cache of the current graph's arrays
-    int32_t cg = -1, citer = -1;
-    const int32_t* in_col = nullptr;
-    const float* in_w = nullptr;
-    const int32_t* in_row = nullptr;
-    const float* xin = nullptr;
-    const float* scale = nullptr;
-    const int32_t* hslot = nullptr;
-    while (!abort) {
-        const int32_t base = base_next;
-        if (base >= P.nchunks) break;
-        const Chunk cur = nk;
-        base_next = __shfl_sync(kFull, base_after, 0);
-        if (lane == 0)
-            base_after = base_next < P.nchunks ? (int32_t)atomicAdd(&P.ctl->queue, (uint32_t)kClaim) : P.nchunks;
-        if (lane < kClaim && base_next + lane < P.nchunks) nk = load_chunk(P.chunks + base_next + lane);
-        for (int i = 0; i < kClaim; ++i) {
-            const int32_t c = base + i;
-            if (c >= P.nchunks) break;
-            const Chunk ck = shfl_chunk(cur, i);
-            const int32_t gi = ck.graph;
-            const int32_t iter = gi < kSmemGraphs ? S.giter[gi] : ldcg(&P.states[gi].iter);
-            if (!kFinal && (gi < kSmemGraphs ? S.gdone[gi] : ldcg(&P.states[gi].done))) continue;
-            const uint32_t slot = q % nslots, round = q / nslots;
-            if (round > 0 && !wait_bar(&S.bar_empty[slot], (round - 1) & 1u, abort_flag, P.ctl)) {
-                abort = true;
-                break;
-            }
-            if (lane == 0) {
-                if (gi != cg || iter != citer) {
-                    const GraphDev& G = P.graphs[gi];
-                    in_col = G.in_col;
-                    in_w = G.in_w;
-                    in_row = G.in_row;
-                    xin = kFinal ? G.x[(iter - 1) & 1] : G.x[iter & 1];
-                    scale = G.scale;
-                    hslot = G.hub_slot;
-                    cg = gi;
-                    citer = iter;
-                }
-                StageInfo& in = S.info[slot];
-                in.ck = ck;
-                in.c = c;
-                in.iter = iter;
-                unsigned char* sp = stages + (size_t)slot * (size_t)L.slot_bytes;
-                const int32_t e0 = ck.nnz_begin, e1 = ck.nnz_end;
-                const int32_t eb = e0 & ~3;
-                const uint32_t ebytes = e1 > e0 ? (uint32_t)(((e1 + 3) & ~3) - eb) * 4u : 0u;
-                const int32_t ra = ck.sub_begin, nr = ck.sub_end - ck.sub_begin;
-                const int32_t rb = ra & ~3;
-                const uint32_t pbytes = nr > 0 ? (uint32_t)(((ra + nr + 1 + 3) & ~3) - rb) * 4u : 0u;
-                const uint32_t xbytes = nr > 0 ? (uint32_t)(((ra + nr + 3) & ~3) - rb) * 4u : 0u;
-                const uint32_t tx = ebytes * (in_w ? 2u : 1u) + pbytes + xbytes * (kFinal ? 1u : 3u);
-                mbar_arrive_tx(&S.bar_full[slot], tx);
-                if (ebytes) {
-                    bulk_load(sp + L.off_col, in_col + eb, ebytes, &S.bar_full[slot]);
-                    if (in_w) bulk_load(sp + L.off_w, in_w + eb, ebytes, &S.bar_full[slot]);
-                }
-                if (nr > 0) {
-                    bulk_load(sp + L.off_rowptr, in_row + rb, pbytes, &S.bar_full[slot]);
-                    bulk_load(sp + L.off_xin, xin + rb, xbytes, &S.bar_full[slot]);
-                    if (!kFinal) {
-                        bulk_load(sp + L.off_scale, scale + rb, xbytes, &S.bar_full[slot]);
-                        bulk_load(sp + L.off_hslot, hslot + rb, xbytes, &S.bar_full[slot]);
-                    }
-                }
-            }
-            __syncwarp();
-            ++q;
-        }
-    }
-    // One end marker per consumer group (the gatherers stop at the first).
-    for (int k = 0; k < kConsumerGroups && !abort; ++k) {
-        const uint32_t slot = q % nslots, round = q / nslots;
-        if (round > 0 && !wait_bar(&S.bar_empty[slot], (round - 1) & 1u, abort_flag, P.ctl)) {
-            abort = true;
-            break;
-        }
-        if (lane == 0) {
-            S.info[slot].c = -1;
-            mbar_arrive(&S.bar_full[slot]);
-        }
-        __syncwarp();
-        ++q;
-    }
-    if (abort && lane == 0) {
-        // Leave no bulk copy in flight into this CTA's shared memory.
-        const uint32_t first = q > nslots ? q - nslots : 0u;
-        for (uint32_t k = first; k < q; ++k) {
-            const unsigned long long t0 = global_ns();
-            while (!mbar_try(&S.bar_full[k % nslots], (k / nslots) & 1u) && global_ns() - t0 < kWaitNs) {
-            }
-        }
-        if (L.hub_count > 0) {
-            const unsigned long long t0 = global_ns();
-            while (!mbar_try(&S.bar_hub, 0u) && global_ns() - t0 < kWaitNs) {
-            }
-        }
-    }
-}
-
-template <bool kFinal>
-__device__ void run_gatherer(const SweepParams& P, CtaShared& S, unsigned char* stages, const float* hub_smem) {
-    constexpr int kPer = kStageEntries / kGatherThreads;  // entries per gatherer thread and stage
-    const int j = threadIdx.x - 32;                       // 0 .. kGatherThreads-1
-    const StageLayout& L = P.lay;
-    const uint32_t nslots = (uint32_t)L.slots;
-    volatile int32_t* abort_flag = &S.abort_flag;
-    bool ok = L.hub_count > 0 ? wait_bar(&S.bar_hub, 0u, abort_flag, P.ctl) : true;
-    int32_t cg = -1, citer = -1;
-    const float* zsrc = nullptr;
-    const float* hub_g = nullptr;
-    const double* z64 = nullptr;
-    const int32_t* hub_ids = nullptr;
-    uint32_t q = 0;
-    for (; ok; ++q) {
-        const uint32_t slot = q % nslots, round = q / nslots;
-        if (!wait_bar(&S.bar_full[slot], round & 1u, abort_flag, P.ctl)) break;
-        const StageInfo& in = S.info[slot];
-        if (in.c < 0) break;
-        const int32_t gi = in.ck.graph, iter = in.iter;
-        if (gi != cg || iter != citer) {
-            const GraphDev& G = P.graphs[gi];
-            zsrc = G.z[iter & 1];
-            hub_g = G.hubz[iter & 1];
-            z64 = G.z64;
-            hub_ids = G.hub_ids;
-            cg = gi;
-            citer = iter;
-        }
-        unsigned char* sp = stages + (size_t)slot * (size_t)L.slot_bytes;
-        int32_t* col = reinterpret_cast<int32_t*>(sp + L.off_col);
-        double* v64 = reinterpret_cast<double*>(sp + L.off_val64);
-        const int32_t eb = in.ck.nnz_begin & ~3;
-        const int32_t lo = in.ck.nnz_begin - eb, hi = in.ck.nnz_end - eb;
-        // Consecutive threads take consecutive entries: conflict-free shared
-        // memory on both the source read and the value write.
-        int32_t cv[kPer];
-#pragma unroll
-        for (int i = 0; i < kPer; ++i) cv[i] = col[j + i * kGatherThreads];
-#pragma unroll
-        for (int i = 0; i < kPer; ++i) {
-            const int k = j + i * kGatherThreads;
-            if (k < lo || k >= hi) continue;
-            const int32_t s = cv[i];
-            if (!kFinal) {
-                if (s >= 0) {
-                    cp_async4(col + k, zsrc + s);
-                } else {
-                    const int32_t h = -s - 1;
-                    if (h < L.hub_count) reinterpret_cast<float*>(col)[k] = hub_smem[h];
-                    else cp_async4(col + k, hub_g + h);
-                }
-            } else {
-                const int32_t idx = s >= 0 ? s : __ldg(hub_ids + (-s - 1));
-                cp_async8(v64 + k, z64 + idx);
-            }
-        }
-        cp_async_commit();
-        // Stage q - kGatherLag has landed: hand it to the consumers.
-        if (q >= (uint32_t)kGatherLag) {
-            cp_async_wait_group<kGatherLag>();
-            mbar_arrive(&S.bar_gath[(q - kGatherLag) % nslots]);
-        }
-    }
-    cp_async_wait_all();
-    for (uint32_t p = q > (uint32_t)kGatherLag ? q - kGatherLag : 0u; p < q; ++p) mbar_arrive(&S.bar_gath[p % nslots]);
+// Sources, mark bits and first-mark row of warp tile t (entries T .. T+255).
+__device__ __forceinline__ void fetch_tile(const WarpCtx& X, int32_t t, int32_t T, int lane, int4& ca, int4& cb,
+                                           uint32_t& bits, int32_t& row) {
+    const int4* c4 = reinterpret_cast<const int4*>(X.cols) + (T >> 2) + 2 * lane;
+    ca = __ldcs(c4);
+    cb = __ldcs(c4 + 1);
+    bits = (__ldcs(X.tile_bits + (size_t)t * (kTileItems / 32) + (lane >> 2)) >> (8 * (lane & 3))) & 0xffu;
+    row = __ldcs(X.tile_row + t);
 }
 
 template <typename Real>
-__device__ __forceinline__ void scan_store(CtaShared& S, int g, int w, Real v);
-template <>
-__device__ __forceinline__ void scan_store<float>(CtaShared& S, int g, int w, float v) { S.scan_f[g][w] = v; }
-template <>
-__device__ __forceinline__ void scan_store<double>(CtaShared& S, int g, int w, double v) { S.scan_d[g][w] = v; }
-template <typename Real>
-__device__ __forceinline__ Real scan_load(const CtaShared& S, int g, int w);
-template <>
-__device__ __forceinline__ float scan_load<float>(const CtaShared& S, int g, int w) { return S.scan_f[g][w]; }
-template <>
-__device__ __forceinline__ double scan_load<double>(const CtaShared& S, int g, int w) { return S.scan_d[g][w]; }
-
-template <typename Real>
-__device__ void run_consumer(const SweepParams& P, CtaShared& S, unsigned char* stages) {
+__device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, const WarpCtx& X,
+                              const float* hub_s, int32_t hub_count, Real* scr) {
     constexpr bool kFinal = std::is_same<Real, double>::value;
-    const int gt = threadIdx.x - 32 * (1 + kGatherWarps);
-    const int g = gt / kGroupThreads, t = gt % kGroupThreads;
-    const int w = t >> 5, lane = t & 31;
-    const int bar_id = 1 + g;
-    const StageLayout& L = P.lay;
-    const uint32_t nslots = (uint32_t)L.slots;
-    volatile int32_t* abort_flag = &S.abort_flag;
-    int32_t cg = -1, citer = -1;
-    SweepView W{};
-    const int k0 = kLaneItems * t;
-    for (uint32_t q = (uint32_t)g;; q += kConsumerGroups) {
-        const uint32_t slot = q % nslots, round = q / nslots;
-        const bool ok = wait_bar(&S.bar_full[slot], round & 1u, abort_flag, P.ctl);
-        StageInfo in;
-        in.c = -1;
-        if (ok) in = S.info[slot];
-        if (group_any(bar_id, !ok || in.c < 0)) break;
-        if (in.ck.graph != cg || in.iter != citer) {
-            cg = in.ck.graph;
-            citer = in.iter;
-            W = make_view<kFinal>(P.graphs[cg], P.states + cg, citer);
-        }
-        unsigned char* sp = stages + (size_t)slot * (size_t)L.slot_bytes;
-        const int32_t e0 = in.ck.nnz_begin, e1 = in.ck.nnz_end;
-        const int32_t eb = e0 & ~3, lo = e0 - eb, hi = e1 - eb;
-        const int32_t ra = in.ck.sub_begin, nr = in.ck.sub_end - in.ck.sub_begin, ro = ra & 3;
-        const int32_t* rowp = reinterpret_cast<const int32_t*>(sp + L.off_rowptr) + ro;
-        uint8_t* mark = sp + L.off_mark;
-        // 1. mark the last entry of every row that ends in this stage
-        for (int j = t; j < nr; j += kGroupThreads) {
-            const int32_t rs = rowp[j], re = rowp[j + 1];
-            if (re <= e1 && re > max(rs, e0)) mark[re - 1 - eb] = 1;
-        }
-        const bool ok2 = wait_bar(&S.bar_gath[slot], round & 1u, abort_flag, P.ctl);
-        if (group_any(bar_id, !ok2)) break;
-        // 2. per-thread segmented sums over entries k0 .. k0+7; row sums are
-        //    written in place at the row's last entry
-        Real* rsum = kFinal ? reinterpret_cast<Real*>(sp + L.off_val64) : reinterpret_cast<Real*>(sp + L.off_col);
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int32_t kb = ck.nnz_begin, ke = ck.nnz_end, T0 = kb & ~7;
+    const int32_t fl = ck.flags;
+    bool head_pending = (fl & kHasHead) && !(fl & kInterior);
+    double head_val = 0.0;
+    double err = 0.0, dsum = 0.0, xsum = 0.0;
+    Real carry = Real(0);  // the row still open at the end of the previous tile
+    int4 ca, cb;
+    uint32_t bits;
+    int32_t row;
+    fetch_tile(X, ck.sub_begin, T0, lane, ca, cb, bits, row);
+    for (int32_t t = ck.sub_begin; t < ck.sub_end; ++t) {
+        const int32_t T = T0 + (t - ck.sub_begin) * kTileItems;
+        const int32_t cc[kLaneItems] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+        const uint32_t mb = bits;
+        const int32_t r0 = row;
+        if (t + 1 < ck.sub_end) fetch_tile(X, t + 1, T + kTileItems, lane, ca, cb, bits, row);
+        // 1. gathers of this tile's entries
+        const int32_t p0 = T + kLaneItems * lane;
         Real v[kLaneItems];
-        if (!kFinal) {
-            const float4 a = *reinterpret_cast<const float4*>(sp + L.off_col + 4 * k0);
-            const float4 b = *reinterpret_cast<const float4*>(sp + L.off_col + 4 * k0 + 16);
-            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-            v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-        } else {
-#pragma unroll
-            for (int u = 0; u < kLaneItems; u += 2) {
-                const double2 d = *reinterpret_cast<const double2*>(sp + L.off_val64 + 8 * (k0 + u));
-                v[u] = (Real)d.x;
-                v[u + 1] = (Real)d.y;
-            }
-        }
-        if (W.weighted) {
-            const float4 a = *reinterpret_cast<const float4*>(sp + L.off_w + 4 * k0);
-            const float4 b = *reinterpret_cast<const float4*>(sp + L.off_w + 4 * k0 + 16);
-            v[0] *= (Real)a.x; v[1] *= (Real)a.y; v[2] *= (Real)a.z; v[3] *= (Real)a.w;
-            v[4] *= (Real)b.x; v[5] *= (Real)b.y; v[6] *= (Real)b.z; v[7] *= (Real)b.w;
-        }
-        const uint2 mk = *reinterpret_cast<const uint2*>(mark + k0);
-        Real acc = Real(0), head_part = Real(0);
-        int first = -1;
 #pragma unroll
         for (int u = 0; u < kLaneItems; ++u) {
-            const int k = k0 + u;
-            if (k >= lo && k < hi) acc += v[u];
-            const uint32_t m = ((u < 4 ? mk.x : mk.y) >> (8 * (u & 3))) & 1u;
-            if (m) {
+            const int32_t p = p0 + u;
+            const int32_t s = cc[u];
+            Real x = Real(0);
+            if (p >= kb && p < ke) {
+                if (kFinal) {
+                    x = X.z64[s >= 0 ? s : __ldg(X.hub_ids + (-s - 1))];
+                } else {
+                    const int32_t h = -s - 1;
+                    x = s >= 0 ? X.zsrc[s] : (h < hub_count ? hub_s[h] : X.hub_g[h]);
+                }
+            }
+            v[u] = x;
+        }
+        if (X.w) {
+            const float4* w4 = reinterpret_cast<const float4*>(X.w) + (T >> 2) + 2 * lane;
+            const float4 wa = __ldcs(w4), wb = __ldcs(w4 + 1);
+            v[0] *= (Real)wa.x; v[1] *= (Real)wa.y; v[2] *= (Real)wa.z; v[3] *= (Real)wa.w;
+            v[4] *= (Real)wb.x; v[5] *= (Real)wb.y; v[6] *= (Real)wb.z; v[7] *= (Real)wb.w;
+        }
+        // 2. mark ordinals: pre = marks of lower lanes, nm = marks of the tile
+        int32_t pre = 0, nm = 0;
+#pragma unroll
+        for (int b = 0; b < kLaneItems; ++b) {
+            const unsigned bb = __ballot_sync(kFull, (mb >> b) & 1u);
+            pre += __popc(bb & lt);
+            nm += __popc(bb);
+        }
+        // the rows this lane finishes first: request their data now
+        float xin0 = 0.f, sc0 = 0.f;
+        int32_t hs0 = -1;
+        if (lane < nm) {
+            const int32_t v0 = r0 + lane;
+            xin0 = X.W.xin[v0];
+            if (!kFinal) {
+                sc0 = X.W.scale[v0];
+                hs0 = X.W.hub_slot[v0];
+            }
+        }
+        // 3. per-lane segment sums; row values by mark ordinal
+        Real acc = Real(0), head_part = Real(0);
+        int first = -1, k = pre;
+#pragma unroll
+        for (int u = 0; u < kLaneItems; ++u) {
+            acc += v[u];
+            if ((mb >> u) & 1u) {
                 if (first < 0) {
                     first = u;
                     head_part = acc;
                 } else {
-                    rsum[k] = acc;
+                    scr[k] = acc;
                 }
+                ++k;
                 acc = Real(0);
             }
         }
-        // 3. segmented scan over the group: (open sum, has a row end)
-        Real sa = acc;
-        int fa = first >= 0 ? 1 : 0;
+        if (lane == 0) {
+            if (first >= 0) head_part = carry + head_part;
+            else acc = carry + acc;
+        }
+        // 4. segmented inclusive scan of the open sums; a lane's segment starts
+        //    at the nearest marked lane at or below it
+        const unsigned mm = __ballot_sync(kFull, first >= 0);
+        const unsigned le = mm & (lt | (1u << lane));
+        const int sl = le ? 31 - __clz(le) : 0;
+        Real S = acc;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const Real us = __shfl_up_sync(kFull, sa, o);
-            const int uf = __shfl_up_sync(kFull, fa, o);
-            if (lane >= o) {
-                if (!fa) sa += us;
-                fa |= uf;
-            }
+            const Real up = __shfl_up_sync(kFull, S, o);
+            if (lane - o >= sl) S += up;
         }
-        Real ex = __shfl_up_sync(kFull, sa, 1);
-        int exf = __shfl_up_sync(kFull, fa, 1);
-        if (lane == 0) {
-            ex = Real(0);
-            exf = 0;
-        }
-        if (lane == 31) {
-            scan_store<Real>(S, g, w, sa);
-            S.scan_flag[g][w] = fa;
-        }
-        group_sync(bar_id);
-        Real cw = Real(0);
-        if (!exf) {
-            for (int w2 = w - 1; w2 >= 0; --w2) {
-                cw += scan_load<Real>(S, g, w2);
-                if (S.scan_flag[g][w2]) break;
-            }
-        }
-        Real tail_val = Real(0);  // the row still open at the end of the stage
-        if (t == 0) {
-            for (int w2 = kGroupWarps - 1; w2 >= 0; --w2) {
-                tail_val += scan_load<Real>(S, g, w2);
-                if (S.scan_flag[g][w2]) break;
-            }
-        }
-        if (first >= 0) rsum[k0 + first] = (exf ? ex : cw + ex) + head_part;
-        group_sync(bar_id);
-        // 4. finish the rows of the stage (not its head row begun in an earlier
-        //    stage, nor its tail row that continues)
-        const int32_t flags = in.ck.flags;
-        const int j_lo = (flags & kHasHead) ? 1 : 0;
-        const int j_hi = nr - ((flags & kHasTail) ? 1 : 0);
-        const float* xin_s = reinterpret_cast<const float*>(sp + L.off_xin) + ro;
-        const float* sc_s = reinterpret_cast<const float*>(sp + L.off_scale) + ro;
-        const int32_t* hs_s = reinterpret_cast<const int32_t*>(sp + L.off_hslot) + ro;
-        double err = 0.0, dsum = 0.0, xsum = 0.0;
-        for (int j = j_lo + t; j < j_hi; j += kGroupThreads) {
-            const int32_t rs = rowp[j], re = rowp[j + 1];
-            const Real sum = re > rs ? rsum[re - 1 - eb] : Real(0);
-            finish_row<kFinal>(W, ra + j, (double)sum, xin_s[j], kFinal ? 0.f : sc_s[j], kFinal ? -1 : hs_s[j], err,
-                               dsum, xsum);
-        }
-        Real head_val = Real(0);
-        if (t == 0 && (flags & kHasHead) && !(flags & kInterior)) head_val = rsum[rowp[1] - 1 - eb];
-        *reinterpret_cast<uint2*>(mark + k0) = make_uint2(0u, 0u);
-        err = warp_sum(err);
-        dsum = warp_sum(dsum);
-        xsum = warp_sum(xsum);
-        if (lane == 0) {
-            S.red[g][w][0] = err;
-            S.red[g][w][1] = dsum;
-            S.red[g][w][2] = xsum;
-        }
-        fence_proxy_async();
+        const Real below = __shfl_up_sync(kFull, S, 1);
+        if (first >= 0) scr[pre] = lane == 0 ? head_part : below + head_part;
+        carry = __shfl_sync(kFull, S, 31);
         __syncwarp();
-        if (lane == 0) mbar_arrive(&S.bar_empty[slot]);
-        group_sync(bar_id);
-        if (w == 0) {
-            double e = 0.0, d = 0.0, x = 0.0;
-            if (lane < kGroupWarps) {
-                e = S.red[g][lane][0];
-                d = S.red[g][lane][1];
-                x = S.red[g][lane][2];
+        // 5. finish the tile's rows; the chunk's first mark ends its head row
+        //    (cut before the chunk), whose piece goes to the span instead
+        for (int32_t j = lane; j < nm; j += 32) {
+            const Real val = scr[j];
+            const int32_t v0 = r0 + j;
+            float xi = xin0, sc = sc0;
+            int32_t hs = hs0;
+            if (j >= 32) {
+                xi = X.W.xin[v0];
+                if (!kFinal) {
+                    sc = X.W.scale[v0];
+                    hs = X.W.hub_slot[v0];
+                }
             }
-            e = warp_sum(e);
-            d = warp_sum(d);
-            x = warp_sum(x);
-            if (lane == 0)
-                stage_accumulate(P, in.c, in.ck, 2 * (int32_t)blockIdx.x + g, e, d, x, (double)head_val,
-                                 (double)tail_val);
+            if (head_pending && j == 0) head_val = (double)val;
+            else finish_row<kFinal>(X.W, v0, (double)val, xi, sc, hs, err, dsum, xsum);
+        }
+        if (nm > 0) head_pending = false;
+        __syncwarp();
+    }
+    err = warp_sum(err);
+    dsum = warp_sum(dsum);
+    xsum = warp_sum(xsum);
+    if (lane == 0) {
+        unsigned long long* a = acc_slot(P, ck.graph, (int32_t)(blockIdx.x * kCtaWarps + (threadIdx.x >> 5)));
+        fx_add(a, err);
+        fx_add(a + 2, dsum);
+        fx_add(a + 4, xsum);
+        if (fl & kInterior) {
+            fx_add(P.span_acc + 2 * ck.head_ta, (double)carry);
+        } else {
+            if (fl & kHasHead) fx_add(P.span_acc + 2 * ck.head_ta, head_val);
+            if (fl & kHasTail) fx_add(P.span_acc + 2 * c, (double)carry);
         }
     }
 }
@@ -759,45 +439,95 @@ template <typename Real>
 __global__ void __launch_bounds__(kCtaThreads, 1) k_sweep(SweepParams P) {
     constexpr bool kFinal = std::is_same<Real, double>::value;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(16) CtaShared S;
-    float* hub_smem = reinterpret_cast<float*>(smem);
-    unsigned char* stages = smem + P.lay.hub_bytes;
-    const int warp = threadIdx.x >> 5;
+    __shared__ __align__(8) uint64_t bar_hub;
+    __shared__ WarpCtx ctx[kCtaWarps];
+    __shared__ int32_t s_idle, s_abort, s_last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int32_t hub_count = kFinal ? 0 : P.hub_count;
+    const size_t hub_bytes = ((size_t)hub_count * sizeof(float) + 127) & ~(size_t)127;
+    float* hub_s = reinterpret_cast<float*>(smem);
+    Real* scr = reinterpret_cast<Real*>(smem + hub_bytes) + (size_t)warp * kTileItems;
     if (threadIdx.x == 0) {
-        S.abort_flag = 0;
-        S.idle = (!kFinal && ldcg(&P.ctl->active) <= 0) ? 1 : 0;  // one reading for the whole CTA
-        for (int i = 0; i < P.lay.slots; ++i) {
-            mbar_init(&S.bar_full[i], 1);
-            mbar_init(&S.bar_gath[i], kGatherThreads);
-            mbar_init(&S.bar_empty[i], kGroupWarps);
+        s_abort = 0;
+        s_last = 0;
+        s_idle = (!kFinal && ldcg(&P.ctl->active) <= 0) ? 1 : 0;  // one reading for the whole CTA
+        if (!s_idle && hub_count > 0) {
+            // Stage graph 0's hub values for this launch's parity.  A CTA that
+            // reads the next parity can only do so after every chunk was taken,
+            // so it gets no work.
+            mbar_init(&bar_hub, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            const uint32_t bytes = (uint32_t)hub_count * (uint32_t)sizeof(float);
+            const float* src = P.graphs[0].hubz[ldcg(&P.states[0].iter) & 1];
+            mbar_arrive_tx(&bar_hub, bytes);
+            for (uint32_t off = 0; off < bytes; off += kCopyPiece)
+                bulk_load(reinterpret_cast<unsigned char*>(hub_s) + off, reinterpret_cast<const unsigned char*>(src) + off,
+                          min(kCopyPiece, bytes - off), &bar_hub);
         }
-        mbar_init(&S.bar_hub, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    for (int i = threadIdx.x; i < min(P.ngraphs, kSmemGraphs); i += kCtaThreads) {
-        S.giter[i] = ldcg(&P.states[i].iter);
-        S.gdone[i] = ldcg(&P.states[i].done);
-    }
-    for (int i = threadIdx.x; i < P.lay.slots * (kStageEntries / 16); i += kCtaThreads) {
-        const int slot = i / (kStageEntries / 16), piece = i % (kStageEntries / 16);
-        *reinterpret_cast<uint4*>(stages + (size_t)slot * P.lay.slot_bytes + P.lay.off_mark + 16 * piece) =
-            make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
-    if (!S.idle) {
-        if (warp == 0) run_producer<kFinal>(P, S, stages, hub_smem);
-        else if (warp <= kGatherWarps) run_gatherer<kFinal>(P, S, stages, hub_smem);
-        else run_consumer<Real>(P, S, stages);
+    if (!s_idle && hub_count > 0) {
+        bool ok = mbar_try(&bar_hub, 0u);
+        if (!ok) {
+            const unsigned long long t0 = global_ns();
+            while (!(ok = mbar_try(&bar_hub, 0u)) && global_ns() - t0 < kWaitNs) {
+            }
+        }
+        if (!ok) atomicExch(&s_abort, 1);
+        __syncthreads();
+        if (s_abort && threadIdx.x == 0) {
+            atomicExch(&P.ctl->error, EGPR_TIMEOUT);
+            // leave no copy in flight into this CTA's shared memory
+            const unsigned long long t0 = global_ns();
+            while (!mbar_try(&bar_hub, 0u) && global_ns() - t0 < kWaitNs) {
+            }
+        }
+    }
+    if (!s_idle && !s_abort) {
+        WarpCtx& X = ctx[warp];
+        if (lane == 0) X.graph = -1;
+        __syncwarp();
+        uint32_t nxt = 0;
+        if (lane == 0) nxt = atomicAdd(&P.ctl->queue, 1u);
+        for (;;) {
+            const int32_t c = (int32_t)__shfl_sync(kFull, nxt, 0);
+            if (c >= P.nchunks) break;
+            if (lane == 0) nxt = atomicAdd(&P.ctl->queue, 1u);  // the next claim, in flight meanwhile
+            const Chunk ck = load_chunk(P.chunks + c);
+            const int32_t gi = ck.graph;
+            GraphState* st = P.states + gi;
+            const int32_t iter = ldcg(&st->iter);
+            if (!kFinal && ldcg(&st->done)) continue;  // frozen graph (same answer for the whole warp)
+            if (gi != X.graph || iter != X.iter) {
+                __syncwarp();
+                if (lane == 0) {
+                    const GraphDev& G = P.graphs[gi];
+                    X.W = make_view<kFinal>(G, st, iter);
+                    X.cols = G.cols;
+                    X.w = G.w;
+                    X.tile_bits = G.tile_bits;
+                    X.tile_row = G.tile_row;
+                    X.zsrc = G.z[iter & 1];
+                    X.hub_g = G.hubz[iter & 1];
+                    X.z64 = G.z64;
+                    X.hub_ids = G.hub_ids;
+                    X.graph = gi;
+                    X.iter = iter;
+                }
+                __syncwarp();
+            }
+            process_chunk<Real>(P, c, ck, X, hub_s, hub_count, scr);
+        }
     }
     __threadfence();  // this CTA's accumulator updates before its exit is counted
     __syncthreads();
     if (threadIdx.x == 0) {
         const uint32_t prev = atomicAdd(&P.ctl->exited, 1u);
-        S.last = prev == gridDim.x - 1 ? 1 : 0;
+        s_last = prev == gridDim.x - 1 ? 1 : 0;
     }
     __syncthreads();
-    if (!S.last) return;
-    // Last CTA out: every stage of this launch is done.
+    if (!s_last) return;
+    // Last CTA out: every chunk of this launch is done.
     __threadfence();
     launch_tail<kFinal>(P);
     if (threadIdx.x == 0) {
@@ -918,9 +648,10 @@ int env_int(const char* name, int dflt, int lo, int hi) {
     return x >= lo && x <= hi ? x : dflt;
 }
 
-// Dynamic shared memory a sweep launch may use on the current device (and the
-// kernel's opt-in to it).
-int smem_budget(int mode) {
+// Dynamic shared memory of a sweep launch: the staged hub values (FP32 sweeps of
+// one graph) and one tile of row values per warp.  The kernel opts in to the
+// device's limit once per device.
+int smem_optin(int mode) {
     static int cache[2][64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -942,43 +673,10 @@ int smem_budget(int mode) {
     return c;
 }
 
-// Stage buffer layout and ring depth.  FP32 sweeps of one graph stage up to
-// kHubCap hub values; the ring keeps EGPR_SLOTS buffers (default 4) and the hub
-// copy takes what is left.
-StageLayout make_layout(int mode, bool weighted, int32_t nhub) {
-    StageLayout L = {};
-    int off = 0;
-    auto take = [&](int bytes) {
-        const int o = off;
-        off += (bytes + 127) & ~127;
-        return o;
-    };
-    L.off_col = take(kStageEntries * 4);
-    L.off_val64 = mode ? take(kStageEntries * 8) : 0;
-    L.off_w = weighted ? take(kStageEntries * 4) : 0;
-    L.off_mark = take(kStageEntries);
-    L.off_rowptr = take(kStageRows * 4);
-    L.off_xin = take(kStageRows * 4);
-    L.off_scale = mode ? 0 : take(kStageRows * 4);
-    L.off_hslot = mode ? 0 : take(kStageRows * 4);
-    L.slot_bytes = off;
-    const int budget = smem_budget(mode);
-    // A gatherer signals stage q only after issuing stage q + kGatherLag, so the
-    // ring holds at least kGatherLag + 1 buffers.
-    const int min_slots = kGatherLag + 1;
-    const int max_slots = std::max(min_slots, std::min(kMaxSlots, budget / L.slot_bytes));
-    L.slots = std::max(min_slots, std::min(max_slots, env_int("EGPR_SLOTS", mode == 0 && nhub > 0 ? 4 : max_slots,
-                                                                 2, kMaxSlots)));
-    int32_t hubs = 0;
-    if (mode == 0 && nhub > 0) {
-        const int left = budget - L.slots * L.slot_bytes;
-        hubs = std::min<int32_t>(nhub, std::max(0, left) / 4) & ~31;
-        hubs = std::min<int32_t>(hubs, env_int("EGPR_HUB_SMEM", kHubCap, 0, kHubCap) & ~31);
-    }
-    L.hub_count = hubs;
-    L.hub_bytes = (hubs * 4 + 127) & ~127;
-    L.dyn_bytes = L.hub_bytes + L.slots * L.slot_bytes;
-    return L;
+size_t scratch_bytes(int mode) { return (size_t)kCtaWarps * kTileItems * (mode ? sizeof(double) : sizeof(float)); }
+
+size_t dyn_smem(int mode, int32_t hub_count) {
+    return (((size_t)hub_count * sizeof(float) + 127) & ~(size_t)127) + scratch_bytes(mode);
 }
 
 SweepParams make_params(Plan& plan, int mode, int use_cond) {
@@ -997,7 +695,16 @@ SweepParams make_params(Plan& plan, int mode, int use_cond) {
     P.cond = plan.cond;
     P.use_cond = use_cond;
     P.ngraphs = plan.ngraphs;
-    P.lay = make_layout(mode, plan.any_weighted != 0, plan.ngraphs == 1 ? plan.hub_count : 0);
+    smem_optin(mode);  // the kernel's opt-in to more than 48 KB of dynamic shared memory
+    int32_t hubs = 0;
+    if (mode == 0 && plan.ngraphs == 1) {
+        // all hub slots (the zero slot included) while they fit, and no more than
+        // EGPR_HUB_SMEM values (tuning)
+        const size_t room = (size_t)smem_optin(0) - scratch_bytes(0);
+        hubs = std::min<int32_t>(plan.hub_count, (int32_t)(room / sizeof(float)) & ~31);
+        hubs = std::min<int32_t>(hubs, env_int("EGPR_HUB_SMEM", kHubCap, 0, kHubCap) & ~31);
+    }
+    P.hub_count = hubs;
     return P;
 }
 
@@ -1027,6 +734,10 @@ cudaLaunchAttributeValue l2_window(const Plan& plan) {
 }
 
 }  // namespace
+
+int32_t hub_stride(int32_t nhub) { return (nhub + 1 + 31) & ~31; }
+
+int sweep_resident_warps() { return sweep_grid() * kCtaWarps; }
 
 // One persistent CTA per SM.
 int sweep_grid() {
@@ -1073,9 +784,10 @@ void plan_set_l2_window(Plan& plan, void* base, size_t bytes) {
 
 GraphDev graph_dev_view(const egpr_graph* g) {
     GraphDev d;
-    d.in_row = g->in_row.as<int32_t>();
-    d.in_col = g->in_col.as<int32_t>();
-    d.in_w = g->weighted ? g->in_w.as<float>() : nullptr;
+    d.cols = g->sw_col.as<int32_t>();
+    d.w = g->weighted ? g->sw_w.as<float>() : nullptr;
+    d.tile_bits = g->tile_bits.as<uint32_t>();
+    d.tile_row = g->tile_row.as<int32_t>();
     d.outw = g->outw.as<double>();
     d.scale = g->scale.as<float>();
     d.tele = g->tele.as<float>();
@@ -1088,7 +800,7 @@ GraphDev graph_dev_view(const egpr_graph* g) {
     d.hub_ids = g->hub_ids.as<int32_t>();
     d.hub_slot = g->hub_slot.as<int32_t>();
     d.hubz[0] = g->hubz.as<float>();
-    d.hubz[1] = g->hubz.as<float>() + std::max(g->nhub, 4);
+    d.hubz[1] = g->hubz.as<float>() + hub_stride(g->nhub);
     d.nhub = g->nhub;
     d.n = g->n;
     d.chunk_begin = d.chunk_end = 0;
@@ -1129,10 +841,10 @@ int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_
     plan.nspans = (int32_t)spans.size();
     plan.max_n = max_n;
     plan.any_weighted = any_w;
-    plan.hub_count = count == 1 ? graphs[0]->nhub : 0;
+    plan.hub_count = count == 1 ? hub_stride(graphs[0]->nhub) : 0;
     plan.grid = std::max(1, std::min(plan.nchunks, sweep_grid()));
-    // accumulator slots: up to one per (CTA, consumer group) for each graph
-    const int32_t per_graph = std::max(1, std::min(2 * plan.grid, 8192 / std::max(1, count)));
+    // accumulator slots: up to 512 per graph, fewer for many graphs
+    const int32_t per_graph = std::max(1, std::min(512, 8192 / std::max(1, count)));
     plan.nacc = per_graph * count;
     plan.h_chunks_all = all;
     if (spans.empty()) spans.push_back(0);
@@ -1182,7 +894,7 @@ int plan_capture_loop(Plan& plan, cudaStream_t stream) {
     kp.func = (void*)k_sweep<float>;
     kp.gridDim = dim3((unsigned)plan.grid);
     kp.blockDim = dim3(kCtaThreads);
-    kp.sharedMemBytes = (unsigned)P.lay.dyn_bytes;
+    kp.sharedMemBytes = (unsigned)dyn_smem(0, P.hub_count);
     kp.kernelParams = args;
     e = cudaGraphAddKernelNode(&knode, cp.conditional.phGraph_out[0], nullptr, 0, &kp);
     if (e != cudaSuccess) goto fail;
@@ -1230,7 +942,7 @@ int launch_loop(Plan& plan, int32_t max_iter, cudaStream_t stream, int32_t* laun
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)plan.grid);
     cfg.blockDim = dim3(kCtaThreads);
-    cfg.dynamicSmemBytes = (size_t)P.lay.dyn_bytes;
+    cfg.dynamicSmemBytes = dyn_smem(0, P.hub_count);
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     if (plan.l2_bytes > 0) {
@@ -1255,7 +967,7 @@ int launch_finish(Plan& plan, bool correction, cudaStream_t stream, int32_t* lau
                                                   plan.ngraphs);
         // The loop's last CTA left the queue reset; the control block keeps the sweep count.
         SweepParams P = make_params(plan, 1, 0);
-        k_sweep<double><<<plan.grid, kCtaThreads, (size_t)P.lay.dyn_bytes, stream>>>(P);
+        k_sweep<double><<<plan.grid, kCtaThreads, dyn_smem(1, 0), stream>>>(P);
         l += 2;
     }
     k_normalize<<<grid, kThreads, 0, stream>>>(plan.d_graphs.as<GraphDev>(), plan.d_states.as<GraphState>(),
