@@ -98,6 +98,9 @@ _SIGNATURES = [
     ("egpr_pagerank_csr", c_int,
      [c_void_p, c_int32, c_void_p, c_int64, c_void_p, c_uint64, c_double, c_int32, c_double, c_void_p,
       POINTER(c_double)]),
+    ("egpr_pagerank_device_noalloc", c_int,
+     [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int32, c_double, c_uint32, c_void_p,
+      c_void_p, POINTER(EgprStats)]),
     ("egpr_cache_stats_get", c_int, [POINTER(EgprCacheStats)]),
     ("egpr_cache_reset", c_int, []),
     ("egpr_cache_set_budget", c_int, [c_int64]),

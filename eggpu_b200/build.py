@@ -23,7 +23,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libegpr.so"
 SYNTH = PKG / "libegpr_synth.so"
 
-CUDA_SOURCES = ["prep.cu", "sweep.cu", "spmm.cu", "api.cu"]
+CUDA_SOURCES = ["prep.cu", "sweep.cu", "spmm.cu", "api.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "--expt-relaxed-constexpr"]

@@ -41,6 +41,8 @@ static int fail_arg(const char* why) {
     return EGPR_INVALID_ARGUMENT;
 }
 
+int arg_error(const char* why) { return fail_arg(why); }
+
 double wall_seconds() {
     using clock = std::chrono::steady_clock;
     return std::chrono::duration<double>(clock::now().time_since_epoch()).count();

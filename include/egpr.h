@@ -202,6 +202,34 @@ EGPR_API int egpr_pagerank_csr(const int32_t* V, int32_t len_V, const int32_t* E
                       const double* W, uint64_t graph_id, double alpha, int32_t max_iter_num,
                       double threshold, double* PR, double* kernel_seconds);
 
+/* ---- solve without allocating --------------------------------------- */
+
+/*
+ * No counterpart in the reference.  PageRank for callers that may not call
+ * cudaMalloc: code inside a framework that owns all device memory through
+ * its own pool, a serving thread with a fixed memory budget, a plug-in whose
+ * host forbids allocations while a request runs.  The caller passes device
+ * pointers: the inbound CSR in_row[n+1] / in_col[nnz] (entries are source
+ * ids, as egpr_graph_export_inbound returns them), optional FP32 weights
+ * in_w[nnz] (NULL = unit weights), the FP64 out-weight sum of every source
+ * out_weight[n], and ranks[n] for the normalised FP64 result.  Same maths,
+ * stop rule and flags as egpr_pagerank (uniform teleport only).
+ *
+ * Nothing is allocated: the solve's buffers live in one fixed device array
+ * compiled into the library (4 MiB + 256 bytes, held on every GPU that loads
+ * the library until the process exits).  Hence the limit n <= 262144; a
+ * larger n returns EGPR_INVALID_ARGUMENT.  The first call on a device looks
+ * up that array's device address (make it before any stream capture).  Every
+ * call reuses the array, so calls that overlap on the GPU (other threads or
+ * other streams) race and give wrong results: serialise them.  Work is
+ * enqueued on `stream` (a cudaStream_t, NULL = default stream); with stats
+ * non-NULL the call waits for it and fills stats.
+ */
+EGPR_API int egpr_pagerank_device_noalloc(int32_t n, int64_t nnz, const int32_t* in_row, const int32_t* in_col,
+                                          const float* in_w, const double* out_weight, double alpha,
+                                          int32_t max_iter, double tol, uint32_t flags, double* ranks,
+                                          void* stream, egpr_stats* stats);
+
 /* Counters of the prepared-graph cache behind egpr_pagerank_csr. */
 EGPR_API int egpr_cache_stats_get(egpr_cache_stats* out);
 /* Drops every graph held by the egpr_pagerank_csr cache. */
