@@ -43,13 +43,16 @@ struct Chunk {
     int32_t pad2;
     int32_t nnz_begin;   // entries [nnz_begin, nnz_end) belong to the chunk
     int32_t nnz_end;
-    int32_t row_end;     // sweep stage: rows before row_end are finished by the stage
-    int32_t pad;
+    int32_t row_end;     // sweep chunk: rows before row_end are finished by the chunk
+    int32_t pad;         // sweep chunk: estimated cost (entries + a charge per row)
 };
 
 // The sweep's warp tiles: kTileItems entries, lane l owning entries 8l..8l+7.
 constexpr int kLaneItems = 8;
 constexpr int kTileItems = 32 * kLaneItems;
+// Per-tile words of the tile table: 8 words of row-end marks (one byte per
+// lane), then 8 words with, per lane, the marks of the lanes below it.
+constexpr int kTileWords = 16;
 // Hub cache: the carried values of the (up to kHubCap - 32) sources with the
 // largest out-degree are kept in shared memory by the sweep; inbound entries
 // from a hub store -(slot + 1) instead of the source id.  Slot nhub holds 0 and
@@ -60,7 +63,7 @@ constexpr int kHubCap = 32768;
 struct GraphDev {
     const int32_t* cols;        // sweep entries: hub-encoded sources, a placeholder in every empty row
     const float* w;             // their weights, NULL = unit weights
-    const uint32_t* tile_bits;  // per warp tile: kTileItems bits, set on entries that end a row
+    const uint32_t* tile_bits;  // per warp tile: kTileWords words (row-end marks, per-lane mark offsets)
     const int32_t* tile_row;    // per warp tile: the row its first mark ends
     const double* outw;      // n, FP64 out-weight sums
     const float* scale;      // n, alpha/outw (FP32) or -1 for dangling vertices
@@ -110,7 +113,7 @@ struct Ctl {
 constexpr int kAccWords = 8;  // words per accumulator slot (6 used; 64-byte slots)
 
 struct SweepParams {
-    const Chunk* chunks;
+    const Chunk* chunks;     // in queue order (costliest chunks of a graph first)
     int32_t nchunks;
     int32_t mode;            // 0 = FP32 sweep, 1 = FP64 correction sweep
     const GraphDev* graphs;

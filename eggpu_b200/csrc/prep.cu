@@ -436,8 +436,18 @@ namespace {
 int chunks_per_warp() {
     static const int v = [] {
         const char* e = std::getenv("EGPR_CHUNKS_PER_WARP");  // tuning: queue granularity
+        const int x = e ? std::atoi(e) : 8;
+        return x >= 1 && x <= 64 ? x : 8;
+    }();
+    return v;
+}
+
+// Cost of finishing one row, in entries (a row costs its entries plus this).
+int row_cost() {
+    static const int v = [] {
+        const char* e = std::getenv("EGPR_ROW_COST");  // tuning
         const int x = e ? std::atoi(e) : 4;
-        return x >= 1 && x <= 64 ? x : 4;
+        return x >= 0 && x <= 64 ? x : 4;
     }();
     return v;
 }
@@ -447,14 +457,16 @@ int chunks_per_warp() {
 // The sweep's work layout, by one host pass over in_row.
 //   * sw_row / sw_col / sw_w: the inbound CSR with a placeholder entry in every
 //     empty row, so that every row ends on an entry of its own;
-//   * chunks: consecutive rows packed while a chunk holds at most chunk_items
-//     entries; a longer row is cut (a span: its chunks add pieces to the span's
-//     accumulator and the sweep finishes the row when the launch ends), and
-//     every cut leaves at least one entry of the row on each side;
+//   * chunks: consecutive rows packed while a chunk's cost (entries plus
+//     row_cost() per row) stays under a cap sized for chunks_per_warp() chunks
+//     per resident warp; a longer row is cut (a span: its chunks add pieces to
+//     the span's accumulator and the sweep finishes the row when the launch
+//     ends), and every cut leaves at least one entry of the row on each side;
 //   * warp tiles: chunk c covers tiles of kTileItems entries from
 //     (start & ~7); per tile a 256-bit mask of the entries that end a row
-//     finished by the chunk, and the first such row (the k-th mark of a tile
-//     ends row tile_row + k, since every row has an entry).
+//     finished by the chunk, per lane the number of marks in the lanes below
+//     it, and the first such row (the k-th mark of a tile ends row
+//     tile_row + k, since every row has an entry).
 int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     const int32_t n = g->n;
     std::vector<int32_t> row((size_t)n + 1);
@@ -471,34 +483,39 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     for (size_t r = (size_t)n; r < sw.size(); ++r) sw[r] = (int32_t)acc;
     const int32_t nnz = (int32_t)acc;
     g->sw_nnz = nnz;
-    // chunks
+    // chunks of about equal cost (entries + row_cost() per row touched)
+    const int64_t R = row_cost();
     const int64_t warps = std::max(1, resident_warps);
-    int64_t target = ((int64_t)nnz + warps * chunks_per_warp() - 1) / (warps * chunks_per_warp());
-    target = std::max<int64_t>(kTileItems, (target + kTileItems - 1) / kTileItems * kTileItems);
-    const int32_t cap_e = (int32_t)std::min<int64_t>(target, 1 << 24);
+    const int64_t total = (int64_t)nnz + R * (int64_t)n;
+    int64_t target = (total + warps * chunks_per_warp() - 1) / (warps * chunks_per_warp());
+    target = std::max<int64_t>(kTileItems + R + 1, target);
+    const int64_t cap = std::min<int64_t>(target, 1 << 24);
     struct B {
         int32_t r, k;  // chunk start: row, entry
     };
     std::vector<B> bs;
     bs.push_back(B{0, 0});
-    int32_t ent = 0, rows = 0, r = 0, pos = 0;
+    int64_t cost = 0;
+    int32_t rows = 0, r = 0, pos = 0;
     while (r < n) {
-        const int32_t rem = sw[(size_t)r + 1] - pos;
-        if (ent + rem <= cap_e) {
+        const int64_t rem = (int64_t)sw[(size_t)r + 1] - pos;
+        if (cost + rem + R <= cap) {
             ++rows;
-            ent += rem;
+            cost += rem + R;
             pos = sw[(size_t)r + 1];
             ++r;
             continue;
         }
-        if ((rows > 0 && rem <= cap_e) || ent >= cap_e) {
+        if ((rows > 0 && rem + R <= cap) || cost + R >= cap) {
             bs.push_back(B{r, pos});  // close the chunk before row r (or its rest)
-            ent = rows = 0;
+            cost = 0;
+            rows = 0;
             continue;
         }
-        pos += cap_e - ent;  // cut: row r continues in the next chunk
+        pos += (int32_t)(cap - cost - R);  // cut: row r continues in the next chunk
         bs.push_back(B{r, pos});
-        ent = rows = 0;
+        cost = 0;
+        rows = 0;
     }
     if (bs.back().r != n || bs.back().k != nnz || bs.size() == 1) bs.push_back(B{n, nnz});
     const int32_t nch = (int32_t)bs.size() - 1;
@@ -524,7 +541,7 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         k.nnz_begin = a.k;
         k.nnz_end = b.k;
         k.row_end = b.r;
-        k.pad = 0;
+        k.pad = (int32_t)std::min<int64_t>((int64_t)(b.k - a.k) + R * (int64_t)(b.r - a.r + 1), INT32_MAX);  // cost
         k.graph = 0;
         k.tail_row = tail ? b.r : -1;
         k.head_ta = -1;
@@ -535,7 +552,7 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     }
     if (ntiles > INT32_MAX / 2) return EGPR_UNSUPPORTED_GRAPH;
     g->ntiles = (int32_t)ntiles;
-    std::vector<uint32_t> bits((size_t)ntiles * (kTileItems / 32), 0u);
+    std::vector<uint32_t> bits((size_t)ntiles * kTileWords, 0u);
     std::vector<int32_t> trow((size_t)ntiles, -1);
     for (int32_t c = 0; c < nch; ++c) {
         const Chunk& k = ch[(size_t)c];
@@ -544,7 +561,7 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         for (int32_t rr = first_row[(size_t)c]; rr < k.row_end; ++rr) {
             const int32_t p = sw[(size_t)rr + 1] - 1 - t0;
             const int32_t t = k.sub_begin + p / kTileItems, i = p % kTileItems;
-            bits[(size_t)t * (kTileItems / 32) + (size_t)(i >> 5)] |= 1u << (i & 31);
+            bits[(size_t)t * kTileWords + (size_t)(i >> 5)] |= 1u << (i & 31);
             if (trow[(size_t)t] < 0) trow[(size_t)t] = rr;
         }
         // a tile without a mark: the row its next mark would end
@@ -552,6 +569,15 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         for (int32_t t = k.sub_end - 1; t >= k.sub_begin; --t) {
             if (trow[(size_t)t] < 0) trow[(size_t)t] = next;
             else next = trow[(size_t)t];
+        }
+    }
+    // per lane, the marks of the lanes below it (lane l owns mask byte l)
+    for (int64_t t = 0; t < ntiles; ++t) {
+        uint32_t* w = bits.data() + (size_t)t * kTileWords;
+        uint32_t below = 0;
+        for (int l = 0; l < 32; ++l) {
+            w[8 + (l >> 2)] |= below << (8 * (l & 3));
+            below += (uint32_t)__builtin_popcount((w[l >> 2] >> (8 * (l & 3))) & 0xffu);
         }
     }
     g->plan.h_spans.clear();
@@ -563,6 +589,24 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     for (int32_t c = nch - 1; c >= 0; --c) {
         Chunk& k = ch[(size_t)c];
         if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
+    }
+    // Queue order = table order: costliest chunks first (stable), so that a
+    // launch ends on small chunks.  Chunk ids (span links) are renumbered.
+    {
+        std::vector<int32_t> perm((size_t)nch), pos_of((size_t)nch);
+        for (int32_t c = 0; c < nch; ++c) perm[(size_t)c] = c;
+        std::stable_sort(perm.begin(), perm.end(),
+                         [&](int32_t a, int32_t b) { return ch[(size_t)a].pad > ch[(size_t)b].pad; });
+        for (int32_t i = 0; i < nch; ++i) pos_of[(size_t)perm[(size_t)i]] = i;
+        std::vector<Chunk> sorted((size_t)nch);
+        for (int32_t i = 0; i < nch; ++i) {
+            Chunk k = ch[(size_t)perm[(size_t)i]];
+            if (k.head_ta >= 0) k.head_ta = pos_of[(size_t)k.head_ta];
+            if (k.tail_tb >= 0) k.tail_tb = pos_of[(size_t)k.tail_tb];
+            sorted[(size_t)i] = k;
+        }
+        ch.swap(sorted);
+        for (int32_t& sp : g->plan.h_spans) sp = pos_of[(size_t)sp];
     }
     // device arrays (a tile reads up to kTileItems + 8 entries past a chunk's start)
     const size_t pad = (size_t)(kTileItems + 16) * sizeof(int32_t);

@@ -276,6 +276,7 @@ struct WarpCtx {
     const int32_t* hub_ids;
     int32_t graph;
     int32_t iter;
+    int32_t done;           // the graph had converged before this launch
 };
 
 __device__ __forceinline__ Chunk load_chunk(const Chunk* p) {
@@ -287,13 +288,17 @@ __device__ __forceinline__ Chunk load_chunk(const Chunk* p) {
     return c;
 }
 
-// Sources, mark bits and first-mark row of warp tile t (entries T .. T+255).
+// Sources, mark bits, marks of the lanes below, and first-mark row of warp
+// tile t (entries T .. T+255).
 __device__ __forceinline__ void fetch_tile(const WarpCtx& X, int32_t t, int32_t T, int lane, int4& ca, int4& cb,
-                                           uint32_t& bits, int32_t& row) {
+                                           uint32_t& bits, uint32_t& below, int32_t& row) {
     const int4* c4 = reinterpret_cast<const int4*>(X.cols) + (T >> 2) + 2 * lane;
     ca = __ldcs(c4);
     cb = __ldcs(c4 + 1);
-    bits = (__ldcs(X.tile_bits + (size_t)t * (kTileItems / 32) + (lane >> 2)) >> (8 * (lane & 3))) & 0xffu;
+    const uint32_t* tw = X.tile_bits + (size_t)t * kTileWords + (lane >> 2);
+    const int sh = 8 * (lane & 3);
+    bits = (__ldcs(tw) >> sh) & 0xffu;
+    below = (__ldcs(tw + 8) >> sh) & 0xffu;
     row = __ldcs(X.tile_row + t);
 }
 
@@ -310,32 +315,34 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
     double err = 0.0, dsum = 0.0, xsum = 0.0;
     Real carry = Real(0);  // the row still open at the end of the previous tile
     int4 ca, cb;
-    uint32_t bits;
+    uint32_t bits, below;
     int32_t row;
-    fetch_tile(X, ck.sub_begin, T0, lane, ca, cb, bits, row);
+    fetch_tile(X, ck.sub_begin, T0, lane, ca, cb, bits, below, row);
     for (int32_t t = ck.sub_begin; t < ck.sub_end; ++t) {
         const int32_t T = T0 + (t - ck.sub_begin) * kTileItems;
         const int32_t cc[kLaneItems] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
         const uint32_t mb = bits;
+        const int32_t pre = (int32_t)below;
         const int32_t r0 = row;
-        if (t + 1 < ck.sub_end) fetch_tile(X, t + 1, T + kTileItems, lane, ca, cb, bits, row);
-        // 1. gathers of this tile's entries
+        if (t + 1 < ck.sub_end) fetch_tile(X, t + 1, T + kTileItems, lane, ca, cb, bits, below, row);
+        // 1. gathers of this tile's entries (only a chunk's first and last
+        //    tiles hold entries of other chunks)
         const int32_t p0 = T + kLaneItems * lane;
         Real v[kLaneItems];
+        auto carried = [&](int32_t s) -> Real {
+            if (kFinal) return X.z64[s >= 0 ? s : __ldg(X.hub_ids + (-s - 1))];
+            const int32_t h = -s - 1;
+            return s >= 0 ? X.zsrc[s] : (h < hub_count ? hub_s[h] : X.hub_g[h]);
+        };
+        if (T >= kb && T + kTileItems <= ke) {
 #pragma unroll
-        for (int u = 0; u < kLaneItems; ++u) {
-            const int32_t p = p0 + u;
-            const int32_t s = cc[u];
-            Real x = Real(0);
-            if (p >= kb && p < ke) {
-                if (kFinal) {
-                    x = X.z64[s >= 0 ? s : __ldg(X.hub_ids + (-s - 1))];
-                } else {
-                    const int32_t h = -s - 1;
-                    x = s >= 0 ? X.zsrc[s] : (h < hub_count ? hub_s[h] : X.hub_g[h]);
-                }
+            for (int u = 0; u < kLaneItems; ++u) v[u] = carried(cc[u]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < kLaneItems; ++u) {
+                const int32_t p = p0 + u;
+                v[u] = (p >= kb && p < ke) ? carried(cc[u]) : Real(0);
             }
-            v[u] = x;
         }
         if (X.w) {
             const float4* w4 = reinterpret_cast<const float4*>(X.w) + (T >> 2) + 2 * lane;
@@ -343,14 +350,8 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
             v[0] *= (Real)wa.x; v[1] *= (Real)wa.y; v[2] *= (Real)wa.z; v[3] *= (Real)wa.w;
             v[4] *= (Real)wb.x; v[5] *= (Real)wb.y; v[6] *= (Real)wb.z; v[7] *= (Real)wb.w;
         }
-        // 2. mark ordinals: pre = marks of lower lanes, nm = marks of the tile
-        int32_t pre = 0, nm = 0;
-#pragma unroll
-        for (int b = 0; b < kLaneItems; ++b) {
-            const unsigned bb = __ballot_sync(kFull, (mb >> b) & 1u);
-            pre += __popc(bb & lt);
-            nm += __popc(bb);
-        }
+        // 2. marks of the tile (pre: marks of the lanes below, from the tile table)
+        const int32_t nm = __shfl_sync(kFull, pre + __popc(mb), 31);
         // the rows this lane finishes first: request their data now
         float xin0 = 0.f, sc0 = 0.f;
         int32_t hs0 = -1;
@@ -484,39 +485,54 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_sweep(SweepParams P) {
         }
     }
     if (!s_idle && !s_abort) {
+        // Each warp keeps one claim and one chunk record ahead of the chunk it
+        // works on; the record is only read once the chunk is done.
         WarpCtx& X = ctx[warp];
         if (lane == 0) X.graph = -1;
         __syncwarp();
-        uint32_t nxt = 0;
-        if (lane == 0) nxt = atomicAdd(&P.ctl->queue, 1u);
-        for (;;) {
-            const int32_t c = (int32_t)__shfl_sync(kFull, nxt, 0);
-            if (c >= P.nchunks) break;
-            if (lane == 0) nxt = atomicAdd(&P.ctl->queue, 1u);  // the next claim, in flight meanwhile
-            const Chunk ck = load_chunk(P.chunks + c);
-            const int32_t gi = ck.graph;
-            GraphState* st = P.states + gi;
-            const int32_t iter = ldcg(&st->iter);
-            if (!kFinal && ldcg(&st->done)) continue;  // frozen graph (same answer for the whole warp)
-            if (gi != X.graph || iter != X.iter) {
-                __syncwarp();
-                if (lane == 0) {
-                    const GraphDev& G = P.graphs[gi];
-                    X.W = make_view<kFinal>(G, st, iter);
-                    X.cols = G.cols;
-                    X.w = G.w;
-                    X.tile_bits = G.tile_bits;
-                    X.tile_row = G.tile_row;
-                    X.zsrc = G.z[iter & 1];
-                    X.hub_g = G.hubz[iter & 1];
-                    X.z64 = G.z64;
-                    X.hub_ids = G.hub_ids;
-                    X.graph = gi;
-                    X.iter = iter;
+        uint32_t claim = 0;
+        if (lane == 0) claim = atomicAdd(&P.ctl->queue, 1u);
+        int32_t c = (int32_t)__shfl_sync(kFull, claim, 0);
+        if (c < P.nchunks) {
+            if (lane == 0) claim = atomicAdd(&P.ctl->queue, 1u);
+            Chunk ck = load_chunk(P.chunks + c);
+            for (;;) {
+                if (ck.graph != X.graph) {
+                    const int32_t gi = ck.graph;
+                    GraphState* st = P.states + gi;
+                    const int32_t iter = ldcg(&st->iter);
+                    const int32_t done = kFinal ? 0 : ldcg(&st->done);
+                    __syncwarp();
+                    if (lane == 0) {
+                        const GraphDev& G = P.graphs[gi];
+                        X.W = make_view<kFinal>(G, st, iter);
+                        X.cols = G.cols;
+                        X.w = G.w;
+                        X.tile_bits = G.tile_bits;
+                        X.tile_row = G.tile_row;
+                        X.zsrc = G.z[iter & 1];
+                        X.hub_g = G.hubz[iter & 1];
+                        X.z64 = G.z64;
+                        X.hub_ids = G.hub_ids;
+                        X.graph = gi;
+                        X.iter = iter;
+                        X.done = done;
+                    }
+                    __syncwarp();
                 }
-                __syncwarp();
+                // the next chunk: its claim was issued one chunk ago
+                const int32_t cn = (int32_t)__shfl_sync(kFull, claim, 0);
+                const bool have = cn < P.nchunks;
+                Chunk nk;
+                if (have) {
+                    nk = load_chunk(P.chunks + cn);
+                    if (lane == 0) claim = atomicAdd(&P.ctl->queue, 1u);
+                }
+                if (!X.done) process_chunk<Real>(P, c, ck, X, hub_s, hub_count, scr);  // else: frozen graph
+                if (!have) break;
+                c = cn;
+                ck = nk;
             }
-            process_chunk<Real>(P, c, ck, X, hub_s, hub_count, scr);
         }
     }
     __threadfence();  // this CTA's accumulator updates before its exit is counted
