@@ -431,6 +431,77 @@ __global__ void k_build_sweep_cols(const int32_t* __restrict__ in_row, const int
     }
 }
 
+// max(1, length of row r); 0 for the closing slot r = n.
+__global__ void k_row_len1(const int32_t* __restrict__ in_row, int32_t n, uint32_t* __restrict__ out) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += (int64_t)gridDim.x * blockDim.x)
+        out[r] = r < n ? (uint32_t)max(1, in_row[r + 1] - in_row[r]) : 0u;
+}
+
+// sw_row[n+1 .. n+7] = sw_row[n] (bulk reads of row data may run past n).
+__global__ void k_pad_tail(int32_t* sw_row, int32_t n) {
+    if (threadIdx.x > 0 && threadIdx.x < 8) sw_row[(int64_t)n + threadIdx.x] = sw_row[n];
+}
+
+// For the ideal boundary d = i * cap: the row r whose cost range holds d
+// (cost of the start of row r = sw_row[r] + R * r), the offset of d into the
+// row's entries, the row's start and its length.
+__global__ void k_chunk_cuts(const int32_t* __restrict__ sw_row, int32_t n, int64_t R, int64_t cap, int32_t ideal,
+                             int4* __restrict__ out) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= ideal; i += gridDim.x * blockDim.x) {
+        const int64_t d = (int64_t)i * cap;
+        int32_t lo = 0, hi = n - 1;  // largest r with sw_row[r] + R*r <= d
+        while (lo < hi) {
+            const int32_t mid = lo + ((hi - lo + 1) >> 1);
+            if ((int64_t)sw_row[mid] + R * mid <= d) lo = mid;
+            else hi = mid - 1;
+        }
+        const int64_t off = d - ((int64_t)sw_row[lo] + R * lo);
+        const int32_t len = sw_row[lo + 1] - sw_row[lo];
+        out[i] = make_int4(lo, (int32_t)(off < (int64_t)len ? off : (int64_t)len), sw_row[lo], len);
+    }
+}
+
+// Every row ends on an entry; mark it in the tile of the chunk that holds it.
+__global__ void k_tile_marks(const int32_t* __restrict__ sw_row, int32_t n, const int32_t* __restrict__ cstart,
+                             const int32_t* __restrict__ ctile, int32_t nch, uint32_t* __restrict__ bits,
+                             int32_t* __restrict__ trow) {
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int32_t p = sw_row[r + 1] - 1;
+        int32_t lo = 0, hi = nch - 1;  // last chunk starting at or before p
+        while (lo < hi) {
+            const int32_t mid = lo + ((hi - lo + 1) >> 1);
+            if (cstart[mid] <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        const int32_t q = p - (cstart[lo] & ~7);
+        const int32_t t = ctile[lo] + q / kTileItems, i = q % kTileItems;
+        atomicOr(&bits[(size_t)t * kTileWords + (i >> 5)], 1u << (i & 31));
+        atomicMin(&trow[t], r);
+    }
+}
+
+// Per lane of every tile: the marks of the lanes below it (one byte per lane).
+__global__ void k_tile_offsets(uint32_t* __restrict__ bits, int64_t ntiles) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t t = warp; t < ntiles; t += nwarps) {
+        uint32_t* w = bits + (size_t)t * kTileWords;
+        const uint32_t mine = __popc((w[lane >> 2] >> (8 * (lane & 3))) & 0xffu);
+        uint32_t incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t up = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += up;
+        }
+        const uint32_t below = incl - mine;
+        uint32_t word = below;
+        word |= __shfl_down_sync(0xffffffffu, below, 1) << 8;
+        word |= __shfl_down_sync(0xffffffffu, below, 2) << 16;
+        word |= __shfl_down_sync(0xffffffffu, below, 3) << 24;
+        if ((lane & 3) == 0) w[8 + (lane >> 2)] = word;
+    }
+}
+
 namespace {
 
 int chunks_per_warp() {
@@ -454,74 +525,73 @@ int row_cost() {
 
 }  // namespace
 
-// The sweep's work layout, by one host pass over in_row.
+// The sweep's work layout, built on the device (the host only sees the chunk
+// boundaries):
 //   * sw_row / sw_col / sw_w: the inbound CSR with a placeholder entry in every
 //     empty row, so that every row ends on an entry of its own;
-//   * chunks: consecutive rows packed while a chunk's cost (entries plus
-//     row_cost() per row) stays under a cap sized for chunks_per_warp() chunks
-//     per resident warp; a longer row is cut (a span: its chunks add pieces to
-//     the span's accumulator and the sweep finishes the row when the launch
-//     ends), and every cut leaves at least one entry of the row on each side;
+//   * chunks: boundaries at multiples of a cost cap along the rows, where a
+//     row costs its entries plus row_cost(); a boundary moves back to the
+//     start of its row unless that row began before the previous boundary (a
+//     row longer than a chunk), which is then cut (a span: its chunks add
+//     pieces to the span's accumulator and the sweep finishes the row when the
+//     launch ends); every cut leaves at least one entry on each side;
 //   * warp tiles: chunk c covers tiles of kTileItems entries from
-//     (start & ~7); per tile a 256-bit mask of the entries that end a row
-//     finished by the chunk, per lane the number of marks in the lanes below
-//     it, and the first such row (the k-th mark of a tile ends row
-//     tile_row + k, since every row has an entry).
+//     (start & ~7); per tile a 256-bit mask of the entries that end a row, per
+//     lane the number of marks in the lanes below it, and the first row a mark
+//     of the tile ends (the k-th mark of a tile ends row tile_row + k, since
+//     every row has an entry).
+// Chunks are stored costliest first, which is their queue order.
 int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     const int32_t n = g->n;
-    std::vector<int32_t> row((size_t)n + 1);
-    int rc = cuda_ok(cudaMemcpyAsync(row.data(), g->in_row.p, row.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s),
-                     "D2H in_row");
-    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "sweep layout"))) return rc;
-    std::vector<int32_t> sw((size_t)n + 8);
-    int64_t acc = 0;
-    for (int32_t r = 0; r < n; ++r) {
-        sw[(size_t)r] = (int32_t)acc;
-        acc += std::max(1, row[(size_t)r + 1] - row[(size_t)r]);
-    }
-    if (acc > (int64_t)INT32_MAX - 4096) return EGPR_UNSUPPORTED_GRAPH;
-    for (size_t r = (size_t)n; r < sw.size(); ++r) sw[r] = (int32_t)acc;
-    const int32_t nnz = (int32_t)acc;
+    TmpAlloc tmp(s);
+    int rc = EGPR_SUCC;
+    // placeholder offsets: sw_row = exclusive scan of max(1, row length)
+    uint32_t* len1 = tmp.get<uint32_t>((size_t)n + 1, &rc);
+    if (rc || (rc = g->sw_row.alloc(((size_t)n + 8) * sizeof(int32_t)))) return rc;
+    k_row_len1<<<grid_for((int64_t)n + 1), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, len1);
+    if ((rc = exclusive_scan_u32(len1, reinterpret_cast<uint32_t*>(g->sw_row.as<int32_t>()), (int64_t)n + 1, s))) return rc;
+    k_pad_tail<<<1, 32, 0, s>>>(g->sw_row.as<int32_t>(), n);
+    uint32_t nnz_u = 0;
+    if ((rc = cuda_ok(cudaMemcpyAsync(&nnz_u, g->sw_row.as<int32_t>() + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "D2H sweep entries")) ||
+        (rc = cuda_ok(cudaStreamSynchronize(s), "sweep layout")))
+        return rc;
+    if ((int64_t)nnz_u > (int64_t)INT32_MAX - 4096) return EGPR_UNSUPPORTED_GRAPH;
+    const int32_t nnz = (int32_t)nnz_u;
     g->sw_nnz = nnz;
-    // chunks of about equal cost (entries + row_cost() per row touched)
+    // chunk boundaries at ideal costs d_i = i * cap
     const int64_t R = row_cost();
     const int64_t warps = std::max(1, resident_warps);
     const int64_t total = (int64_t)nnz + R * (int64_t)n;
-    int64_t target = (total + warps * chunks_per_warp() - 1) / (warps * chunks_per_warp());
-    target = std::max<int64_t>(kTileItems + R + 1, target);
-    const int64_t cap = std::min<int64_t>(target, 1 << 24);
+    int64_t cap = (total + warps * chunks_per_warp() - 1) / (warps * chunks_per_warp());
+    cap = std::min<int64_t>(std::max<int64_t>(kTileItems + R + 1, cap), 1 << 24);
+    const int64_t ideal = std::max<int64_t>(1, (total + cap - 1) / cap);
+    int4* d_cut = tmp.get<int4>((size_t)ideal + 1, &rc);
+    if (rc) return rc;
+    k_chunk_cuts<<<grid_for(ideal + 1), kThreads, 0, s>>>(g->sw_row.as<int32_t>(), n, R, cap, (int32_t)ideal, d_cut);
+    std::vector<int4> cut((size_t)ideal + 1);
+    if ((rc = cuda_ok(cudaMemcpyAsync(cut.data(), d_cut, cut.size() * sizeof(int4), cudaMemcpyDeviceToHost, s), "D2H chunk cuts")) ||
+        (rc = cuda_ok(cudaStreamSynchronize(s), "sweep layout")))
+        return rc;
     struct B {
-        int32_t r, k;  // chunk start: row, entry
+        int32_t r, k, rs;  // boundary: row, entry, start of that row
     };
     std::vector<B> bs;
-    bs.push_back(B{0, 0});
-    int64_t cost = 0;
-    int32_t rows = 0, r = 0, pos = 0;
-    while (r < n) {
-        const int64_t rem = (int64_t)sw[(size_t)r + 1] - pos;
-        if (cost + rem + R <= cap) {
-            ++rows;
-            cost += rem + R;
-            pos = sw[(size_t)r + 1];
-            ++r;
-            continue;
+    bs.push_back(B{0, 0, 0});
+    for (int64_t i = 1; i < ideal; ++i) {
+        const int4 c = cut[(size_t)i];  // (row, offset into the row, row start, row length)
+        const B& p = bs.back();
+        if (c.z > p.k) {
+            bs.push_back(B{c.x, c.z, c.z});  // the row's start
+        } else if (c.w >= 2) {
+            const int32_t k = c.z + std::min(std::max(c.y, 1), c.w - 1);  // a cut inside a long row
+            if (c.x == p.r && k > p.k) bs.push_back(B{c.x, k, c.z});
         }
-        if ((rows > 0 && rem + R <= cap) || cost + R >= cap) {
-            bs.push_back(B{r, pos});  // close the chunk before row r (or its rest)
-            cost = 0;
-            rows = 0;
-            continue;
-        }
-        pos += (int32_t)(cap - cost - R);  // cut: row r continues in the next chunk
-        bs.push_back(B{r, pos});
-        cost = 0;
-        rows = 0;
     }
-    if (bs.back().r != n || bs.back().k != nnz || bs.size() == 1) bs.push_back(B{n, nnz});
+    bs.push_back(B{n, nnz, nnz});
     const int32_t nch = (int32_t)bs.size() - 1;
     std::vector<Chunk>& ch = g->plan.h_chunks;
     ch.assign((size_t)nch, Chunk{});
-    std::vector<int32_t> first_row((size_t)nch);
+    std::vector<int32_t> cstart((size_t)nch), ctile((size_t)nch);
     int64_t ntiles = 0;
     for (int32_t c = 0; c < nch; ++c) {
         const B& a = bs[(size_t)c];
@@ -529,8 +599,8 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         const int32_t t0 = a.k & ~7;
         const int32_t nt = std::max<int32_t>(1, (b.k - t0 + kTileItems - 1) / kTileItems);
         Chunk& k = ch[(size_t)c];
-        const bool head = a.r < n && a.k > sw[(size_t)a.r];
-        const bool tail = b.r < n && b.k > sw[(size_t)b.r];
+        const bool head = a.r < n && a.k > a.rs;
+        const bool tail = b.r < n && b.k > b.rs;
         int32_t f = 0;
         if (head) f |= kHasHead;
         if (tail) f |= kHasTail;
@@ -547,39 +617,27 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         k.head_ta = -1;
         k.tail_tb = -1;
         k.pad2 = 0;
-        first_row[(size_t)c] = a.r;
+        cstart[(size_t)c] = a.k;
+        ctile[(size_t)c] = (int32_t)ntiles;
         ntiles += nt;
     }
     if (ntiles > INT32_MAX / 2) return EGPR_UNSUPPORTED_GRAPH;
     g->ntiles = (int32_t)ntiles;
-    std::vector<uint32_t> bits((size_t)ntiles * kTileWords, 0u);
-    std::vector<int32_t> trow((size_t)ntiles, -1);
-    for (int32_t c = 0; c < nch; ++c) {
-        const Chunk& k = ch[(size_t)c];
-        const int32_t t0 = k.nnz_begin & ~7;
-        // rows finished by the chunk: [first row, row_end); each ends on an entry in (begin, end]
-        for (int32_t rr = first_row[(size_t)c]; rr < k.row_end; ++rr) {
-            const int32_t p = sw[(size_t)rr + 1] - 1 - t0;
-            const int32_t t = k.sub_begin + p / kTileItems, i = p % kTileItems;
-            bits[(size_t)t * kTileWords + (size_t)(i >> 5)] |= 1u << (i & 31);
-            if (trow[(size_t)t] < 0) trow[(size_t)t] = rr;
-        }
-        // a tile without a mark: the row its next mark would end
-        int32_t next = k.row_end;
-        for (int32_t t = k.sub_end - 1; t >= k.sub_begin; --t) {
-            if (trow[(size_t)t] < 0) trow[(size_t)t] = next;
-            else next = trow[(size_t)t];
-        }
-    }
-    // per lane, the marks of the lanes below it (lane l owns mask byte l)
-    for (int64_t t = 0; t < ntiles; ++t) {
-        uint32_t* w = bits.data() + (size_t)t * kTileWords;
-        uint32_t below = 0;
-        for (int l = 0; l < 32; ++l) {
-            w[8 + (l >> 2)] |= below << (8 * (l & 3));
-            below += (uint32_t)__builtin_popcount((w[l >> 2] >> (8 * (l & 3))) & 0xffu);
-        }
-    }
+    // tile tables: marks by row ends, then per-lane offsets
+    int32_t* d_cstart = tmp.get<int32_t>((size_t)nch, &rc);
+    int32_t* d_ctile = tmp.get<int32_t>((size_t)nch, &rc);
+    if (rc || (rc = g->tile_bits.alloc((size_t)ntiles * kTileWords * sizeof(uint32_t))) ||
+        (rc = g->tile_row.alloc((size_t)ntiles * sizeof(int32_t))))
+        return rc;
+    if ((rc = cuda_ok(cudaMemcpyAsync(d_cstart, cstart.data(), (size_t)nch * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D chunk starts")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(d_ctile, ctile.data(), (size_t)nch * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D chunk tiles")) ||
+        (rc = cuda_ok(cudaMemsetAsync(g->tile_bits.p, 0, g->tile_bits.bytes, s), "memset")) ||
+        (rc = cuda_ok(cudaMemsetAsync(g->tile_row.p, 0x7f, g->tile_row.bytes, s), "memset")))
+        return rc;
+    k_tile_marks<<<grid_for(n), kThreads, 0, s>>>(g->sw_row.as<int32_t>(), n, d_cstart, d_ctile, nch,
+                                                   g->tile_bits.as<uint32_t>(), g->tile_row.as<int32_t>());
+    k_tile_offsets<<<grid_for(ntiles * 32), kThreads, 0, s>>>(g->tile_bits.as<uint32_t>(), ntiles);
+    // span links (row order), then the queue order: costliest chunks first
     g->plan.h_spans.clear();
     for (int32_t c = 0; c < nch; ++c) {
         Chunk& k = ch[(size_t)c];
@@ -590,8 +648,6 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         Chunk& k = ch[(size_t)c];
         if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
     }
-    // Queue order = table order: costliest chunks first (stable), so that a
-    // launch ends on small chunks.  Chunk ids (span links) are renumbered.
     {
         std::vector<int32_t> perm((size_t)nch), pos_of((size_t)nch);
         for (int32_t c = 0; c < nch; ++c) perm[(size_t)c] = c;
@@ -608,19 +664,12 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         ch.swap(sorted);
         for (int32_t& sp : g->plan.h_spans) sp = pos_of[(size_t)sp];
     }
-    // device arrays (a tile reads up to kTileItems + 8 entries past a chunk's start)
+    // entries (a tile reads up to kTileItems + 8 entries past a chunk's start)
     const size_t pad = (size_t)(kTileItems + 16) * sizeof(int32_t);
-    if ((rc = g->sw_row.alloc(sw.size() * sizeof(int32_t))) ||
-        (rc = g->sw_col.alloc((size_t)nnz * sizeof(int32_t) + pad)) ||
-        (g->weighted && (rc = g->sw_w.alloc((size_t)nnz * sizeof(float) + pad))) ||
-        (rc = g->tile_bits.alloc(bits.size() * sizeof(uint32_t))) ||
-        (rc = g->tile_row.alloc(trow.size() * sizeof(int32_t))))
+    if ((rc = g->sw_col.alloc((size_t)nnz * sizeof(int32_t) + pad)) ||
+        (g->weighted && (rc = g->sw_w.alloc((size_t)nnz * sizeof(float) + pad))))
         return rc;
-    if ((rc = cuda_ok(cudaMemcpyAsync(g->sw_row.p, sw.data(), sw.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D sweep rows")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(g->tile_bits.p, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "H2D tile masks")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(g->tile_row.p, trow.data(), trow.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D tile rows")) ||
-        (rc = cuda_ok(cudaMemsetAsync(g->sw_col.p, 0, g->sw_col.bytes, s), "memset")))
-        return rc;
+    if ((rc = cuda_ok(cudaMemsetAsync(g->sw_col.p, 0, g->sw_col.bytes, s), "memset"))) return rc;
     if (g->weighted && (rc = cuda_ok(cudaMemsetAsync(g->sw_w.p, 0, g->sw_w.bytes, s), "memset"))) return rc;
     k_build_sweep_cols<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(
         g->in_row.as<int32_t>(), g->in_col.as<int32_t>(), g->weighted ? g->in_w.as<float>() : nullptr, n,
