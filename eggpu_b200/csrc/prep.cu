@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "egpr_internal.cuh"
@@ -339,6 +340,42 @@ inline int grid_for(int64_t work, int per_block = kThreads) {
 
 int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SUCC : set_cuda_error(e, what); }
 
+// Stream-ordered scratch of the preparation comes from a pool per device that
+// keeps up to EGPR_SCRATCH_KEEP_MB (default 4096) MiB after it is freed, so
+// preparing graph after graph does not map fresh pages every time.
+cudaMemPool_t scratch_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        const char* e = std::getenv("EGPR_SCRATCH_KEEP_MB");
+        const long long mb = e ? std::atoll(e) : 4096;
+        unsigned long long keep = (unsigned long long)std::max(0LL, mb) << 20;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
+    cudaMemPool_t pool = scratch_pool();
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
+}
+
 struct TmpAlloc {
     cudaStream_t s;
     std::vector<void*> ptrs;
@@ -349,7 +386,7 @@ struct TmpAlloc {
     template <typename T>
     T* get(size_t count, int* rc) {
         void* p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s);
+        cudaError_t e = scratch_alloc(&p, std::max<size_t>(count, 1) * sizeof(T), s);
         if (e != cudaSuccess) {
             set_cuda_error(e, "cudaMallocAsync (preparation scratch)");
             *rc = EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM;
@@ -391,7 +428,7 @@ int exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t len, cudaStrea
         return cuda_ok(cudaGetLastError(), "scan");
     }
     uint32_t* sums = nullptr;
-    cudaError_t e = cudaMallocAsync(&sums, (size_t)ntiles * sizeof(uint32_t), s);
+    cudaError_t e = scratch_alloc(reinterpret_cast<void**>(&sums), (size_t)ntiles * sizeof(uint32_t), s);
     if (e != cudaSuccess) {
         set_cuda_error(e, "cudaMallocAsync (scan)");
         return EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM;
@@ -669,8 +706,9 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     if ((rc = g->sw_col.alloc((size_t)nnz * sizeof(int32_t) + pad)) ||
         (g->weighted && (rc = g->sw_w.alloc((size_t)nnz * sizeof(float) + pad))))
         return rc;
-    if ((rc = cuda_ok(cudaMemsetAsync(g->sw_col.p, 0, g->sw_col.bytes, s), "memset"))) return rc;
-    if (g->weighted && (rc = cuda_ok(cudaMemsetAsync(g->sw_w.p, 0, g->sw_w.bytes, s), "memset"))) return rc;
+    // every entry is written below; only the padding past the last one is cleared
+    if ((rc = cuda_ok(cudaMemsetAsync(g->sw_col.as<int32_t>() + nnz, 0, pad, s), "memset"))) return rc;
+    if (g->weighted && (rc = cuda_ok(cudaMemsetAsync(g->sw_w.as<float>() + nnz, 0, pad, s), "memset"))) return rc;
     k_build_sweep_cols<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(
         g->in_row.as<int32_t>(), g->in_col.as<int32_t>(), g->weighted ? g->in_w.as<float>() : nullptr, n,
         g->sw_row.as<int32_t>(), g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr,
