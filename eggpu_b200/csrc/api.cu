@@ -87,6 +87,7 @@ void Plan::release() {
     d_ctl.release();
     d_acc.release();
     d_span_acc.release();
+    d_span_cnt.release();
     d_span_list.release();
     ngraphs = nchunks = grid = any_weighted = max_n = nspans = nacc = 0;
 }
@@ -303,7 +304,7 @@ static uint64_t bits_of(double x) {
 int64_t egpr_graph::device_bytes() const {
     return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes + sub_coord.bytes +
                      sw_row.bytes + sw_col.bytes + sw_w.bytes + tile_bits.bytes + tile_row.bytes +
-                     hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_acc.bytes + plan.d_span_acc.bytes +
+                     hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_acc.bytes + plan.d_span_acc.bytes + plan.d_span_cnt.bytes +
                      plan.d_span_list.bytes +
                      scale.bytes + tele.bytes + x0.bytes + x1.bytes + z0.bytes + z1.bytes + out.bytes + z64.bytes +
                      plan.d_chunks.bytes + plan.d_graphs.bytes + plan.d_states.bytes + plan.d_ndang.bytes +

@@ -40,11 +40,11 @@ struct Chunk {
     int32_t head_ta;     // global chunk id where the head row's span starts
     int32_t tail_tb;     // global chunk id where the tail row's span ends
     int32_t tail_row;    // vertex id of the tail row (span rows are finalised by row id)
-    int32_t pad2;
+    int32_t pad2;        // sweep chunk: chunks of its tail row's span
     int32_t nnz_begin;   // entries [nnz_begin, nnz_end) belong to the chunk
     int32_t nnz_end;
     int32_t row_end;     // sweep chunk: rows before row_end are finished by the chunk
-    int32_t pad;         // sweep chunk: estimated cost (entries + a charge per row)
+    int32_t pad;         // sweep chunk: chunks of its head row's span (estimated cost while preparing)
 };
 
 // The sweep's warp tiles: kTileItems entries, lane l owning entries 8l..8l+7.
@@ -122,7 +122,8 @@ struct SweepParams {
     // of 2^-32 and of 2^-64) with integer atomics, so their order does not
     // change the result.
     unsigned long long* acc;       // kAccWords per slot: err, dangling, rank sums
-    unsigned long long* span_acc;  // 2 per stage (span start stage): the cut row's sum
+    unsigned long long* span_acc;  // 2 per chunk (span start chunk): the cut row's sum
+    uint32_t* span_cnt;            // per chunk (span start chunk): pieces added so far
     const int32_t* span_list;  // span start stages
     int32_t nspans;
     int32_t acc_sub;           // accumulator slots per graph
@@ -151,7 +152,7 @@ struct Plan {
     int32_t any_weighted = 0;
     int32_t hub_count = 0;   // hubs of the plan's graph (one-graph plans)
     int32_t max_n = 0;
-    DevBuf d_chunks, d_graphs, d_states, d_ndang, d_ctl, d_span_list, d_acc, d_span_acc;
+    DevBuf d_chunks, d_graphs, d_states, d_ndang, d_ctl, d_span_list, d_acc, d_span_acc, d_span_cnt;
     std::vector<Chunk> h_chunks;      // a graph's own chunk table (local ids)
     std::vector<int32_t> h_spans;     // a graph's span start chunks (local ids)
     std::vector<Chunk> h_chunks_all;  // the plan's table (global ids)

@@ -686,6 +686,15 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
         if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
     }
     {
+        // chunks of the span each chunk adds to (its head row's, its tail row's),
+        // counted before the renumbering
+        std::vector<int32_t> hparts((size_t)nch, 0), tparts((size_t)nch, 0);
+        for (int32_t c = 0; c < nch; ++c) {
+            const Chunk& k = ch[(size_t)c];
+            if (k.flags & kInterior) hparts[(size_t)c] = k.tail_tb - k.head_ta + 1;
+            else if (k.flags & kHasHead) hparts[(size_t)c] = c - k.head_ta + 1;
+            if ((k.flags & kHasTail) && !(k.flags & kInterior)) tparts[(size_t)c] = k.tail_tb - c + 1;
+        }
         std::vector<int32_t> perm((size_t)nch), pos_of((size_t)nch);
         for (int32_t c = 0; c < nch; ++c) perm[(size_t)c] = c;
         std::stable_sort(perm.begin(), perm.end(),
@@ -696,6 +705,8 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
             Chunk k = ch[(size_t)perm[(size_t)i]];
             if (k.head_ta >= 0) k.head_ta = pos_of[(size_t)k.head_ta];
             if (k.tail_tb >= 0) k.tail_tb = pos_of[(size_t)k.tail_tb];
+            k.pad = hparts[(size_t)perm[(size_t)i]];
+            k.pad2 = tparts[(size_t)perm[(size_t)i]];
             sorted[(size_t)i] = k;
         }
         ch.swap(sorted);

@@ -144,23 +144,23 @@ __device__ SweepView make_view(const GraphDev& G, GraphState* st, int32_t iter) 
 // residual compares the stored FP32 iterates, so the loop can stop once they no
 // longer change even when tol*n is below FP32 resolution.  FP64 correction
 // sweep: writes the FP64 result.
-template <bool kFinal>
+template <bool kFinal, typename Acc>
 __device__ __forceinline__ void finish_row(const SweepView& W, int32_t v, double acc, float xin, float scale,
-                                           int32_t hs, double& err, double& dsum, double& xsum) {
+                                           int32_t hs, Acc& err, Acc& dsum, double& xsum) {
     double val;
     if (W.personalised) val = (acc + W.one_minus_alpha * (double)__ldg(W.tele + v)) + W.dmass;
     else val = acc + W.jump;
     if (!kFinal) {
         const float xo = (float)val;
-        err += fabs((double)xo - (double)xin);
+        err += (Acc)fabsf(xo - xin);
         W.xout[v] = xo;
         const float zo = scale >= 0.f ? xo * scale : 0.f;
         W.zout[v] = zo;
         if (hs >= 0) W.hub_out[hs] = zo;
-        if (scale < 0.f) dsum += (double)xo;
+        if (scale < 0.f) dsum += (Acc)xo;
         xsum += (double)xo;
     } else {
-        err += fabs(val - (double)xin);
+        err += (Acc)fabs(val - (double)xin);
         W.out[v] = val;
         xsum += val;
     }
@@ -191,44 +191,58 @@ __device__ __forceinline__ unsigned long long* acc_slot(const SweepParams& P, in
     return P.acc + (size_t)kAccWords * ((size_t)gi * (size_t)P.acc_sub + (size_t)(k % P.acc_sub));
 }
 
-// End of a launch, run by the whole last CTA to leave the queue: finishes the
-// rows cut between chunks, then per graph turns the accumulators into the
-// residual, dangling mass and rank sum, clears them, and advances the graph's
-// state (pagerank.py:117-131).
+// A piece of a row cut between chunks has been added to the span's
+// accumulator (lane 0).  The last of the span's chunks to arrive finishes the
+// row; the sum is exact fixed point, so it does not matter which one that is.
+template <bool kFinal>
+__device__ void span_arrive(const SweepParams& P, const SweepView& W, int32_t ta, int32_t parts, int32_t slot) {
+    __threadfence();
+    const uint32_t prev = atomicAdd(&P.span_cnt[ta], 1u);
+    if (prev != (uint32_t)(parts - 1)) return;
+    __threadfence();
+    unsigned long long* sa = P.span_acc + 2 * ta;
+    const double sum = fx_join(ldcg_u64(sa), ldcg_u64(sa + 1));
+    sa[0] = 0ull;
+    sa[1] = 0ull;
+    P.span_cnt[ta] = 0u;
+    const int32_t v = __ldg(&P.chunks[ta].tail_row);
+    double e = 0.0, d = 0.0, x = 0.0;
+    finish_row<kFinal, double>(W, v, sum, W.xin[v], kFinal ? 0.f : W.scale[v], kFinal ? -1 : W.hub_slot[v], e, d, x);
+    unsigned long long* a = acc_slot(P, __ldg(&P.chunks[ta].graph), slot);
+    fx_add(a, e);
+    fx_add(a + 2, d);
+    fx_add(a + 4, x);
+}
+
+// End of a launch, run by the whole last CTA to leave the queue: per graph,
+// turns the accumulators into the residual, dangling mass and rank sum, clears
+// them, and advances the graph's state (pagerank.py:117-131).
 template <bool kFinal>
 __device__ void launch_tail(const SweepParams& P) {
     const int tid = threadIdx.x;
-    for (int32_t q = tid; q < P.nspans; q += blockDim.x) {
-        const int32_t ta = P.span_list[q];
-        const int32_t gi = __ldg(&P.chunks[ta].graph);
-        const int32_t v = __ldg(&P.chunks[ta].tail_row);
-        GraphState* st = P.states + gi;
-        if (!kFinal && ldcg(&st->done)) continue;
-        unsigned long long* sa = P.span_acc + 2 * ta;
-        const double sum = fx_join(ldcg_u64(sa), ldcg_u64(sa + 1));
-        sa[0] = 0ull;
-        sa[1] = 0ull;
-        const SweepView W = make_view<kFinal>(P.graphs[gi], st, ldcg(&st->iter));
-        double e = 0.0, d = 0.0, x = 0.0;
-        finish_row<kFinal>(W, v, sum, W.xin[v], kFinal ? 0.f : W.scale[v], kFinal ? -1 : W.hub_slot[v], e, d, x);
-        unsigned long long* a = acc_slot(P, gi, tid);
-        fx_add(a, e);
-        fx_add(a + 2, d);
-        fx_add(a + 4, x);
-    }
     __threadfence();
     __syncthreads();
     const int warp = tid >> 5, lane = tid & 31;
     for (int32_t gi = warp; gi < P.ngraphs; gi += (int32_t)(blockDim.x >> 5)) {
         GraphState* st = P.states + gi;
         if (!kFinal && ldcg(&st->done)) continue;
+        // all of a lane's loads first (they are independent), then the clears
         unsigned long long w[6] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
-        for (int32_t k = lane; k < P.acc_sub; k += 32) {
-            unsigned long long* a = P.acc + (size_t)kAccWords * ((size_t)gi * (size_t)P.acc_sub + (size_t)k);
+        for (int32_t k0 = 0; k0 < P.acc_sub; k0 += 64) {
+            unsigned long long* a = P.acc + (size_t)kAccWords * ((size_t)gi * (size_t)P.acc_sub + (size_t)(k0 + lane));
+            unsigned long long* b = a + (size_t)kAccWords * 32;
+            const bool ha = k0 + lane < P.acc_sub, hb = k0 + 32 + lane < P.acc_sub;
+            unsigned long long ra[6], rb[6];
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
-                w[i] += ldcg_u64(a + i);
-                a[i] = 0ull;
+                ra[i] = ha ? ldcg_u64(a + i) : 0ull;
+                rb[i] = hb ? ldcg_u64(b + i) : 0ull;
+            }
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                w[i] += ra[i] + rb[i];
+                if (ha) a[i] = 0ull;
+                if (hb) b[i] = 0ull;
             }
         }
 #pragma unroll
@@ -290,49 +304,64 @@ __device__ __forceinline__ Chunk load_chunk(const Chunk* p) {
 
 // Sources, mark bits, marks of the lanes below, and first-mark row of warp
 // tile t (entries T .. T+255).
-__device__ __forceinline__ void fetch_tile(const WarpCtx& X, int32_t t, int32_t T, int lane, int4& ca, int4& cb,
-                                           uint32_t& bits, uint32_t& below, int32_t& row) {
-    const int4* c4 = reinterpret_cast<const int4*>(X.cols) + (T >> 2) + 2 * lane;
+__device__ __forceinline__ void fetch_tile(const int32_t* cols, const uint32_t* tile_bits, const int32_t* tile_row,
+                                           int32_t t, int32_t T, int lane, int4& ca, int4& cb, uint32_t& bits,
+                                           uint32_t& below, int32_t& row) {
+    const int4* c4 = reinterpret_cast<const int4*>(cols) + (T >> 2) + 2 * lane;
     ca = __ldcs(c4);
     cb = __ldcs(c4 + 1);
-    const uint32_t* tw = X.tile_bits + (size_t)t * kTileWords + (lane >> 2);
+    const uint32_t* tw = tile_bits + (size_t)t * kTileWords + (lane >> 2);
     const int sh = 8 * (lane & 3);
     bits = (__ldcs(tw) >> sh) & 0xffu;
     below = (__ldcs(tw + 8) >> sh) & 0xffu;
-    row = __ldcs(X.tile_row + t);
+    row = __ldcs(tile_row + t);
 }
 
 template <typename Real>
 __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, const WarpCtx& X,
                               const float* hub_s, int32_t hub_count, Real* scr) {
     constexpr bool kFinal = std::is_same<Real, double>::value;
+    using Acc = Real;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int32_t kb = ck.nnz_begin, ke = ck.nnz_end, T0 = kb & ~7;
     const int32_t fl = ck.flags;
     bool head_pending = (fl & kHasHead) && !(fl & kInterior);
     double head_val = 0.0;
-    double err = 0.0, dsum = 0.0, xsum = 0.0;
+    // per-lane sums of the chunk: residual and dangling mass in FP32 for the
+    // FP32 sweep (they steer the stop rule and the next dangling term, at far
+    // below FP32 iterate resolution), the rank sum always in FP64
+    Acc err = Acc(0), dsum = Acc(0);
+    double xsum = 0.0;
     Real carry = Real(0);  // the row still open at the end of the previous tile
+    // this chunk's pointers, held in registers
+    const int32_t* cols = X.cols;
+    const uint32_t* tbits = X.tile_bits;
+    const int32_t* trows = X.tile_row;
+    const float* zsrc = X.zsrc;
+    const float* hub_g = X.hub_g;
     int4 ca, cb;
     uint32_t bits, below;
     int32_t row;
-    fetch_tile(X, ck.sub_begin, T0, lane, ca, cb, bits, below, row);
+    fetch_tile(cols, tbits, trows, ck.sub_begin, T0, lane, ca, cb, bits, below, row);
     for (int32_t t = ck.sub_begin; t < ck.sub_end; ++t) {
         const int32_t T = T0 + (t - ck.sub_begin) * kTileItems;
         const int32_t cc[kLaneItems] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
         const uint32_t mb = bits;
         const int32_t pre = (int32_t)below;
         const int32_t r0 = row;
-        if (t + 1 < ck.sub_end) fetch_tile(X, t + 1, T + kTileItems, lane, ca, cb, bits, below, row);
+        if (t + 1 < ck.sub_end) fetch_tile(cols, tbits, trows, t + 1, T + kTileItems, lane, ca, cb, bits, below, row);
         // 1. gathers of this tile's entries (only a chunk's first and last
         //    tiles hold entries of other chunks)
         const int32_t p0 = T + kLaneItems * lane;
         Real v[kLaneItems];
+        // One load per entry through a generic pointer: z in global memory, or
+        // the hub copy in shared memory (global when not staged).
         auto carried = [&](int32_t s) -> Real {
             if (kFinal) return X.z64[s >= 0 ? s : __ldg(X.hub_ids + (-s - 1))];
             const int32_t h = -s - 1;
-            return s >= 0 ? X.zsrc[s] : (h < hub_count ? hub_s[h] : X.hub_g[h]);
+            const float* ptr = s >= 0 ? zsrc + s : (h < hub_count ? hub_s + h : hub_g + h);
+            return *ptr;
         };
         if (T >= kb && T + kTileItems <= ke) {
 #pragma unroll
@@ -419,19 +448,27 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
         if (nm > 0) head_pending = false;
         __syncwarp();
     }
-    err = warp_sum(err);
-    dsum = warp_sum(dsum);
+    const double err64 = warp_sum((double)err);
+    const double dsum64 = warp_sum((double)dsum);
     xsum = warp_sum(xsum);
     if (lane == 0) {
         unsigned long long* a = acc_slot(P, ck.graph, (int32_t)(blockIdx.x * kCtaWarps + (threadIdx.x >> 5)));
-        fx_add(a, err);
-        fx_add(a + 2, dsum);
+        fx_add(a, err64);
+        fx_add(a + 2, dsum64);
         fx_add(a + 4, xsum);
+        const int32_t slot = (int32_t)(blockIdx.x * kCtaWarps + (threadIdx.x >> 5));
         if (fl & kInterior) {
             fx_add(P.span_acc + 2 * ck.head_ta, (double)carry);
+            span_arrive<kFinal>(P, X.W, ck.head_ta, ck.pad, slot);
         } else {
-            if (fl & kHasHead) fx_add(P.span_acc + 2 * ck.head_ta, head_val);
-            if (fl & kHasTail) fx_add(P.span_acc + 2 * c, (double)carry);
+            if (fl & kHasHead) {
+                fx_add(P.span_acc + 2 * ck.head_ta, head_val);
+                span_arrive<kFinal>(P, X.W, ck.head_ta, ck.pad, slot);
+            }
+            if (fl & kHasTail) {
+                fx_add(P.span_acc + 2 * c, (double)carry);
+                span_arrive<kFinal>(P, X.W, c, ck.pad2, slot);
+            }
         }
     }
 }
@@ -704,6 +741,7 @@ SweepParams make_params(Plan& plan, int mode, int use_cond) {
     P.states = plan.d_states.as<GraphState>();
     P.acc = plan.d_acc.as<unsigned long long>();
     P.span_acc = plan.d_span_acc.as<unsigned long long>();
+    P.span_cnt = plan.d_span_cnt.as<uint32_t>();
     P.acc_sub = plan.nacc / std::max(1, plan.ngraphs);
     P.span_list = plan.d_span_list.as<int32_t>();
     P.nspans = plan.nspans;
@@ -859,8 +897,10 @@ int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_
     plan.any_weighted = any_w;
     plan.hub_count = count == 1 ? hub_stride(graphs[0]->nhub) : 0;
     plan.grid = std::max(1, std::min(plan.nchunks, sweep_grid()));
-    // accumulator slots: up to 512 per graph, fewer for many graphs
-    const int32_t per_graph = std::max(1, std::min(512, 8192 / std::max(1, count)));
+    // accumulator slots: 64 per graph (few for the launch's last CTA to read,
+    // enough that concurrent chunks rarely add to the same address), fewer
+    // for many graphs
+    const int32_t per_graph = std::max(1, std::min(64, 8192 / std::max(1, count)));
     plan.nacc = per_graph * count;
     plan.h_chunks_all = all;
     if (spans.empty()) spans.push_back(0);
@@ -871,6 +911,7 @@ int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_
         (rc = plan.d_ndang.alloc((size_t)count * sizeof(int32_t))) ||
         (rc = plan.d_acc.alloc((size_t)plan.nacc * kAccWords * sizeof(unsigned long long))) ||
         (rc = plan.d_span_acc.alloc(all.size() * 2 * sizeof(unsigned long long))) ||
+        (rc = plan.d_span_cnt.alloc(all.size() * sizeof(uint32_t))) ||
         (rc = plan.d_span_list.alloc(spans.size() * sizeof(int32_t))) || (rc = plan.d_ctl.alloc(sizeof(Ctl))))
         return rc;
     if ((rc = cuda_ok(cudaMemcpyAsync(plan.d_chunks.p, all.data(), all.size() * sizeof(Chunk), cudaMemcpyHostToDevice, stream), "H2D chunks")) ||
@@ -943,6 +984,7 @@ int launch_init(Plan& plan, double alpha, int32_t max_iter, double tol, bool per
     k_init_ctl<<<1, 1, 0, stream>>>(plan.d_ctl.as<Ctl>(), plan.ngraphs, max_iter + 1);
     cudaMemsetAsync(plan.d_acc.p, 0, plan.d_acc.bytes, stream);
     cudaMemsetAsync(plan.d_span_acc.p, 0, plan.d_span_acc.bytes, stream);
+    cudaMemsetAsync(plan.d_span_cnt.p, 0, plan.d_span_cnt.bytes, stream);
     return cuda_ok(cudaGetLastError(), "init launch");
 }
 
