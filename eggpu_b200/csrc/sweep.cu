@@ -381,6 +381,17 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
         }
         // 2. marks of the tile (pre: marks of the lanes below, from the tile table)
         const int32_t nm = __shfl_sync(kFull, pre + __popc(mb), 31);
+        if (nm == 0) {
+            // No row ends in this tile (inside a long row): its entries all join
+            // the open row.
+            Real part = v[0];
+#pragma unroll
+            for (int u = 1; u < kLaneItems; ++u) part += v[u];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+            carry = carry + part;
+            continue;
+        }
         // the rows this lane finishes first: request their data now
         float xin0 = 0.f, sc0 = 0.f;
         int32_t hs0 = -1;
