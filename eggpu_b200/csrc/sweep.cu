@@ -90,6 +90,12 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// Shared-memory load by 32-bit shared address (read-only data of the launch).
+__device__ __forceinline__ float lds_f32(uint32_t a) {
+    float x;
+    asm("ld.shared.f32 %0, [%1];" : "=f"(x) : "r"(a));
+    return x;
+}
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -291,6 +297,7 @@ struct WarpCtx {
     int32_t graph;
     int32_t iter;
     int32_t done;           // the graph had converged before this launch
+    int32_t hub_slots;      // hub codes of the graph: slots 0 .. nhub (the zero slot)
 };
 
 __device__ __forceinline__ Chunk load_chunk(const Chunk* p) {
@@ -340,6 +347,8 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
     const int32_t* trows = X.tile_row;
     const float* zsrc = X.zsrc;
     const float* hub_g = X.hub_g;
+    const bool hubs_local = hub_count >= X.hub_slots;       // every hub code reads shared memory
+    const uint32_t hub_m4 = smem_u32(hub_s) - 4u;           // shared address of hub slot -1
     int4 ca, cb;
     uint32_t bits, below;
     int32_t row;
@@ -355,13 +364,20 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
         //    tiles hold entries of other chunks)
         const int32_t p0 = T + kLaneItems * lane;
         Real v[kLaneItems];
-        // One load per entry through a generic pointer: z in global memory, or
-        // the hub copy in shared memory (global when not staged).
+        // One load per entry: z from global memory, a hub from the CTA's shared
+        // copy (predicated pair); a graph whose hubs are not all staged reads
+        // the rest of them from its global hub copy.
         auto carried = [&](int32_t s) -> Real {
             if (kFinal) return X.z64[s >= 0 ? s : __ldg(X.hub_ids + (-s - 1))];
-            const int32_t h = -s - 1;
-            const float* ptr = s >= 0 ? zsrc + s : (h < hub_count ? hub_s + h : hub_g + h);
-            return *ptr;
+            float x;
+            if (hubs_local) {
+                if (s >= 0) x = __ldg(zsrc + s);
+                else x = lds_f32(hub_m4 - 4u * (uint32_t)s);
+            } else {
+                const int32_t h = -s - 1;
+                x = s >= 0 ? __ldg(zsrc + s) : (h < hub_count ? lds_f32(hub_m4 - 4u * (uint32_t)s) : hub_g[h]);
+            }
+            return (Real)x;
         };
         if (T >= kb && T + kTileItems <= ke) {
 #pragma unroll
@@ -441,20 +457,15 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
         __syncwarp();
         // 5. finish the tile's rows; the chunk's first mark ends its head row
         //    (cut before the chunk), whose piece goes to the span instead
-        for (int32_t j = lane; j < nm; j += 32) {
-            const Real val = scr[j];
+        if (lane < nm) {
+            const Real val = scr[lane];
+            if (head_pending && lane == 0) head_val = (double)val;
+            else finish_row<kFinal>(X.W, r0 + lane, (double)val, xin0, sc0, hs0, err, dsum, xsum);
+        }
+        for (int32_t j = lane + 32; j < nm; j += 32) {  // tiles that end more than 32 rows
             const int32_t v0 = r0 + j;
-            float xi = xin0, sc = sc0;
-            int32_t hs = hs0;
-            if (j >= 32) {
-                xi = X.W.xin[v0];
-                if (!kFinal) {
-                    sc = X.W.scale[v0];
-                    hs = X.W.hub_slot[v0];
-                }
-            }
-            if (head_pending && j == 0) head_val = (double)val;
-            else finish_row<kFinal>(X.W, v0, (double)val, xi, sc, hs, err, dsum, xsum);
+            finish_row<kFinal>(X.W, v0, (double)scr[j], X.W.xin[v0], kFinal ? 0.f : X.W.scale[v0],
+                               kFinal ? -1 : X.W.hub_slot[v0], err, dsum, xsum);
         }
         if (nm > 0) head_pending = false;
         __syncwarp();
@@ -562,6 +573,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_sweep(SweepParams P) {
                         X.hub_g = G.hubz[iter & 1];
                         X.z64 = G.z64;
                         X.hub_ids = G.hub_ids;
+                        X.hub_slots = G.nhub + 1;
                         X.graph = gi;
                         X.iter = iter;
                         X.done = done;
