@@ -48,27 +48,104 @@ double wall_seconds() {
     return std::chrono::duration<double>(clock::now().time_since_epoch()).count();
 }
 
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+cudaStream_t g_alloc_streams[64] = {};
+
+int current_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return dev;
+}
+
+// A non-blocking stream per device that orders pool allocations and frees.
+cudaStream_t alloc_stream(int dev) {
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_alloc_streams[dev] && cudaStreamCreateWithFlags(&g_alloc_streams[dev], cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        g_alloc_streams[dev] = nullptr;
+    }
+    return g_alloc_streams[dev];
+}
+}  // namespace
+
+cudaMemPool_t device_pool() {
+    const int dev = current_device();
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        const char* e = std::getenv("EGPR_POOL_KEEP_MB");
+        const long long mb = e ? std::atoll(e) : 8192;
+        unsigned long long keep = (unsigned long long)std::max(0LL, mb) << 20;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pools[dev] = p;
+    }
+    return g_pools[dev];
+}
+
+// Device buffers come from the device pool: an allocation is ordered on the
+// device's allocation stream and waited for, so it is usable from any stream.
 int DevBuf::alloc(size_t b) {
     release();
     if (b == 0) b = 16;
-    cudaError_t e = cudaMalloc(&p, b);
+    const int d = current_device();
+    cudaMemPool_t pool = device_pool();
+    cudaStream_t s = alloc_stream(d);
+    cudaError_t e;
+    if (pool && s) {
+        e = cudaMallocFromPoolAsync(&p, b, pool, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        pooled = true;
+    } else {
+        e = cudaMalloc(&p, b);
+        pooled = false;
+    }
     if (e != cudaSuccess) {
+        if (p && pooled) cudaFreeAsync(p, s);
         p = nullptr;
-        set_cuda_error(e, "cudaMalloc");
+        cudaGetLastError();
+        set_cuda_error(e, "device allocation");
         return EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM;
     }
+    dev = d;
     bytes = b;
     g_live_bytes += (int64_t)b;
     return EGPR_SUCC;
 }
 
+// Like cudaFree, a release first waits for the device, so no launch still in
+// flight can read the buffer once the pool hands it out again.
 void DevBuf::release() {
     if (p) {
-        cudaFree(p);
+        if (pooled) {
+            int cur = current_device();
+            if (dev >= 0 && cur != dev) cudaSetDevice(dev);
+            cudaDeviceSynchronize();
+            cudaFreeAsync(p, alloc_stream(dev));
+            if (cur >= 0 && cur != dev) cudaSetDevice(cur);
+        } else {
+            cudaFree(p);
+        }
         g_live_bytes -= (int64_t)bytes;
     }
     p = nullptr;
     bytes = 0;
+    dev = -1;
+    pooled = false;
 }
 
 Plan::~Plan() { release(); }

@@ -138,6 +138,8 @@ struct SweepParams {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    int dev = -1;         // device of the allocation
+    bool pooled = false;  // from device_pool() (else cudaMalloc)
     int alloc(size_t b);
     void release();
     template <typename T>
@@ -209,6 +211,11 @@ struct egpr_graph {
 
 namespace egpr {
 
+// The library's memory pool of the current device: device buffers and
+// preparation scratch come from it, and it keeps up to EGPR_POOL_KEEP_MB
+// (default 8192) MiB of freed memory for reuse (null if pools are unavailable).
+cudaMemPool_t device_pool();
+
 // Status helpers.
 int set_cuda_error(cudaError_t e, const char* what);
 int check_device(const egpr_graph* g);
@@ -217,7 +224,7 @@ double wall_seconds();
 // Preparation (prep.cu).
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
 int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
-int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s);
+int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* sorted_dst, cudaStream_t s);
 int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
 
 // Plans and sweeps (sweep.cu).

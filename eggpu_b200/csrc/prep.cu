@@ -207,6 +207,30 @@ __global__ void k_out_weight(const int32_t* __restrict__ V, const int32_t* __res
     }
 }
 
+// Unit weights: the out-weight sum is the count of valid entries, exact in any
+// order, so one warp counts a row.
+__global__ void k_out_degree(const int32_t* __restrict__ V, const int32_t* __restrict__ E, int32_t n,
+                             double* __restrict__ outw, uint32_t* __restrict__ hub_key,
+                             uint32_t* __restrict__ hub_val) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = warp; u < n; u += nwarps) {
+        const int32_t b = V[u], e = V[u + 1];
+        int32_t c = 0;
+        for (int32_t p = b + lane; p < e; p += 32) {
+            const int32_t v = E[p];
+            c += (v >= 0 && v < n) ? 1 : 0;
+        }
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) {
+            outw[u] = (double)c;
+            hub_key[u] = ~(uint32_t)c;
+            hub_val[u] = (uint32_t)u;
+        }
+    }
+}
+
 __global__ void k_hub_slots(const uint32_t* __restrict__ ranked, int32_t nhub, int32_t* __restrict__ hub_ids,
                             int32_t* __restrict__ hub_slot) {
     for (int32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nhub; s += gridDim.x * blockDim.x) {
@@ -340,39 +364,10 @@ inline int grid_for(int64_t work, int per_block = kThreads) {
 
 int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SUCC : set_cuda_error(e, what); }
 
-// Stream-ordered scratch of the preparation comes from a pool per device that
-// keeps up to EGPR_SCRATCH_KEEP_MB (default 4096) MiB after it is freed, so
-// preparing graph after graph does not map fresh pages every time.
-cudaMemPool_t scratch_pool() {
-    static std::mutex mu;
-    static cudaMemPool_t pools[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    std::lock_guard<std::mutex> lock(mu);
-    if (!pools[dev]) {
-        cudaMemPoolProps props = {};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaMemPool_t p = nullptr;
-        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        const char* e = std::getenv("EGPR_SCRATCH_KEEP_MB");
-        const long long mb = e ? std::atoll(e) : 4096;
-        unsigned long long keep = (unsigned long long)std::max(0LL, mb) << 20;
-        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
-        pools[dev] = p;
-    }
-    return pools[dev];
-}
-
+// Stream-ordered scratch of the preparation comes from the library's device
+// pool (device_pool), which keeps freed memory for the next preparation.
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
-    cudaMemPool_t pool = scratch_pool();
+    cudaMemPool_t pool = device_pool();
     return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
 }
 
@@ -539,6 +534,30 @@ __global__ void k_tile_offsets(uint32_t* __restrict__ bits, int64_t ntiles) {
     }
 }
 
+// Entry i (destination dst[i]) of the inbound CSR to its place in the sweep's copy.
+__global__ void k_sweep_cols_by_entry(const uint32_t* __restrict__ dst, const int32_t* __restrict__ in_row,
+                                      const int32_t* __restrict__ in_col, const float* __restrict__ in_w, int64_t nnz,
+                                      const int32_t* __restrict__ sw_row, int32_t* __restrict__ sw_col,
+                                      float* __restrict__ sw_w) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = dst[i];
+        const int64_t o = i + (int64_t)(sw_row[r] - in_row[r]);
+        sw_col[o] = in_col[i];
+        if (sw_w) sw_w[o] = in_w[i];
+    }
+}
+
+// The placeholder entry of every empty row.
+__global__ void k_sweep_placeholders(const int32_t* __restrict__ in_row, int32_t n, const int32_t* __restrict__ sw_row,
+                                     int32_t* __restrict__ sw_col, float* __restrict__ sw_w, int32_t zero_code) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        if (in_row[r + 1] == in_row[r]) {
+            sw_col[sw_row[r]] = zero_code;
+            if (sw_w) sw_w[sw_row[r]] = 0.f;
+        }
+    }
+}
+
 namespace {
 
 int chunks_per_warp() {
@@ -578,7 +597,7 @@ int row_cost() {
 //     of the tile ends (the k-th mark of a tile ends row tile_row + k, since
 //     every row has an entry).
 // Chunks are stored costliest first, which is their queue order.
-int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
+int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* sorted_dst, cudaStream_t s) {
     const int32_t n = g->n;
     TmpAlloc tmp(s);
     int rc = EGPR_SUCC;
@@ -720,10 +739,20 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     // every entry is written below; only the padding past the last one is cleared
     if ((rc = cuda_ok(cudaMemsetAsync(g->sw_col.as<int32_t>() + nnz, 0, pad, s), "memset"))) return rc;
     if (g->weighted && (rc = cuda_ok(cudaMemsetAsync(g->sw_w.as<float>() + nnz, 0, pad, s), "memset"))) return rc;
-    k_build_sweep_cols<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(
-        g->in_row.as<int32_t>(), g->in_col.as<int32_t>(), g->weighted ? g->in_w.as<float>() : nullptr, n,
-        g->sw_row.as<int32_t>(), g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr,
-        -(g->nhub + 1));
+    if (sorted_dst && g->nnz > 0) {
+        // entry-parallel: entry i of row r moves by the number of empty rows before r
+        k_sweep_cols_by_entry<<<grid_for(g->nnz), kThreads, 0, s>>>(
+            sorted_dst, g->in_row.as<int32_t>(), g->in_col.as<int32_t>(), g->weighted ? g->in_w.as<float>() : nullptr,
+            g->nnz, g->sw_row.as<int32_t>(), g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr);
+        k_sweep_placeholders<<<grid_for(n), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, g->sw_row.as<int32_t>(),
+                                                             g->sw_col.as<int32_t>(),
+                                                             g->weighted ? g->sw_w.as<float>() : nullptr, -(g->nhub + 1));
+    } else {
+        k_build_sweep_cols<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(
+            g->in_row.as<int32_t>(), g->in_col.as<int32_t>(), g->weighted ? g->in_w.as<float>() : nullptr, n,
+            g->sw_row.as<int32_t>(), g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr,
+            -(g->nhub + 1));
+    }
     return cuda_ok(cudaStreamSynchronize(s), "sweep layout");
 }
 
@@ -808,10 +837,12 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             return rc;
         cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * sizeof(uint32_t), s);
         cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s);
-        k_out_weight<<<grid_for(n), kThreads, 0, s>>>(dV, dE, dW, n, g->outw.as<double>(), hkey, hval);
+        if (dW) k_out_weight<<<grid_for(n), kThreads, 0, s>>>(dV, dE, dW, n, g->outw.as<double>(), hkey, hval);
+        else k_out_degree<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, dE, n, g->outw.as<double>(), hkey, hval);
         if (m > 0) k_in_degree_keys<<<grid_for(m), kThreads, 0, s>>>(dE, m, n, indeg, keys, vals);
         if ((rc = exclusive_scan_u32(indeg, reinterpret_cast<uint32_t*>(g->in_row.as<int32_t>()), (int64_t)n + 1, s)))
             return rc;
+        const uint32_t* sorted_dst = nullptr;  // destination of every inbound entry, in entry order
         int32_t nnz32 = 0;
         if ((rc = cuda_ok(cudaMemcpyAsync(&nnz32, g->in_row.as<int32_t>() + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s), "D2H nnz")) ||
             (rc = cuda_ok(cudaStreamSynchronize(s), "preparation")))
@@ -830,6 +861,7 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             bool alt = false;
             if ((rc = radix_sort_pairs(keys, vals, keys2, vals2, m, bits, s, tmp, &alt))) return rc;
             const uint32_t* sorted_ids = alt ? vals2 : vals;
+            sorted_dst = alt ? keys2 : keys;
             k_expand_src<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, n, src);
             if (nnz > 0)
                 k_gather_inbound<<<grid_for(nnz), kThreads, 0, s>>>(sorted_ids, nnz, src, dW, g->in_col.as<int32_t>(),
@@ -870,7 +902,7 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                                                                        g->sub_coord.as<int2>());
         g->n_dangling = (int32_t)hc[0];
         g->n_dangling_solve = (int32_t)hc[1];
-        if ((rc = build_sweep_layout(g, sweep_resident_warps(), s))) return rc;
+        if ((rc = build_sweep_layout(g, sweep_resident_warps(), sorted_dst, s))) return rc;
     }
     cudaEventRecord(g->ev1, s);
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "preparation"))) return rc;
