@@ -218,6 +218,7 @@ cudaMemPool_t device_pool();
 
 // Status helpers.
 int set_cuda_error(cudaError_t e, const char* what);
+int arg_error(const char* why);  // EGPR_INVALID_ARGUMENT with a message
 int check_device(const egpr_graph* g);
 double wall_seconds();
 

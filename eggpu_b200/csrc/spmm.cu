@@ -4,27 +4,39 @@
 // Maths per column j (the reference's power iteration, easygraph/functions/
 // centrality/pagerank.py:112-139, with the (1-alpha)/n teleport term replaced
 // by (1-alpha) * p_j[v]; dangling mass stays uniform):
-//     X_new[v][j] = sum_{u -> v} w_uv * alpha * X[u][j] / outw[u]
+//     X_new[v][j] = alpha * sum_{u -> v} X[u][j] * w_uv / outw[u]
 //                 + (1-alpha) * p_j[v] + alpha * D_j / n
 // Column j stops on its own L1 rule err_j < tol*n and keeps its own count.
 //
-// Layout: columns in panels of 32 (one warp lane per column); X is
-// panel-major [panel][vertex][32] FP32, so gathering one source row of a panel
-// is one coalesced 128-byte load.  Teleport vectors are sparse per vertex
-// (seed sets), so the epilogue reads two offsets per row.
+// Layout, built once per graph and kept with it:
+//   * the entry stream: the inbound CSR in row order with one placeholder in
+//     every empty row (the sweep's padded CSR), padded with placeholders to a
+//     whole number of chunks.  Per entry the source vertex, with bit 31 set on
+//     the last entry of each row (placeholders read the all-zero row n), and
+//     the coefficient w / outw[source] in FP32 and in FP64 (0 for placeholders
+//     and for sources whose out-weight is at most 1e-15);
+//   * chunks of C consecutive entries (C a multiple of 32).  A row cut by a
+//     chunk boundary is a span: each chunk it touches stores its piece, and the
+//     last of them to arrive adds the pieces in chunk order and finishes the row
+//     (deterministic, no waiting);
+//   * iterates panel-major, [panel][n + 1][32] FP32: 32 columns per panel, so
+//     one source row of a panel is one 128-byte line; row n stays zero.
 //
-// Work split: the single-vector sweep's merge-path sub-tiles, with one warp per
-// 256-item slice of a sub-tile instead of one thread per 8 items: every warp
-// walks its slice once, its 32 lanes accumulating their 32 columns, with up to
-// kBatch gathers in flight.  Rows cut between warps, sub-tiles and chunks are
-// combined exactly as in the single-vector sweep (deterministic, no waiting).
-// Work units are (panel, chunk) pairs in panel-major order, so all CTAs sweep
-// one panel's working set at a time and each inbound entry loaded into shared
-// memory feeds 32 columns.
+// Sweep (one launch): warps claim (panel, chunk) units from a queue in
+// panel-major order, so all SMs gather from one 128 MB-class panel at a time.
+// A warp reads 32 entries with one coalesced load; its half-warps take the
+// even and the odd entries, each lane gathering two columns with one 8-byte
+// load (two source rows per warp instruction).  Row sums go to a per-warp
+// buffer in shared memory; the rows a batch finishes are then written in one
+// pass (previous iterate, teleport, dangling term), with their loads issued
+// together.  Column sums (residual, dangling mass, rank sum) are converted to
+// fixed point per chunk and added with integer atomics, so their value does not
+// depend on which warp ran which chunk.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -34,10 +46,26 @@
 namespace egpr {
 namespace {
 
-constexpr int kLanes = 32;
-constexpr int kWarpsS = kThreads / 32;
-constexpr int kItemsPerWarp = kSubItems / kWarpsS;
-constexpr int kBatch = 8;
+constexpr unsigned kAll = 0xffffffffu;
+constexpr int kLanes = 32;          // columns per panel
+constexpr int kSpWarps = 24;        // warps per CTA of the FP32 sweep (one CTA per SM)
+constexpr int kSpWarps64 = 16;      // of the FP64 sweep (its row buffers are twice as large)
+template <bool kF64>
+__host__ __device__ constexpr int sp_threads() { return 32 * (kF64 ? kSpWarps64 : kSpWarps); }
+constexpr int kMaxPanels = 16;      // panels of one device solve (larger batches run in groups)
+constexpr int kAccQ = 4;            // fixed-point words per column and panel
+constexpr int32_t kRowEnd = (int32_t)0x80000000u;  // entry: last of its row
+constexpr uint32_t kDangBit = 0x80000000u;         // row meta: dangling vertex
+
+struct SpChunk {
+    int32_t e0, e1;   // entries [e0, e1)
+    int32_t r0;       // the row of entry e0 (the chunk's first row end finishes it)
+    int32_t flags;    // kHasHead / kHasTail / kInterior
+    int32_t hkey;     // head (or interior) span: its first chunk
+    int32_t hparts;   // chunks of that span
+    int32_t tparts;   // tail span (first chunk = this one): chunks of it
+    int32_t trow;     // the row of entry e1 - 1
+};
 
 struct ColState {
     double dmass;
@@ -53,142 +81,494 @@ struct ColState {
 };
 
 struct SpmmParams {
-    const Chunk* chunks;
+    const SpChunk* chunks;
     int32_t nchunks;
     int32_t npanels;
     int32_t n;
+    int32_t tele_ld;          // floats per teleport row (npanels * 32)
     int32_t max_iter;
-    const int32_t* in_row;
-    const int32_t* in_col;   // hub entries store -(slot + 1)
-    const int32_t* hub_ids;
-    const float* in_w;
-    const int2* sub_coord;
-    const double* outw;
-    const float* scale;     // alpha/outw or -1 (dangling)
-    const int32_t* tele_ptr;  // n+1
-    const int32_t* tele_col;  // entries: column
-    const float* tele_val;    // entries: teleport probability
-    float* X[2];
-    double* out64;
+    const int32_t* src;       // entry stream: source | row-end bit
+    const float* coef32;
+    const double* coef64;
+    const uint32_t* meta;     // per vertex: dangling bit | teleport row + 1 (0: none)
+    const float* tele;        // teleport rows: p_j[v] for the vertices that have one
+    float* X[2];              // iterates, panel-major [panel][n + 1][32]
+    double* out64;            // FP64 result, same layout
     ColState* cols;
     double alpha;
     double tol_n;
-    double* chunk_part;   // [panel][chunk][3][32]
-    double* piece;        // [panel][chunk][2][32]
-    uint32_t* span_cnt;   // [panel][chunk]
-    double* span_part;    // [panel][chunk][3][32]
-    uint32_t* panel_arrive;
+    void* parts;              // [panel][chunk][2][32] pieces of cut rows (Real)
+    uint32_t* span_cnt;       // [panel][chunk] arrivals per span (reset by the last)
+    unsigned long long* gacc; // [panel][kAccQ][32] fixed-point column sums
     Ctl* ctl;
 };
 
+template <bool kF64>
+using RealT = typename std::conditional<kF64, double, float>::type;
+
 template <typename Real>
-struct SpmmSmem {
-    int32_t col[kSubItems];
-    float w[kSubItems];
-    float sc[kSubItems];        // FP32 sweep: max(scale, 0) of the source
-    double outw[kSubItems];     // FP64 sweep: out-weight of the source
-    int32_t rowend[kSubItems + 1];
-    Real first_val[kWarpsS][kLanes];
-    Real carry_val[kWarpsS][kLanes];
-    int32_t first_row[kWarpsS];
-    int32_t carry_row[kWarpsS];
-    Real sub_carry[kLanes];
-    Real head_val[kLanes];
-    double red[3][kWarpsS][kLanes];
-    int32_t head_pending;
-    int32_t unit;
-    int32_t is_last;
+struct V2 {
+    Real x, y;
 };
 
-__device__ __forceinline__ size_t pidx(int32_t p, int32_t c, int32_t nchunks) {
+template <bool kF64>
+struct SpSmem {
+    RealT<kF64> rows[kF64 ? kSpWarps64 : kSpWarps][32][kLanes];  // row sums of the batch in flight, per warp
+    unsigned long long acc[kMaxPanels][kAccQ][kLanes];
+    int32_t idle;
+};
+
+__device__ __forceinline__ size_t pc_index(int32_t p, int32_t c, int32_t nchunks) {
     return (size_t)p * (size_t)nchunks + (size_t)c;
 }
 
-struct LaneView {
-    const float* xin;   // this lane's previous iterate (panel base)
-    float* xout;        // FP32 sweep output (panel base)
-    double* out64;      // FP64 sweep output (panel base)
-    double dmass;
-    bool live;          // lane's column takes part
+// Fixed point.  FP32 sweep: one word in units of 2^-40 per quantity (a chunk's
+// per-column sums are below 2^10, their totals below 2^23).  FP64 sweep: two
+// words, units of 2^-32 and of 2^-64 (the remainder, rounded), as the
+// single-vector sweep keeps them.
+__device__ __forceinline__ unsigned long long fx40(double v) {
+    return (unsigned long long)__double2ll_rn(v * 1099511627776.0);
+}
+__device__ __forceinline__ double fx40_join(unsigned long long w) {
+    return (double)(long long)w * (1.0 / 1099511627776.0);
+}
+__device__ __forceinline__ void fx64_split(double v, unsigned long long& hi, unsigned long long& lo) {
+    const double t = v * 4294967296.0;  // exact
+    const double f = floor(t);
+    hi = (unsigned long long)(long long)f;
+    lo = (unsigned long long)rint((t - f) * 4294967296.0);
+}
+__device__ __forceinline__ double fx64_join(unsigned long long hi, unsigned long long lo) {
+    return (double)(long long)hi * (1.0 / 4294967296.0) + (double)lo * (1.0 / 18446744073709551616.0);
+}
+
+// Adds a lane's two columns of (err, dsum, xsum) to the CTA's accumulators of
+// panel p (lanes of the lower half-warp; each holds columns c2, c2 + 1).
+template <bool kF64>
+__device__ __forceinline__ void acc_add(SpSmem<kF64>& S, int32_t p, int c2, double e0, double e1, double d0,
+                                        double d1, double x0, double x1) {
+    unsigned long long* a = &S.acc[p][0][0];
+    if (!kF64) {
+        if (e0 != 0.0) atomicAdd(a + 0 * kLanes + c2, fx40(e0));
+        if (e1 != 0.0) atomicAdd(a + 0 * kLanes + c2 + 1, fx40(e1));
+        if (d0 != 0.0) atomicAdd(a + 1 * kLanes + c2, fx40(d0));
+        if (d1 != 0.0) atomicAdd(a + 1 * kLanes + c2 + 1, fx40(d1));
+        if (x0 != 0.0) atomicAdd(a + 2 * kLanes + c2, fx40(x0));
+        if (x1 != 0.0) atomicAdd(a + 2 * kLanes + c2 + 1, fx40(x1));
+    } else {
+        unsigned long long h, l;
+        fx64_split(e0, h, l);
+        atomicAdd(a + 0 * kLanes + c2, h);
+        atomicAdd(a + 1 * kLanes + c2, l);
+        fx64_split(e1, h, l);
+        atomicAdd(a + 0 * kLanes + c2 + 1, h);
+        atomicAdd(a + 1 * kLanes + c2 + 1, l);
+        fx64_split(x0, h, l);
+        atomicAdd(a + 2 * kLanes + c2, h);
+        atomicAdd(a + 3 * kLanes + c2, l);
+        fx64_split(x1, h, l);
+        atomicAdd(a + 2 * kLanes + c2 + 1, h);
+        atomicAdd(a + 3 * kLanes + c2 + 1, l);
+    }
+}
+
+// What a lane needs of the panel its warp works on.  The lane holds columns
+// c2 and c2 + 1 (c2 = 2 * (lane % 16)); both half-warps hold the same columns.
+template <bool kF64>
+struct Lane {
+    const float* xa;  // gathered iterate of column c2 (panel base); FP32 sweep: of both columns
+    const float* xb;  // FP64 sweep: of column c2 + 1
+    float* xout;      // FP32 sweep: the next iterate (panel base)
+    double* out64;    // FP64 sweep: the result (panel base)
+    RealT<kF64> dm0, dm1;  // dangling term of the two columns
+    int32_t p;
+    bool live0, live1;
 };
 
-template <typename Real>
-__device__ __forceinline__ void finish_row_s(const SpmmParams& P, const LaneView& L, int32_t col, int32_t v,
-                                             double acc, double& err, double& dsum, double& xsum) {
-    if (!L.live) return;
-    double t = 0.0;
-    const int32_t e0 = P.tele_ptr[v], e1 = P.tele_ptr[v + 1];
-    for (int32_t e = e0; e < e1; ++e)
-        if (P.tele_col[e] == col) t += (double)P.tele_val[e];
-    const double val = (acc + (1.0 - P.alpha) * t) + L.dmass;
-    const size_t off = (size_t)v * kLanes + (threadIdx.x & 31);
-    const double prev = (double)L.xin[off];
-    if constexpr (std::is_same<Real, float>::value) {
-        const float xo = (float)val;
-        err += fabs((double)xo - prev);
-        L.xout[off] = xo;
-        if (P.scale[v] < 0.f) dsum += (double)xo;
-        xsum += (double)xo;
+// Reads the lane's two column states for panel p; skip = no column of the
+// panel takes part in this sweep.
+template <bool kF64>
+__device__ Lane<kF64> make_lane(const SpmmParams& P, int32_t p, bool& skip) {
+    const int lane = threadIdx.x & 31, c2 = 2 * (lane & 15);
+    const ColState* cs = P.cols + (size_t)p * kLanes + c2;
+    const int32_t a0 = __ldcg(&cs[0].active), a1 = __ldcg(&cs[1].active);
+    const int32_t d0 = __ldcg(&cs[0].done), d1 = __ldcg(&cs[1].done);
+    const int32_t i0 = __ldcg(&cs[0].iter), i1 = __ldcg(&cs[1].iter);
+    const size_t pbase = (size_t)p * ((size_t)P.n + 1) * kLanes;
+    Lane<kF64> L;
+    L.p = p;
+    L.xout = nullptr;
+    L.out64 = nullptr;
+    if (!kF64) {
+        L.live0 = a0 && !d0;
+        L.live1 = a1 && !d1;
+        const unsigned lm = __ballot_sync(kAll, L.live0 || L.live1);
+        skip = lm == 0u;
+        // live columns of a panel have taken the same number of sweeps
+        const int32_t it = __shfl_sync(kAll, L.live0 ? i0 : i1, lm ? __ffs(lm) - 1 : 0);
+        const int par = it & 1;
+        L.xa = P.X[par] + pbase;
+        L.xb = L.xa;
+        L.xout = P.X[par ^ 1] + pbase;
+        L.dm0 = (RealT<kF64>)__ldcg(&cs[0].dmass);
+        L.dm1 = (RealT<kF64>)__ldcg(&cs[1].dmass);
     } else {
-        err += fabs(val - prev);
-        L.out64[off] = val;
-        xsum += val;
+        // each column's x_{k-1}, recomputed to x_k in FP64
+        L.live0 = a0 != 0;
+        L.live1 = a1 != 0;
+        skip = __ballot_sync(kAll, L.live0 || L.live1) == 0u;
+        L.xa = P.X[(i0 - 1) & 1] + pbase;
+        L.xb = P.X[(i1 - 1) & 1] + pbase;
+        L.out64 = P.out64 + pbase;
+        L.dm0 = (RealT<kF64>)__ldcg(&cs[0].dmass_prev);
+        L.dm1 = (RealT<kF64>)__ldcg(&cs[1].dmass_prev);
     }
+    return L;
 }
 
-// Warp-level span arrival (warp 0 of the CTA); pieces combined lane-wise in chunk order.
-template <typename Real>
-__device__ void span_arrive_s(const SpmmParams& P, const LaneView& L, int32_t col, int32_t p, int32_t ta,
-                              int32_t participants) {
-    const int lane = threadIdx.x & 31;
-    uint32_t prev = 0;
-    if (lane == 0) prev = atomicAdd(&P.span_cnt[pidx(p, ta, P.nchunks)], 1u);
-    prev = __shfl_sync(0xffffffffu, prev, 0);
-    if (prev != (uint32_t)(participants - 1)) return;
-    __threadfence();
-    const Chunk cta = P.chunks[ta];
-    const int32_t tb = cta.tail_tb;
-    double sum = __ldcg(&P.piece[(pidx(p, ta, P.nchunks) * 2 + 1) * kLanes + lane]);
-    for (int32_t q = ta + 1; q < tb; ++q) sum += __ldcg(&P.piece[(pidx(p, q, P.nchunks) * 2 + 1) * kLanes + lane]);
-    sum += __ldcg(&P.piece[(pidx(p, tb, P.nchunks) * 2) * kLanes + lane]);
-    if (lane == 0) P.span_cnt[pidx(p, ta, P.nchunks)] = 0u;
-    double e = 0.0, d = 0.0, x = 0.0;
-    finish_row_s<Real>(P, L, col, cta.tail_row, sum, e, d, x);
-    double* sp = P.span_part + pidx(p, ta, P.nchunks) * 3 * kLanes;
-    sp[lane] = e;
-    sp[kLanes + lane] = d;
-    sp[2 * kLanes + lane] = x;
-    __threadfence();
-}
+// Per-lane sums of a chunk (at most a few thousand rows) for its two columns,
+// in the sweep's precision; each chunk's sums are then added as fixed point.
+template <bool kF64>
+struct LaneSums {
+    RealT<kF64> e0 = 0, e1 = 0;  // residual
+    RealT<kF64> d0 = 0, d1 = 0;  // dangling mass (FP32 sweep)
+    RealT<kF64> x0 = 0, x1 = 0;  // rank sum
+};
 
-template <typename Real>
-__device__ void panel_reduce(const SpmmParams& P, SpmmSmem<Real>& S, int32_t p) {
-    __threadfence();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double e = 0.0, d = 0.0, x = 0.0;
-    for (int32_t c = warp; c < P.nchunks; c += kWarpsS) {
-        const size_t b = pidx(p, c, P.nchunks) * 3 * kLanes;
-        e += __ldcg(&P.chunk_part[b + lane]) + __ldcg(&P.span_part[b + lane]);
-        d += __ldcg(&P.chunk_part[b + kLanes + lane]) + __ldcg(&P.span_part[b + kLanes + lane]);
-        x += __ldcg(&P.chunk_part[b + 2 * kLanes + lane]) + __ldcg(&P.span_part[b + 2 * kLanes + lane]);
-        P.span_part[b + lane] = 0.0;
-        P.span_part[b + kLanes + lane] = 0.0;
-        P.span_part[b + 2 * kLanes + lane] = 0.0;
+// One finished row v of the lane's two columns: rs = sum of the inbound
+// terms without alpha, pa/pb = previous value of the columns, mt = row meta.
+template <bool kF64>
+__device__ __forceinline__ void row_out(const SpmmParams& P, const Lane<kF64>& L, int c2, int32_t v,
+                                        RealT<kF64> rsx, RealT<kF64> rsy, RealT<kF64> pa, RealT<kF64> pb,
+                                        uint32_t mt, LaneSums<kF64>& A) {
+    using Real = RealT<kF64>;
+    const Real alpha = (Real)P.alpha, oma = (Real)(1.0 - P.alpha);
+    Real tx = Real(0), ty = Real(0);
+    const uint32_t t = mt & ~kDangBit;
+    if (t) {  // a teleport row (seed vertices only)
+        const float2 tl =
+            __ldg(reinterpret_cast<const float2*>(P.tele + (size_t)(t - 1) * (size_t)P.tele_ld + L.p * kLanes + c2));
+        tx = (Real)tl.x;
+        ty = (Real)tl.y;
     }
-    S.red[0][warp][lane] = e;
-    S.red[1][warp][lane] = d;
-    S.red[2][warp][lane] = x;
-    __syncthreads();
-    if (warp == 0) {
-        e = 0.0; d = 0.0; x = 0.0;
-        for (int w = 0; w < kWarpsS; ++w) {
-            e += S.red[0][w][lane];
-            d += S.red[1][w][lane];
-            x += S.red[2][w][lane];
+    const Real vx = fma(alpha, rsx, fma(oma, tx, L.dm0));
+    const Real vy = fma(alpha, rsy, fma(oma, ty, L.dm1));
+    const size_t off = (size_t)v * kLanes + c2;
+    if (!kF64) {
+        float* o = L.xout + off;
+        if (L.live0 && L.live1) {
+            __stcs(reinterpret_cast<float2*>(o), make_float2((float)vx, (float)vy));
+        } else {
+            if (L.live0) __stcs(o, (float)vx);
+            if (L.live1) __stcs(o + 1, (float)vy);
         }
-        ColState* cs = P.cols + (size_t)p * kLanes + lane;
-        if constexpr (std::is_same<Real, float>::value) {
+    } else {
+        double* o = L.out64 + off;
+        if (L.live0 && L.live1) {
+            *reinterpret_cast<double2*>(o) = make_double2((double)vx, (double)vy);
+        } else {
+            if (L.live0) o[0] = (double)vx;
+            if (L.live1) o[1] = (double)vy;
+        }
+    }
+    const bool dang = (mt & kDangBit) != 0u;
+    if (L.live0) {
+        A.e0 += fabs(vx - pa);
+        A.x0 += vx;
+        if (!kF64 && dang) A.d0 += vx;
+    }
+    if (L.live1) {
+        A.e1 += fabs(vy - pb);
+        A.x1 += vy;
+        if (!kF64 && dang) A.d1 += vy;
+    }
+}
+
+template <bool kF64>
+__device__ __forceinline__ RealT<kF64>* part_ptr(const SpmmParams& P, int32_t p, int32_t c, int slot) {
+    return reinterpret_cast<RealT<kF64>*>(P.parts) + (pc_index(p, c, P.nchunks) * 2 + (size_t)slot) * kLanes;
+}
+
+template <bool kF64>
+__device__ __forceinline__ V2<RealT<kF64>> load_part(const SpmmParams& P, int32_t p, int32_t c, int slot, int c2) {
+    const RealT<kF64>* q = part_ptr<kF64>(P, p, c, slot) + c2;
+    V2<RealT<kF64>> r;
+    if (!kF64) {
+        const float2 v = __ldcg(reinterpret_cast<const float2*>(q));
+        r.x = v.x;
+        r.y = v.y;
+    } else {
+        const double2 v = __ldcg(reinterpret_cast<const double2*>(q));
+        r.x = v.x;
+        r.y = v.y;
+    }
+    return r;
+}
+
+template <bool kF64>
+__device__ __forceinline__ void store_part(const SpmmParams& P, int32_t p, int32_t c, int slot, int c2,
+                                           RealT<kF64> x, RealT<kF64> y) {
+    RealT<kF64>* q = part_ptr<kF64>(P, p, c, slot) + c2;
+    q[0] = x;
+    q[1] = y;
+}
+
+// The previous value of the lane's two columns at row v.
+template <bool kF64>
+__device__ __forceinline__ void prev_of(const Lane<kF64>& L, int c2, int32_t v, RealT<kF64>& a, RealT<kF64>& b) {
+    const size_t off = (size_t)v * kLanes + c2;
+    if (!kF64) {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(L.xa + off));
+        a = q.x;
+        b = q.y;
+    } else {
+        a = (double)__ldg(L.xa + off);
+        b = (double)__ldg(L.xb + off + 1);
+    }
+}
+
+// A chunk's piece of span `key` (spanning `parts` chunks) is stored.  The last
+// of the span's chunks to arrive adds the pieces in chunk order (the first
+// chunk's tail piece, whole chunks, the last chunk's head piece) and finishes
+// the row; its column sums are added on their own, so the totals do not depend
+// on which chunk that was.
+template <bool kF64>
+__device__ void span_arrive(const SpmmParams& P, SpSmem<kF64>& S, const Lane<kF64>& L, int32_t p, int32_t key,
+                            int32_t parts) {
+    using Real = RealT<kF64>;
+    const int lane = threadIdx.x & 31, g = lane >> 4, c2 = 2 * (lane & 15);
+    uint32_t prev = 0;
+    if (lane == 0) prev = atomicAdd(&P.span_cnt[pc_index(p, key, P.nchunks)], 1u);
+    prev = __shfl_sync(kAll, prev, 0);
+    if (prev != (uint32_t)(parts - 1)) return;
+    __threadfence();
+    if (lane == 0) P.span_cnt[pc_index(p, key, P.nchunks)] = 0u;
+    if (g != 0) return;
+    const int32_t cb = key + parts - 1;
+    V2<Real> s = load_part<kF64>(P, p, key, 1, c2);
+    for (int32_t q = key + 1; q < cb; ++q) {
+        const V2<Real> t = load_part<kF64>(P, p, q, 0, c2);
+        s.x += t.x;
+        s.y += t.y;
+    }
+    {
+        const V2<Real> t = load_part<kF64>(P, p, cb, 0, c2);
+        s.x += t.x;
+        s.y += t.y;
+    }
+    const int32_t v = __ldg(&P.chunks[key].trow);
+    Real pa, pb;
+    prev_of<kF64>(L, c2, v, pa, pb);
+    LaneSums<kF64> A;
+    row_out<kF64>(P, L, c2, v, s.x, s.y, pa, pb, __ldg(P.meta + v), A);
+    acc_add<kF64>(S, p, c2, (double)A.e0, (double)A.e1, (double)A.d0, (double)A.d1, (double)A.x0, (double)A.x1);
+}
+
+// One (panel, chunk) unit.
+template <bool kF64>
+__device__ void process_unit(const SpmmParams& P, SpSmem<kF64>& S, int32_t p, int32_t c, const Lane<kF64>& L) {
+    using Real = RealT<kF64>;
+    using Coef = RealT<kF64>;  // FP32 coefficients for the FP32 sweep, FP64 ones for the FP64 sweep
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 4, c2 = 2 * (lane & 15);
+    SpChunk ck;
+    {
+        const int4* q = reinterpret_cast<const int4*>(P.chunks + c);
+        const int4 a = __ldg(q), b = __ldg(q + 1);
+        ck.e0 = a.x; ck.e1 = a.y; ck.r0 = a.z; ck.flags = a.w;
+        ck.hkey = b.x; ck.hparts = b.y; ck.tparts = b.z; ck.trow = b.w;
+    }
+    Real(*rows)[kLanes] = S.rows[warp];
+    const int32_t* __restrict__ src = P.src;
+    const Coef* __restrict__ coef = kF64 ? reinterpret_cast<const Coef*>(P.coef64)
+                                         : reinterpret_cast<const Coef*>(P.coef32);
+    const float* __restrict__ xa = L.xa;
+    const float* __restrict__ xb = L.xb;
+    Real ax = Real(0), ay = Real(0);  // this half-warp's part of the open row
+    LaneSums<kF64> A;
+    int32_t rb = ck.r0;  // the row the next row end finishes
+    bool head_pending = (ck.flags & kHasHead) && !(ck.flags & kInterior);
+    int32_t ent = __ldcs(src + ck.e0 + lane);
+    Coef cf = __ldcs(coef + ck.e0 + lane);
+    for (int32_t b = ck.e0; b < ck.e1; b += 32) {
+        const int32_t ec = ent;
+        const Coef cc = cf;
+        if (b + 32 < ck.e1) {
+            ent = __ldcs(src + b + 32 + lane);
+            cf = __ldcs(coef + b + 32 + lane);
+        }
+        const uint32_t m = __ballot_sync(kAll, ec < 0);
+        const int nr = __popc(m);
+        uint32_t mt = 0u;  // meta of the batch's rows, lane k: row rb + k
+        if (lane < nr) mt = __ldg(P.meta + rb + lane);
+        int ord = 0;
+        auto emit = [&](Real tx, Real ty) {
+            const Real sx = tx + __shfl_xor_sync(kAll, tx, 16);
+            const Real sy = ty + __shfl_xor_sync(kAll, ty, 16);
+            if (g == 0) *reinterpret_cast<V2<Real>*>(&rows[ord][c2]) = V2<Real>{sx, sy};
+            ++ord;
+        };
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            Real gx[8], gy[8];
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                const int32_t u = __shfl_sync(kAll, ec, 16 * h + 2 * s + g) & 0x7fffffff;
+                const size_t off = (size_t)u * kLanes + c2;
+                if (!kF64) {
+                    const float2 v = __ldg(reinterpret_cast<const float2*>(xa + off));
+                    gx[s] = v.x;
+                    gy[s] = v.y;
+                } else {
+                    gx[s] = (Real)__ldg(xa + off);
+                    gy[s] = (Real)__ldg(xb + off + 1);
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                const Coef q = __shfl_sync(kAll, cc, 16 * h + 2 * s + g);
+                const uint32_t mp = (m >> (16 * h + 2 * s)) & 3u;  // row ends at the even / odd entry
+                if (mp == 0u) {
+                    ax = fma(q, gx[s], ax);
+                    ay = fma(q, gy[s], ay);
+                } else {
+                    const Real px = q * gx[s], py = q * gy[s];
+                    if (mp & 1u) {
+                        emit(g == 0 ? ax + px : ax, g == 0 ? ay + py : ay);
+                        ax = g == 0 ? Real(0) : px;
+                        ay = g == 0 ? Real(0) : py;
+                    } else {
+                        ax += px;
+                        ay += py;
+                    }
+                    if (mp & 2u) {
+                        emit(ax, ay);
+                        ax = Real(0);
+                        ay = Real(0);
+                    }
+                }
+            }
+        }
+        if (nr == 0) continue;
+        __syncwarp();
+        int k0 = 0;
+        if (head_pending) {  // the chunk's first row end finishes a row cut before it: its piece
+            if (g == 0) store_part<kF64>(P, p, c, 0, c2, rows[0][c2], rows[0][c2 + 1]);
+            head_pending = false;
+            k0 = 1;
+        }
+        // the batch's rows: half-warp g takes rows k0 + g, k0 + g + 2, ...
+        for (int kk = k0; kk < nr; kk += 8) {
+            Real pa[4], pb[4];
+            uint32_t mr[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int k = kk + 2 * i + g;
+                mr[i] = __shfl_sync(kAll, mt, k & 31);
+                if (k < nr) prev_of<kF64>(L, c2, rb + k, pa[i], pb[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int k = kk + 2 * i + g;
+                if (k < nr) row_out<kF64>(P, L, c2, rb + k, rows[k][c2], rows[k][c2 + 1], pa[i], pb[i], mr[i], A);
+            }
+        }
+        rb += nr;
+        __syncwarp();
+    }
+    // the row still open at the end of the chunk: the chunk's piece of a span
+    const int32_t f = ck.flags;
+    if (f & kHasTail) {
+        const Real tx = ax + __shfl_xor_sync(kAll, ax, 16);
+        const Real ty = ay + __shfl_xor_sync(kAll, ay, 16);
+        if (g == 0) store_part<kF64>(P, p, c, (f & kInterior) ? 0 : 1, c2, tx, ty);
+    }
+    // the chunk's column sums (both half-warps, fixed order)
+    {
+        const double e0 = (double)A.e0 + (double)__shfl_xor_sync(kAll, A.e0, 16);
+        const double e1 = (double)A.e1 + (double)__shfl_xor_sync(kAll, A.e1, 16);
+        const double d0 = (double)A.d0 + (double)__shfl_xor_sync(kAll, A.d0, 16);
+        const double d1 = (double)A.d1 + (double)__shfl_xor_sync(kAll, A.d1, 16);
+        const double x0 = (double)A.x0 + (double)__shfl_xor_sync(kAll, A.x0, 16);
+        const double x1 = (double)A.x1 + (double)__shfl_xor_sync(kAll, A.x1, 16);
+        if (g == 0) acc_add<kF64>(S, p, c2, e0, e1, d0, d1, x0, x1);
+    }
+    if (f & (kHasHead | kHasTail)) {
+        __threadfence();  // the pieces before the arrivals
+        __syncwarp();
+        if (f & kInterior) {
+            span_arrive<kF64>(P, S, L, p, ck.hkey, ck.hparts);
+        } else {
+            if (f & kHasHead) span_arrive<kF64>(P, S, L, p, ck.hkey, ck.hparts);
+            if (f & kHasTail) span_arrive<kF64>(P, S, L, p, c, ck.tparts);
+        }
+    }
+}
+
+// The sweep: persistent CTAs, warps claiming units; the last CTA to finish
+// turns the column sums into the column states (pagerank.py:117-131 per
+// column) and decides whether the CUDA-graph loop runs another sweep.
+template <bool kF64>
+__global__ void __launch_bounds__(sp_threads<kF64>(), 1)
+k_spmm(const SpmmParams* __restrict__ Pd, cudaGraphConditionalHandle cond, int32_t use_cond) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SpSmem<kF64>& S = *reinterpret_cast<SpSmem<kF64>*>(smem_raw);
+    __shared__ SpmmParams P;
+    __shared__ int32_t s_last;
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) {
+        P = *Pd;
+        S.idle = (!kF64 && __ldcg(&Pd->ctl->active) <= 0) ? 1 : 0;
+    }
+    __syncthreads();
+    const int32_t nacc = P.npanels * kAccQ * kLanes;
+    unsigned long long* sacc = &S.acc[0][0][0];
+    for (int32_t i = tid; i < nacc; i += sp_threads<kF64>()) sacc[i] = 0ull;
+    __syncthreads();
+    if (!S.idle) {
+        const int32_t units = P.npanels * P.nchunks;
+        int32_t u = 0;
+        if (lane == 0) u = (int32_t)atomicAdd(&P.ctl->queue, 1u);
+        u = __shfl_sync(kAll, u, 0);
+        int32_t cur = -1;
+        bool skip = true;
+        Lane<kF64> L;
+        while (u < units) {
+            int32_t next = 0;
+            if (lane == 0) next = (int32_t)atomicAdd(&P.ctl->queue, 1u);  // claimed one ahead
+            const int32_t p = u / P.nchunks, c = u - p * P.nchunks;
+            if (p != cur) {
+                L = make_lane<kF64>(P, p, skip);
+                cur = p;
+            }
+            if (!skip) process_unit<kF64>(P, S, p, c, L);
+            u = __shfl_sync(kAll, next, 0);
+        }
+    }
+    __syncthreads();
+    for (int32_t i = tid; i < nacc; i += sp_threads<kF64>()) {
+        const unsigned long long w = sacc[i];
+        if (w) atomicAdd(P.gacc + i, w);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(&P.ctl->exited, 1u) == gridDim.x - 1 ? 1 : 0;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int32_t j = tid; j < P.npanels * kLanes; j += sp_threads<kF64>()) {
+        const int32_t p = j / kLanes, col = j - p * kLanes;
+        unsigned long long w[kAccQ];
+#pragma unroll
+        for (int q = 0; q < kAccQ; ++q) {
+            unsigned long long* a = P.gacc + ((size_t)p * kAccQ + q) * kLanes + col;
+            w[q] = __ldcg(a);
+            *a = 0ull;
+        }
+        ColState* cs = P.cols + j;
+        if (!kF64) {
             if (cs->active && !cs->done) {
+                const double e = fx40_join(w[0]), d = fx40_join(w[1]), x = fx40_join(w[2]);
                 cs->residual = e;
                 cs->dsum = d;
                 cs->xsum = x;
@@ -203,252 +583,131 @@ __device__ void panel_reduce(const SpmmParams& P, SpmmSmem<Real>& S, int32_t p) 
                     atomicSub(&P.ctl->active, 1);
                 }
             }
-        } else {
-            if (cs->active) {
-                cs->residual64 = e;
-                cs->xsum = x;
-            }
+        } else if (cs->active) {
+            cs->residual64 = fx64_join(w[0], w[1]);
+            cs->xsum = fx64_join(w[2], w[3]);
         }
-        if (lane == 0) P.panel_arrive[p] = 0u;
-        __threadfence();
     }
+    __threadfence();
     __syncthreads();
-}
-
-template <typename Real>
-__device__ void process_unit(const SpmmParams& P, int32_t p, int32_t c, SpmmSmem<Real>& S) {
-    constexpr bool kFinal = std::is_same<Real, double>::value;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int32_t col = p * kLanes + lane;
-    const ColState cs = P.cols[col];
-    const size_t pbase = (size_t)p * (size_t)P.n * kLanes;
-    LaneView L;
-    if (!kFinal) {
-        L.live = cs.active && !cs.done;
-        const unsigned live_mask = __ballot_sync(0xffffffffu, L.live);
-        if (live_mask == 0u) return;  // whole panel frozen (same answer in every warp)
-        const int src_lane = __ffs(live_mask) - 1;
-        const int32_t it = __shfl_sync(0xffffffffu, cs.iter, src_lane);  // active columns share the count
-        const int par = it & 1;
-        L.xin = P.X[par] + pbase;
-        L.xout = P.X[par ^ 1] + pbase;
-        L.out64 = nullptr;
-        L.dmass = cs.dmass;
-    } else {
-        L.live = cs.active != 0;
-        const int par = (cs.iter - 1) & 1;  // x_{k-1} of this column
-        L.xin = P.X[par] + pbase;
-        L.xout = nullptr;
-        L.out64 = P.out64 + pbase;
-        L.dmass = cs.dmass_prev;
-    }
-    // Gather base: the previous iterate of the active columns (FP32 sweep) or
-    // each column's x_{k-1} (FP64 sweep).
-    const float* __restrict__ gbase = L.xin;
-    const Chunk ck = P.chunks[c];
-    double err = 0.0, dsum = 0.0, xsum = 0.0;
-    if (tid < kLanes) {
-        S.sub_carry[tid] = Real(0);
-        S.head_val[tid] = Real(0);
-    }
-    if (tid == 0) S.head_pending = (ck.flags & kHasHead) ? 1 : 0;
-    for (int32_t sidx = ck.sub_begin; sidx < ck.sub_end; ++sidx) {
-        const int2 a = P.sub_coord[sidx];
-        const int2 b = P.sub_coord[sidx + 1];
-        const int32_t ra = a.x, ka = a.y;
-        const int32_t nnz_sub = b.y - a.y;
-        const int32_t nrows = b.x - a.x;
-        for (int32_t i = tid; i < nnz_sub; i += kThreads) {
-            const int32_t cu = P.in_col[ka + i];
-            const int32_t u = cu >= 0 ? cu : P.hub_ids[-cu - 1];  // hub entries store -(slot + 1)
-            S.col[i] = u;
-            S.w[i] = P.in_w ? P.in_w[ka + i] : 1.0f;
-            if constexpr (kFinal) S.outw[i] = P.outw[u];
-            else S.sc[i] = fmaxf(P.scale[u], 0.f);
-        }
-        for (int32_t i = tid; i < nrows; i += kThreads) S.rowend[i] = P.in_row[ra + i + 1] - ka;
-        __syncthreads();
-        // This warp's slice of the merge path: [d0, d1).
-        const int32_t total = nrows + nnz_sub;
-        const int32_t d0 = min(warp * kItemsPerWarp, total);
-        const int32_t d1 = min(d0 + kItemsPerWarp, total);
-        auto search = [&](int32_t diag) {
-            int32_t lo = max(diag - nnz_sub, 0), hi = min(diag, nrows);
-            while (lo < hi) {
-                const int32_t mid = (lo + hi) >> 1;
-                if (S.rowend[mid] <= diag - mid - 1) lo = mid + 1;
-                else hi = mid;
-            }
-            return lo;
-        };
-        const int32_t i0 = search(d0), i1 = search(d1);
-        const int32_t j0 = d0 - i0, j1 = d1 - i1;
-        int32_t i = i0;
-        Real acc = Real(0);
-        int32_t first = -1;
-        auto complete_row = [&](int32_t r) {
-            if (first < 0) {
-                first = r;
-                S.first_val[warp][lane] = acc;
-            } else if (!(r == 0 && S.head_pending)) {
-                finish_row_s<Real>(P, L, col, ra + r, (double)acc, err, dsum, xsum);
-            }
-            acc = Real(0);
-        };
-        for (int32_t jb = j0; jb < j1; jb += kBatch) {
-            Real v[kBatch];
-#pragma unroll
-            for (int q = 0; q < kBatch; ++q) {
-                const int32_t jj = jb + q;
-                if (jj < j1) {
-                    const int32_t u = S.col[jj];
-                    if constexpr (kFinal) {
-                        const double o = S.outw[jj];
-                        const double xv = (double)gbase[(size_t)u * kLanes + lane];
-                        v[q] = o <= 1e-15 ? 0.0 : P.alpha * xv / o;
-                    } else {
-                        v[q] = gbase[(size_t)u * kLanes + lane] * S.sc[jj];
-                    }
-                } else {
-                    v[q] = Real(0);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < kBatch; ++q) {
-                const int32_t jj = jb + q;
-                if (jj < j1) {
-                    while (i < i1 && S.rowend[i] <= jj) {
-                        complete_row(i);
-                        ++i;
-                    }
-                    acc += (Real)S.w[jj] * v[q];
-                }
-            }
-        }
-        while (i < i1) {
-            complete_row(i);
-            ++i;
-        }
-        if (lane == 0) {
-            S.first_row[warp] = first;
-            S.carry_row[warp] = i;
-        }
-        S.carry_val[warp][lane] = acc;
-        __syncthreads();
-        // Fix-up of each warp's first completed row with the earlier warps' carries.
-        const int32_t fr = S.first_row[warp];
-        const Real cin = S.sub_carry[lane];
-        if (fr >= 0) {
-            Real vsum = S.first_val[warp][lane];
-            int32_t t = warp - 1;
-            while (t >= 0 && S.carry_row[t] == fr) {
-                vsum += S.carry_val[t][lane];
-                --t;
-            }
-            if (t < 0 && fr == 0) vsum += cin;
-            if (fr == 0 && S.head_pending) S.head_val[lane] = vsum;
-            else finish_row_s<Real>(P, L, col, ra + fr, (double)vsum, err, dsum, xsum);
-        }
-        Real out_carry = Real(0);
-        if (warp == kWarpsS - 1) {
-            int32_t t = kWarpsS - 1;
-            while (t >= 0 && S.carry_row[t] == nrows) {
-                out_carry += S.carry_val[t][lane];
-                --t;
-            }
-            if (t < 0 && nrows == 0) out_carry += cin;
-        }
-        __syncthreads();
-        if (warp == kWarpsS - 1) S.sub_carry[lane] = out_carry;
-        if (tid == 0 && nrows > 0) S.head_pending = 0;
-    }
-    __syncthreads();
-    // Per-column partials of this unit (fixed order over warps).
-    S.red[0][warp][lane] = err;
-    S.red[1][warp][lane] = dsum;
-    S.red[2][warp][lane] = xsum;
-    __syncthreads();
-    if (warp == 0) {
-        double e = 0.0, d = 0.0, x = 0.0;
-        for (int w = 0; w < kWarpsS; ++w) {
-            e += S.red[0][w][lane];
-            d += S.red[1][w][lane];
-            x += S.red[2][w][lane];
-        }
-        const size_t u = pidx(p, c, P.nchunks);
-        P.chunk_part[u * 3 * kLanes + lane] = e;
-        P.chunk_part[u * 3 * kLanes + kLanes + lane] = d;
-        P.chunk_part[u * 3 * kLanes + 2 * kLanes + lane] = x;
-        const int32_t f = ck.flags;
-        if ((f & kHasHead) && !(f & kInterior)) P.piece[(u * 2) * kLanes + lane] = (double)S.head_val[lane];
-        if (f & kHasTail) P.piece[(u * 2 + 1) * kLanes + lane] = (double)S.sub_carry[lane];
-        __threadfence();
-        if (f & kInterior) {
-            span_arrive_s<Real>(P, L, col, p, ck.head_ta, ck.tail_tb - ck.head_ta + 1);
-        } else {
-            if (f & kHasHead) span_arrive_s<Real>(P, L, col, p, ck.head_ta, c - ck.head_ta + 1);
-            if (f & kHasTail) span_arrive_s<Real>(P, L, col, p, c, ck.tail_tb - c + 1);
+    if (tid == 0) {
+        P.ctl->queue = 0u;
+        P.ctl->exited = 0u;
+        if (!kF64) {
+            const int32_t launches = P.ctl->launches + 1;
+            P.ctl->launches = launches;
+            const int32_t active = __ldcg(&P.ctl->active);
+            const bool more = active > 0 && launches < P.ctl->cap;
+            if (active > 0 && launches >= P.ctl->cap) P.ctl->error = EGPR_TIMEOUT;
+            if (use_cond) cudaGraphSetConditional(cond, more ? 1u : 0u);
         }
         __threadfence();
-        uint32_t prev = 0;
-        if (lane == 0) prev = atomicAdd(&P.panel_arrive[p], 1u);
-        if (lane == 0) S.is_last = (prev == (uint32_t)(P.nchunks - 1)) ? 1 : 0;
-    }
-    __syncthreads();
-    if (S.is_last) panel_reduce<Real>(P, S, p);
-    __syncthreads();
-}
-
-template <typename Real>
-__global__ void __launch_bounds__(kThreads)
-k_spmm(const SpmmParams* __restrict__ Pdev, cudaGraphConditionalHandle cond, int32_t use_cond) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SpmmSmem<Real>& S = *reinterpret_cast<SpmmSmem<Real>*>(smem_raw);
-    __shared__ SpmmParams P;
-    if (threadIdx.x == 0) P = *Pdev;
-    __syncthreads();
-    constexpr bool kFinal = std::is_same<Real, double>::value;
-    const bool idle = !kFinal && __ldcg(&P.ctl->active) <= 0;
-    const int32_t units = P.npanels * P.nchunks;
-    if (!idle) {
-        for (;;) {
-            if (threadIdx.x == 0) S.unit = (int32_t)atomicAdd(&P.ctl->queue, 1u);
-            __syncthreads();
-            const int32_t u = S.unit;
-            __syncthreads();
-            if (u >= units) break;
-            process_unit<Real>(P, u / P.nchunks, u % P.nchunks, S);
-        }
-    }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const uint32_t prev = atomicAdd(&P.ctl->exited, 1u);
-        if (prev == gridDim.x - 1) {
-            P.ctl->queue = 0u;
-            P.ctl->exited = 0u;
-            if (!kFinal) {
-                const int32_t launches = P.ctl->launches + 1;
-                P.ctl->launches = launches;
-                const int32_t active = __ldcg(&P.ctl->active);
-                const bool more = active > 0 && launches < P.ctl->cap;
-                if (active > 0 && launches >= P.ctl->cap) P.ctl->error = EGPR_TIMEOUT;
-                if (use_cond) cudaGraphSetConditional(cond, more ? 1u : 0u);
-            }
-            __threadfence();
-        }
     }
 }
 
-// X0 = 1/n on live columns, 0 on padding; column states.
-__global__ void k_spmm_init(float* X0, ColState* cols, int32_t n, int32_t npanels, int32_t k, double alpha,
-                            int32_t ndang) {
+// ---- layout ------------------------------------------------------------------------
+// Entry stream from the sweep's padded CSR: resolved sources and coefficients;
+// entries past the last one are placeholders.
+__global__ void k_sp_entries(const int32_t* __restrict__ sw_col, const float* __restrict__ sw_w, int64_t sw_nnz,
+                             int64_t epad, const int32_t* __restrict__ hub_ids, int32_t nhub,
+                             const double* __restrict__ outw, int32_t n, int32_t* __restrict__ src,
+                             float* __restrict__ c32, double* __restrict__ c64) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < epad; e += (int64_t)gridDim.x * blockDim.x) {
+        int32_t s = n;
+        double cf = 0.0;
+        if (e < sw_nnz) {
+            const int32_t code = sw_col[e];
+            if (code != -(nhub + 1)) {  // not a placeholder
+                s = code >= 0 ? code : hub_ids[-code - 1];
+                const double o = outw[s];
+                const double w = sw_w ? (double)sw_w[e] : 1.0;
+                cf = o <= 1e-15 ? 0.0 : w / o;
+            } else {
+                s = n;
+            }
+        }
+        src[e] = s;
+        c32[e] = (float)cf;
+        c64[e] = cf;
+    }
+}
+
+// Bit 31 on the last entry of every row.
+__global__ void k_sp_marks(const int32_t* __restrict__ sw_row, int32_t n, int32_t* __restrict__ src) {
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int32_t e = sw_row[r + 1] - 1;
+        src[e] |= kRowEnd;
+    }
+}
+
+// The row of entry e (every row has at least one entry): the largest r < n
+// with sw_row[r] <= e.
+__device__ __forceinline__ int32_t row_of(const int32_t* __restrict__ sw_row, int32_t n, int32_t e) {
+    int32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int32_t mid = (lo + hi + 1) >> 1;
+        if (sw_row[mid] <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_sp_chunks(const int32_t* __restrict__ sw_row, int32_t n, int32_t sw_nnz, int32_t C, int32_t nch,
+                            SpChunk* __restrict__ out) {
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nch) return;
+    SpChunk k;
+    k.e0 = c * C;
+    k.e1 = k.e0 + C;
+    const int32_t last = min(k.e1, sw_nnz) - 1;  // last real entry of the chunk
+    k.r0 = row_of(sw_row, n, k.e0);
+    const int32_t rl = row_of(sw_row, n, last);
+    const bool head = sw_row[k.r0] < k.e0;
+    const bool tail = sw_row[rl + 1] > k.e1;
+    k.flags = (head ? kHasHead : 0) | (tail ? kHasTail : 0) | ((head && tail && k.r0 == rl) ? kInterior : 0);
+    k.hkey = -1;
+    k.hparts = 0;
+    k.tparts = 0;
+    if (head) {
+        k.hkey = sw_row[k.r0] / C;
+        k.hparts = ((k.flags & kInterior) ? (sw_row[k.r0 + 1] - 1) / C : c) - k.hkey + 1;
+    }
+    if (tail && !(k.flags & kInterior)) k.tparts = (sw_row[rl + 1] - 1) / C - c + 1;
+    k.trow = rl;
+    out[c] = k;
+}
+
+// ---- per solve -----------------------------------------------------------------------
+// Row meta: dangling bit (out-weight <= 1e-15, pagerank.py:106-108).
+__global__ void k_sp_meta(const double* __restrict__ outw, int32_t n, uint32_t* __restrict__ meta) {
+    for (int32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        meta[v] = outw[v] <= 1e-15 ? kDangBit : 0u;
+}
+
+// Teleport rows of the seed vertices.
+__global__ void k_sp_tele_rows(const int32_t* __restrict__ tv, int32_t nt, uint32_t* __restrict__ meta) {
+    const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nt) meta[tv[t]] |= (uint32_t)(t + 1);
+}
+
+// X0 = 1/n on live columns, 0 on padding columns and on row n of both
+// iterates; column states.
+__global__ void k_sp_init(float* X0, float* X1, ColState* cols, int32_t n, int32_t npanels, int32_t k, double alpha,
+                          int32_t ndang) {
     const float x0 = (float)(1.0 / (double)n);
-    const int64_t total = (int64_t)npanels * n * kLanes;
+    const int64_t rowsz = ((int64_t)n + 1) * kLanes;
+    const int64_t total = (int64_t)npanels * rowsz;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t lane = (int32_t)(i & 31);
-        const int32_t p = (int32_t)(i / ((int64_t)n * kLanes));
-        X0[i] = (p * kLanes + lane) < k ? x0 : 0.f;
+        const int32_t p = (int32_t)(i / rowsz);
+        const int64_t v = (i - p * rowsz) >> 5;
+        if (v == n) {
+            X0[i] = 0.f;
+            X1[i] = 0.f;
+        } else {
+            X0[i] = (p * kLanes + lane) < k ? x0 : 0.f;
+        }
     }
     const int32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < npanels * kLanes) {
@@ -469,30 +728,30 @@ __global__ void k_spmm_init(float* X0, ColState* cols, int32_t n, int32_t npanel
 
 // out[j*n + v] = final iterate / its sum (panel-major FP64 or FP32 source),
 // transposed through shared memory so both sides are coalesced.
-__global__ void k_spmm_normalize(const double* __restrict__ out64, const float* X0, const float* X1,
-                                 const ColState* __restrict__ cols, int32_t n, int32_t k, int32_t from_fp32,
-                                 double* __restrict__ out) {
+__global__ void k_sp_normalize(const double* __restrict__ out64, const float* X0, const float* X1,
+                               const ColState* __restrict__ cols, int32_t n, int32_t k, int32_t from_fp32,
+                               double* __restrict__ out) {
     __shared__ double tile[32][33];
     const int32_t p = blockIdx.y;
     const int32_t v0 = blockIdx.x * 32;
-    const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;  // 8 rows per pass
+    const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
     const int32_t col = p * kLanes + lane;
     const ColState cs = cols[col];
     const float* xl = (cs.iter & 1) ? X1 : X0;
     const double inv = cs.xsum > 0.0 ? 1.0 / cs.xsum : 0.0;
     const double uni = 1.0 / (double)n;
-    for (int r = row; r < 32; r += kThreads / 32) {
+    for (int r = row; r < 32; r += blockDim.x / 32) {
         const int32_t v = v0 + r;
         double val = 0.0;
         if (v < n) {
-            const size_t off = ((size_t)p * n + v) * kLanes + lane;
+            const size_t off = ((size_t)p * ((size_t)n + 1) + v) * kLanes + lane;
             const double raw = from_fp32 ? (double)xl[off] : out64[off];
             val = cs.xsum > 0.0 ? raw * inv : uni;
         }
         tile[r][lane] = val;
     }
     __syncthreads();
-    for (int r = row; r < 32; r += kThreads / 32) {
+    for (int r = row; r < 32; r += blockDim.x / 32) {
         const int32_t j = p * kLanes + r;
         const int32_t v = v0 + lane;
         if (j < k && v < n) out[(size_t)j * n + v] = tile[lane][r];
@@ -501,39 +760,50 @@ __global__ void k_spmm_normalize(const double* __restrict__ out64, const float* 
 
 int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SUCC : set_cuda_error(e, what); }
 
-size_t smem_bytes(bool final) {
-    return final ? sizeof(SpmmSmem<double>) : sizeof(SpmmSmem<float>);
-}
+size_t smem_bytes(bool f64) { return f64 ? sizeof(SpSmem<true>) : sizeof(SpSmem<false>); }
 
-int spmm_grid(bool final) {
+int spmm_grid(bool f64) {
     static int cached[2][64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    int& c = cached[final ? 1 : 0][dev];
+    int& c = cached[f64 ? 1 : 0][dev];
     if (c > 0) return c;
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (final) {
-        cudaFuncSetAttribute(k_spmm<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(true));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_spmm<double>, kThreads, smem_bytes(true));
+    if (f64) {
+        cudaFuncSetAttribute(k_spmm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(true));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_spmm<true>, sp_threads<true>(), smem_bytes(true));
     } else {
-        cudaFuncSetAttribute(k_spmm<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(false));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_spmm<float>, kThreads, smem_bytes(false));
+        cudaFuncSetAttribute(k_spmm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(false));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_spmm<false>, sp_threads<false>(), smem_bytes(false));
     }
     c = sms * std::max(per, 1);
     return c;
 }
 
+// Entries per chunk (a multiple of 32).
+int32_t chunk_entries() {
+    static const int32_t v = [] {
+        const char* e = std::getenv("EGPR_SPMM_CHUNK");
+        const int x = e ? std::atoi(e) : 1024;
+        return (x >= 64 && x <= (1 << 16)) ? (x & ~31) : 1024;
+    }();
+    return v;
+}
+
 }  // namespace
 
-// Per-handle SpMM workspace (grow-only by panel count).
+// Per-graph SpMM workspace: the layout (entry stream and chunks, built on the
+// first batched solve) and the solve buffers, grown to the largest group of
+// panels solved so far.
 struct SpmmWork {
-    int32_t npanels = 0;
+    int32_t C = 0;
     int32_t nchunks = 0;
-    std::vector<Chunk> chunks;
-    DevBuf d_chunks, X0, X1, out64, out, cols, chunk_part, piece, span_cnt, span_part, panel_arrive, ctl, tele_ptr,
-        tele_col, tele_val, params;
+    int64_t epad = 0;
+    DevBuf src, c32, c64, chunks;
+    int32_t cap_panels = 0;
+    DevBuf X0, X1, out64, cols, parts, span_cnt, gacc, ctl, meta, params, out, tele, tele_v;
     cudaGraph_t cg = nullptr;
     cudaGraphExec_t cg_exec = nullptr;
     cudaGraphConditionalHandle cond = 0;
@@ -549,6 +819,233 @@ void spmm_work_release(egpr_graph* g) {
     g->spmm = nullptr;
 }
 
+namespace {
+
+int grid_1d(int64_t work) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 148 * 32));
+}
+
+int build_spmm_layout(egpr_graph* g, SpmmWork& w, cudaStream_t s) {
+    const int32_t n = g->n;
+    const int32_t C = chunk_entries();
+    if (g->sw_nnz <= 0 || g->sw_nnz > (int64_t)INT32_MAX - 2 * C) return arg_error("graph too large for the batched solve");
+    const int32_t nch = (int32_t)((g->sw_nnz + C - 1) / C);
+    const int64_t epad = (int64_t)nch * C;
+    int rc;
+    if ((rc = w.src.alloc((size_t)epad * sizeof(int32_t))) || (rc = w.c32.alloc((size_t)epad * sizeof(float))) ||
+        (rc = w.c64.alloc((size_t)epad * sizeof(double))) || (rc = w.chunks.alloc((size_t)nch * sizeof(SpChunk))))
+        return rc;
+    k_sp_entries<<<grid_1d(epad), 256, 0, s>>>(g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr,
+                                               g->sw_nnz, epad, g->hub_ids.as<int32_t>(), g->nhub,
+                                               g->outw.as<double>(), n, w.src.as<int32_t>(), w.c32.as<float>(),
+                                               w.c64.as<double>());
+    k_sp_marks<<<grid_1d(n), 256, 0, s>>>(g->sw_row.as<int32_t>(), n, w.src.as<int32_t>());
+    k_sp_chunks<<<(nch + 255) / 256, 256, 0, s>>>(g->sw_row.as<int32_t>(), n, (int32_t)g->sw_nnz, C, nch,
+                                                  w.chunks.as<SpChunk>());
+    if ((rc = cuda_ok(cudaGetLastError(), "SpMM layout"))) return rc;
+    w.C = C;
+    w.nchunks = nch;
+    w.epad = epad;
+    return EGPR_SUCC;
+}
+
+int ensure_capacity(egpr_graph* g, SpmmWork& w, int32_t npanels, cudaStream_t s) {
+    if (w.cap_panels >= npanels) return EGPR_SUCC;
+    const int32_t n = g->n;
+    const size_t xs = (size_t)npanels * ((size_t)n + 1) * kLanes;
+    const size_t units = (size_t)npanels * w.nchunks;
+    int rc;
+    if ((rc = w.X0.alloc(xs * sizeof(float))) || (rc = w.X1.alloc(xs * sizeof(float))) ||
+        (rc = w.out64.alloc(xs * sizeof(double))) ||
+        (rc = w.cols.alloc((size_t)npanels * kLanes * sizeof(ColState))) ||
+        (rc = w.parts.alloc(units * 2 * kLanes * sizeof(double))) ||
+        (rc = w.span_cnt.alloc(units * sizeof(uint32_t))) ||
+        (rc = w.gacc.alloc((size_t)npanels * kAccQ * kLanes * sizeof(unsigned long long))) ||
+        (rc = w.ctl.alloc(sizeof(Ctl))) || (rc = w.params.alloc(sizeof(SpmmParams))) ||
+        (rc = w.meta.alloc(((size_t)n + 1) * sizeof(uint32_t))))
+        return rc;
+    if ((rc = cuda_ok(cudaMemsetAsync(w.X1.p, 0, xs * sizeof(float), s), "memset")) ||
+        (rc = cuda_ok(cudaMemsetAsync(w.span_cnt.p, 0, units * sizeof(uint32_t), s), "memset")) ||
+        (rc = cuda_ok(cudaMemsetAsync(w.gacc.p, 0, (size_t)npanels * kAccQ * kLanes * sizeof(unsigned long long), s),
+                      "memset")))
+        return rc;
+    // the loop graph holds the parameter block's address
+    if (w.cg_exec) cudaGraphExecDestroy(w.cg_exec);
+    if (w.cg) cudaGraphDestroy(w.cg);
+    w.cg_exec = nullptr;
+    w.cg = nullptr;
+    w.cg_failed = false;
+    w.cap_panels = npanels;
+    return EGPR_SUCC;
+}
+
+// The sweep loop as a CUDA-graph while node whose body is one k_spmm launch.
+void build_loop_graph(SpmmWork& w, int grid) {
+    if (w.cg_exec || w.cg_failed) return;
+    const SpmmParams* Pd = w.params.as<SpmmParams>();
+    cudaGraph_t cg = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    cudaGraphConditionalHandle h = 0;
+    cudaGraphNode_t cnode = nullptr, knode = nullptr;
+    cudaGraphNodeParams cp = {};
+    bool ok = cudaGraphCreate(&cg, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&h, cg, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&cnode, cg, nullptr, 0, &cp) == cudaSuccess;
+    }
+    if (ok) {
+        int32_t one = 1;
+        void* args[3] = {(void*)&Pd, (void*)&h, (void*)&one};
+        cudaKernelNodeParams kp = {};
+        kp.func = (void*)k_spmm<false>;
+        kp.gridDim = dim3((unsigned)grid);
+        kp.blockDim = dim3(sp_threads<false>());
+        kp.sharedMemBytes = (unsigned)smem_bytes(false);
+        kp.kernelParams = args;
+        ok = cudaGraphAddKernelNode(&knode, cp.conditional.phGraph_out[0], nullptr, 0, &kp) == cudaSuccess &&
+             cudaGraphInstantiate(&ex, cg, 0) == cudaSuccess;
+    }
+    if (ok) {
+        w.cg = cg;
+        w.cg_exec = ex;
+        w.cond = h;
+    } else {
+        cudaGetLastError();
+        if (cg) cudaGraphDestroy(cg);
+        w.cg_failed = true;
+    }
+}
+
+using ColEntries = std::vector<std::pair<int32_t, float>>;
+
+// One device solve over columns [j0, j0 + kg) (kg <= kMaxPanels * 32).
+int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, double tol, int32_t j0, int32_t kg,
+                const std::vector<ColEntries>& per_col, uint32_t flags, double* out, egpr_stats* stats) {
+    const double t0 = wall_seconds();
+    const int32_t n = g->n;
+    cudaStream_t s = g->stream;
+    const int32_t npanels = (kg + kLanes - 1) / kLanes;
+    int rc;
+    if ((rc = ensure_capacity(g, w, npanels, s))) return rc;
+    // teleport rows: one per vertex that has a teleport entry in the group
+    const int32_t ld = npanels * kLanes;
+    std::vector<int32_t> tidx((size_t)n, -1), tv;
+    for (int32_t jj = 0; jj < kg; ++jj)
+        for (const auto& pr : per_col[(size_t)(j0 + jj)])
+            if (tidx[(size_t)pr.first] < 0) {
+                tidx[(size_t)pr.first] = (int32_t)tv.size();
+                tv.push_back(pr.first);
+            }
+    const int32_t nt = (int32_t)tv.size();
+    std::vector<float> tt((size_t)std::max(nt, 1) * ld, 0.f);
+    for (int32_t jj = 0; jj < kg; ++jj)
+        for (const auto& pr : per_col[(size_t)(j0 + jj)]) tt[(size_t)tidx[(size_t)pr.first] * ld + jj] = pr.second;
+    if ((rc = w.tele.alloc(tt.size() * sizeof(float))) ||
+        (rc = w.tele_v.alloc((size_t)std::max(nt, 1) * sizeof(int32_t))) ||
+        (rc = w.out.alloc((size_t)kg * n * sizeof(double))))
+        return rc;
+    if ((rc = cuda_ok(cudaMemcpyAsync(w.tele.p, tt.data(), tt.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+                      "H2D teleport")) ||
+        (nt > 0 && (rc = cuda_ok(cudaMemcpyAsync(w.tele_v.p, tv.data(), (size_t)nt * sizeof(int32_t),
+                                                 cudaMemcpyHostToDevice, s), "H2D teleport"))))
+        return rc;
+
+    SpmmParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.chunks = w.chunks.as<SpChunk>();
+    P.nchunks = w.nchunks;
+    P.npanels = npanels;
+    P.n = n;
+    P.tele_ld = ld;
+    P.max_iter = max_iter;
+    P.src = w.src.as<int32_t>();
+    P.coef32 = w.c32.as<float>();
+    P.coef64 = w.c64.as<double>();
+    P.meta = w.meta.as<uint32_t>();
+    P.tele = w.tele.as<float>();
+    P.X[0] = w.X0.as<float>();
+    P.X[1] = w.X1.as<float>();
+    P.out64 = w.out64.as<double>();
+    P.cols = w.cols.as<ColState>();
+    P.alpha = alpha;
+    P.tol_n = tol * (double)n;
+    P.parts = w.parts.p;
+    P.span_cnt = w.span_cnt.as<uint32_t>();
+    P.gacc = w.gacc.as<unsigned long long>();
+    P.ctl = w.ctl.as<Ctl>();
+    Ctl c{};
+    c.active = kg;
+    c.cap = max_iter + 1;
+    if ((rc = cuda_ok(cudaMemcpyAsync(w.params.p, &P, sizeof(P), cudaMemcpyHostToDevice, s), "H2D params")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(w.ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D ctl")))
+        return rc;
+    const SpmmParams* Pd = w.params.as<SpmmParams>();
+    const int grid = spmm_grid(false);
+    const int grid64 = spmm_grid(true);
+    if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event"))) return rc;
+    k_sp_meta<<<grid_1d(n), 256, 0, s>>>(g->outw.as<double>(), n, w.meta.as<uint32_t>());
+    if (nt > 0) k_sp_tele_rows<<<(nt + 255) / 256, 256, 0, s>>>(w.tele_v.as<int32_t>(), nt, w.meta.as<uint32_t>());
+    k_sp_init<<<grid_1d((int64_t)npanels * (n + 1) * kLanes), 256, 0, s>>>(
+        w.X0.as<float>(), w.X1.as<float>(), w.cols.as<ColState>(), n, npanels, kg, alpha, g->n_dangling_solve);
+    int32_t launches = nt > 0 ? 3 : 2;
+    build_loop_graph(w, grid);
+    if (w.cg_exec) {
+        if ((rc = cuda_ok(cudaGraphLaunch(w.cg_exec, s), "graph launch"))) return rc;
+    } else {
+        for (int32_t it = 0; it < max_iter; ++it) k_spmm<false><<<grid, sp_threads<false>(), smem_bytes(false), s>>>(Pd, 0, 0);
+        if ((rc = cuda_ok(cudaGetLastError(), "spmm launch"))) return rc;
+    }
+    const bool correction = (flags & EGPR_FLAG_NO_CORRECTION) == 0;
+    if (correction) {
+        k_spmm<true><<<grid64, sp_threads<true>(), smem_bytes(true), s>>>(Pd, 0, 0);
+        launches += 1;
+    }
+    {
+        dim3 gr((unsigned)((n + 31) / 32), (unsigned)npanels);
+        k_sp_normalize<<<gr, 256, 0, s>>>(w.out64.as<double>(), w.X0.as<float>(), w.X1.as<float>(),
+                                          w.cols.as<ColState>(), n, kg, correction ? 0 : 1, w.out.as<double>());
+        launches += 1;
+    }
+    if ((rc = cuda_ok(cudaGetLastError(), "spmm finish"))) return rc;
+    if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
+    if ((rc = cuda_ok(cudaMemcpyAsync(out, w.out.p, (size_t)kg * n * sizeof(double), cudaMemcpyDeviceToHost, s),
+                      "D2H ranks")))
+        return rc;
+    std::vector<ColState> hc((size_t)npanels * kLanes);
+    Ctl ctl;
+    if ((rc = cuda_ok(cudaMemcpyAsync(hc.data(), w.cols.p, hc.size() * sizeof(ColState), cudaMemcpyDeviceToHost, s),
+                      "D2H cols")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(&ctl, w.ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s), "D2H ctl")) ||
+        (rc = cuda_ok(cudaStreamSynchronize(s), "batch solve")))
+        return rc;
+    if (ctl.error) return ctl.error;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    if (stats) {
+        // compulsory bytes of one sweep: per panel the entry stream, the
+        // previous and the next iterate, and the row meta
+        const int64_t bytes = (int64_t)npanels * (w.epad * 8 + 2 * ((int64_t)n + 1) * kLanes * 4 + 4 * (int64_t)n);
+        for (int32_t jj = 0; jj < kg; ++jj) {
+            egpr_stats& st = stats[jj];
+            st.iterations = hc[(size_t)jj].iter;
+            st.converged = hc[(size_t)jj].converged;
+            st.residual = hc[(size_t)jj].residual;
+            st.kernel_seconds = ms * 1e-3;
+            st.total_seconds = wall_seconds() - t0;
+            st.bytes_per_iter = bytes;
+            st.launches = launches + ctl.launches;
+            st.reserved = 0;
+        }
+    }
+    return EGPR_SUCC;
+}
+
+}  // namespace
+
 int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, int32_t k,
                     const double* teleport_dense, const int32_t* seed_ptr, const int32_t* seeds, uint32_t flags,
                     double* out, egpr_stats* stats) {
@@ -558,21 +1055,20 @@ int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, i
     if (max_iter < 1) max_iter = 1;
     if (!(tol > 0.0)) tol = 0.0;
     const int32_t n = g->n;
-    // Sparse teleport entries grouped by vertex.
-    std::vector<int64_t> cnt((size_t)n + 1, 0);
-    std::vector<std::vector<std::pair<int32_t, float>>> per_col((size_t)k);
+    // teleport entries per column: (vertex, probability)
+    std::vector<ColEntries> per_col((size_t)k);
     for (int32_t j = 0; j < k; ++j) {
         auto& ent = per_col[(size_t)j];
         if (teleport_dense) {
             const double* pj = teleport_dense + (size_t)j * n;
-            double s = 0.0;
+            double sum = 0.0;
             for (int32_t v = 0; v < n; ++v) {
                 if (!(pj[v] >= 0.0) || !std::isfinite(pj[v])) return EGPR_INVALID_ARGUMENT;
-                s += pj[v];
+                sum += pj[v];
             }
-            if (!(s > 0.0)) return EGPR_INVALID_ARGUMENT;
+            if (!(sum > 0.0)) return EGPR_INVALID_ARGUMENT;
             for (int32_t v = 0; v < n; ++v)
-                if (pj[v] > 0.0) ent.emplace_back(v, (float)(pj[v] / s));
+                if (pj[v] > 0.0) ent.emplace_back(v, (float)(pj[v] / sum));
         } else {
             const int32_t b = seed_ptr[j], e = seed_ptr[j + 1];
             if (e <= b || b < 0) return EGPR_INVALID_ARGUMENT;
@@ -583,7 +1079,6 @@ int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, i
             const float val = (float)(1.0 / (double)sv.size());
             for (int32_t v : sv) ent.emplace_back(v, val);
         }
-        for (auto& pr : ent) cnt[(size_t)pr.first + 1]++;
     }
     if (g->nnz == 0) {  // pagerank.py:96-98: no edges -> uniform
         for (size_t i = 0; i < (size_t)k * n; ++i) out[i] = 1.0 / n;
@@ -594,198 +1089,24 @@ int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, i
             }
         return EGPR_SUCC;
     }
-    for (int32_t v = 0; v < n; ++v) cnt[(size_t)v + 1] += cnt[(size_t)v];
-    const int64_t nent = cnt[(size_t)n];
-    std::vector<int32_t> tptr((size_t)n + 1), tcol((size_t)std::max<int64_t>(nent, 1));
-    std::vector<float> tval((size_t)std::max<int64_t>(nent, 1));
-    {
-        std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1);
-        for (int32_t j = 0; j < k; ++j)
-            for (auto& pr : per_col[(size_t)j]) {
-                const int64_t pos = cur[(size_t)pr.first]++;
-                tcol[(size_t)pos] = j;
-                tval[(size_t)pos] = pr.second;
-            }
-        for (int32_t v = 0; v <= n; ++v) tptr[(size_t)v] = (int32_t)cnt[(size_t)v];
-    }
-    cudaStream_t s = g->stream;
-    const int32_t npanels = (k + kLanes - 1) / kLanes;
     if (!g->spmm) g->spmm = new SpmmWork();
     SpmmWork& w = *g->spmm;
-    if (w.npanels < npanels || w.chunks.empty()) {
-        // Coarser chunks than the single-vector sweep: units = panels x chunks.
-        const int grid = spmm_grid(false);
-        const int32_t target = std::max(1, (2 * grid + npanels - 1) / npanels);
-        const int32_t chunk_subs = std::max<int32_t>(1, (g->nsub + target - 1) / target);
-        if ((rc = build_chunk_table(g, chunk_subs, w.chunks, s))) return rc;
-        w.nchunks = (int32_t)w.chunks.size();
-        const size_t units = (size_t)npanels * w.nchunks;
-        const size_t xs = (size_t)npanels * n * kLanes;
-        if ((rc = w.d_chunks.alloc(w.chunks.size() * sizeof(Chunk))) || (rc = w.X0.alloc(xs * sizeof(float))) ||
-            (rc = w.X1.alloc(xs * sizeof(float))) || (rc = w.out64.alloc(xs * sizeof(double))) ||
-            (rc = w.cols.alloc((size_t)npanels * kLanes * sizeof(ColState))) ||
-            (rc = w.chunk_part.alloc(units * 3 * kLanes * sizeof(double))) ||
-            (rc = w.piece.alloc(units * 2 * kLanes * sizeof(double))) ||
-            (rc = w.span_cnt.alloc(units * sizeof(uint32_t))) ||
-            (rc = w.span_part.alloc(units * 3 * kLanes * sizeof(double))) ||
-            (rc = w.panel_arrive.alloc((size_t)npanels * sizeof(uint32_t))) || (rc = w.ctl.alloc(sizeof(Ctl))) ||
-            (rc = w.params.alloc(sizeof(SpmmParams))))
+    cudaStream_t s = g->stream;
+    if (!w.C && (rc = build_spmm_layout(g, w, s))) return rc;
+    // device solves of up to kMaxPanels panels each
+    constexpr int32_t kGroup = kMaxPanels * kLanes;
+    for (int32_t j0 = 0; j0 < k; j0 += kGroup) {
+        const int32_t kg = std::min(kGroup, k - j0);
+        if ((rc = solve_group(g, w, alpha, max_iter, tol, j0, kg, per_col, flags, out + (size_t)j0 * n,
+                              stats ? stats + j0 : nullptr)))
             return rc;
-        if ((rc = cuda_ok(cudaMemcpyAsync(w.d_chunks.p, w.chunks.data(), w.chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s), "H2D chunks")) ||
-            (rc = cuda_ok(cudaMemsetAsync(w.span_cnt.p, 0, units * sizeof(uint32_t), s), "memset")) ||
-            (rc = cuda_ok(cudaMemsetAsync(w.span_part.p, 0, units * 3 * kLanes * sizeof(double), s), "memset")) ||
-            (rc = cuda_ok(cudaMemsetAsync(w.panel_arrive.p, 0, (size_t)npanels * sizeof(uint32_t), s), "memset")))
-            return rc;
-        if (w.cg_exec) cudaGraphExecDestroy(w.cg_exec);
-        if (w.cg) cudaGraphDestroy(w.cg);
-        w.cg_exec = nullptr;
-        w.cg = nullptr;
-        w.cg_failed = false;
-        w.npanels = npanels;
     }
-    if ((size_t)k * n * sizeof(double) > w.out.bytes && (rc = w.out.alloc((size_t)k * n * sizeof(double)))) return rc;
-    if ((rc = w.tele_ptr.alloc(tptr.size() * sizeof(int32_t))) || (rc = w.tele_col.alloc(tcol.size() * sizeof(int32_t))) ||
-        (rc = w.tele_val.alloc(tval.size() * sizeof(float))))
-        return rc;
-    if ((rc = cuda_ok(cudaMemcpyAsync(w.tele_ptr.p, tptr.data(), tptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D teleport")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(w.tele_col.p, tcol.data(), tcol.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D teleport")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(w.tele_val.p, tval.data(), tval.size() * sizeof(float), cudaMemcpyHostToDevice, s), "H2D teleport")))
-        return rc;
-    // Per-vertex scale for this alpha (the single-vector set-up kernel writes it).
-    if ((rc = launch_init(g->plan, alpha, max_iter, tol, false, s))) return rc;
-
-    SpmmParams P;
-    P.chunks = w.d_chunks.as<Chunk>();
-    P.nchunks = w.nchunks;
-    P.npanels = npanels;
-    P.n = n;
-    P.max_iter = max_iter;
-    P.in_row = g->in_row.as<int32_t>();
-    P.in_col = g->in_col.as<int32_t>();
-    P.hub_ids = g->hub_ids.as<int32_t>();
-    P.in_w = g->weighted ? g->in_w.as<float>() : nullptr;
-    P.sub_coord = g->sub_coord.as<int2>();
-    P.outw = g->outw.as<double>();
-    P.scale = g->scale.as<float>();
-    P.tele_ptr = w.tele_ptr.as<int32_t>();
-    P.tele_col = w.tele_col.as<int32_t>();
-    P.tele_val = w.tele_val.as<float>();
-    P.X[0] = w.X0.as<float>();
-    P.X[1] = w.X1.as<float>();
-    P.out64 = w.out64.as<double>();
-    P.cols = w.cols.as<ColState>();
-    P.alpha = alpha;
-    P.tol_n = tol * (double)n;
-    P.chunk_part = w.chunk_part.as<double>();
-    P.piece = w.piece.as<double>();
-    P.span_cnt = w.span_cnt.as<uint32_t>();
-    P.span_part = w.span_part.as<double>();
-    P.panel_arrive = w.panel_arrive.as<uint32_t>();
-    P.ctl = w.ctl.as<Ctl>();
-    if ((rc = cuda_ok(cudaMemcpyAsync(w.params.p, &P, sizeof(P), cudaMemcpyHostToDevice, s), "H2D params"))) return rc;
-    const SpmmParams* Pd = w.params.as<SpmmParams>();
-    const int units = npanels * w.nchunks;
-    const int grid = std::max(1, std::min(units, spmm_grid(false)));
-    const int grid_final = std::max(1, std::min(units, spmm_grid(true)));
-    if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event"))) return rc;
-    {
-        const int64_t total = (int64_t)npanels * n * kLanes;
-        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + kThreads - 1) / kThreads, 148 * 16));
-        const int need = (npanels * kLanes + kThreads - 1) / kThreads;
-        k_spmm_init<<<std::max(blocks, need), kThreads, 0, s>>>(w.X0.as<float>(), w.cols.as<ColState>(), n, npanels, k,
-                                                                 alpha, g->n_dangling_solve);
-    }
-    // Control block: active columns = k, cap = max_iter + 1 sweeps.
-    {
-        Ctl c{};
-        c.active = k;
-        c.cap = max_iter + 1;
-        if ((rc = cuda_ok(cudaMemcpyAsync(w.ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D ctl"))) return rc;
-    }
-    // The sweep loop: a CUDA-graph while node whose body is one k_spmm launch,
-    // built once per workspace (its only argument is the parameter block).
-    if (!w.cg_exec && !w.cg_failed) {
-        cudaGraph_t cg = nullptr;
-        cudaGraphExec_t ex = nullptr;
-        cudaGraphConditionalHandle h = 0;
-        cudaGraphNode_t cnode = nullptr, knode = nullptr;
-        cudaGraphNodeParams cp = {};
-        bool ok = cudaGraphCreate(&cg, 0) == cudaSuccess &&
-                  cudaGraphConditionalHandleCreate(&h, cg, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
-        if (ok) {
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = h;
-            cp.conditional.type = cudaGraphCondTypeWhile;
-            cp.conditional.size = 1;
-            ok = cudaGraphAddNode(&cnode, cg, nullptr, 0, &cp) == cudaSuccess;
-        }
-        if (ok) {
-            int32_t one = 1;
-            void* args[3] = {(void*)&Pd, (void*)&h, (void*)&one};
-            cudaKernelNodeParams kp = {};
-            kp.func = (void*)k_spmm<float>;
-            kp.gridDim = dim3((unsigned)grid);
-            kp.blockDim = dim3(kThreads);
-            kp.sharedMemBytes = (unsigned)smem_bytes(false);
-            kp.kernelParams = args;
-            ok = cudaGraphAddKernelNode(&knode, cp.conditional.phGraph_out[0], nullptr, 0, &kp) == cudaSuccess &&
-                 cudaGraphInstantiate(&ex, cg, 0) == cudaSuccess;
-        }
-        if (ok) {
-            w.cg = cg;
-            w.cg_exec = ex;
-            w.cond = h;
-        } else {
-            cudaGetLastError();
-            if (cg) cudaGraphDestroy(cg);
-            w.cg_failed = true;
-        }
-    }
-    int32_t launches = 2;  // set-up kernels
-    if (w.cg_exec) {
-        if ((rc = cuda_ok(cudaGraphLaunch(w.cg_exec, s), "graph launch"))) return rc;
-    } else {
-        for (int32_t it = 0; it < max_iter; ++it)
-            k_spmm<float><<<grid, kThreads, smem_bytes(false), s>>>(Pd, 0, 0);
-        if ((rc = cuda_ok(cudaGetLastError(), "spmm launch"))) return rc;
-    }
-    const bool correction = (flags & EGPR_FLAG_NO_CORRECTION) == 0;
-    if (correction) {
-        k_spmm<double><<<grid_final, kThreads, smem_bytes(true), s>>>(Pd, 0, 0);
-        launches += 1;
-    }
-    {
-        dim3 gr((unsigned)((n + 31) / 32), (unsigned)npanels);
-        k_spmm_normalize<<<gr, kThreads, 0, s>>>(w.out64.as<double>(), w.X0.as<float>(), w.X1.as<float>(),
-                                                 w.cols.as<ColState>(), n, k, correction ? 0 : 1, w.out.as<double>());
-        launches += 1;
-    }
-    if ((rc = cuda_ok(cudaGetLastError(), "spmm finish"))) return rc;
-    if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
-    if ((rc = cuda_ok(cudaMemcpyAsync(out, w.out.p, (size_t)k * n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ranks")))
-        return rc;
-    std::vector<ColState> hc((size_t)npanels * kLanes);
-    Ctl ctl;
-    if ((rc = cuda_ok(cudaMemcpyAsync(hc.data(), w.cols.p, hc.size() * sizeof(ColState), cudaMemcpyDeviceToHost, s), "D2H cols")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(&ctl, w.ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s), "D2H ctl")) ||
-        (rc = cuda_ok(cudaStreamSynchronize(s), "batch solve")))
-        return rc;
-    if (ctl.error) return ctl.error;
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
-    if (stats) {
-        const int64_t bytes = 4 * ((int64_t)n + 1) + 4 * g->nnz * (g->weighted ? 2 : 1) + 4 * (int64_t)n +
-                              12 * (int64_t)n * k;
+    if (stats && k > kGroup) {  // the whole batch's device time in every column
+        double ks = 0.0;
+        for (int32_t j0 = 0; j0 < k; j0 += kGroup) ks += stats[j0].kernel_seconds;
         for (int32_t j = 0; j < k; ++j) {
-            egpr_stats& st = stats[j];
-            st.iterations = hc[(size_t)j].iter;
-            st.converged = hc[(size_t)j].converged;
-            st.residual = hc[(size_t)j].residual;
-            st.kernel_seconds = ms * 1e-3;
-            st.total_seconds = wall_seconds() - t0;
-            st.bytes_per_iter = bytes;
-            st.launches = launches + ctl.launches;
-            st.reserved = 0;
+            stats[j].kernel_seconds = ks;
+            stats[j].total_seconds = wall_seconds() - t0;
         }
     }
     return EGPR_SUCC;

@@ -339,6 +339,26 @@ def test_ppr_batch_is_deterministic_and_columns_independent():
     assert np.abs(sub - a[5:9]).sum(axis=1).max() <= L1_TOL
 
 
+def test_ppr_batch_rows_across_many_chunks_and_several_device_groups():
+    # vertex 0 has an inbound entry from every other vertex (a row cut into
+    # several chunks), and 520 columns need two device solves of 16 panels
+    rng = np.random.default_rng(5)
+    n = 4000
+    src = np.concatenate([np.arange(1, n), rng.integers(0, n, 6000)])
+    dst = np.concatenate([np.zeros(n - 1, np.int64), rng.integers(0, n, 6000)])
+    keep = src != dst
+    pairs = np.unique(np.stack([src[keep], dst[keep]], 1).astype(np.int32), axis=0)  # sorted by source
+    V = np.zeros(n + 1, np.int32)
+    V[1:] = np.cumsum(np.bincount(pairs[:, 0], minlength=n))
+    E = np.ascontiguousarray(pairs[:, 1])
+    sets = synth.seed_sets(n, 520, 1, 8, seed=4)
+    pg = _native.PreparedGraph(V, E)
+    ranks, stats = pg.pagerank_seeds(sets, alpha=0.85, max_iter=100, tol=1e-9)
+    assert ranks.shape == (520, n)
+    for j in (0, 31, 255, 511, 512, 519):
+        _check_against_oracle(V, E, None, ranks[j], stats[j], 0.85, 100, 1e-9, teleport=_seed_teleport(n, sets[j]))
+
+
 def test_ppr_through_the_api_batch():
     G = DiGraph()
     G.add_edges_from([("a", "b"), ("b", "c"), ("c", "a"), ("c", "d"), ("d", "a")])
