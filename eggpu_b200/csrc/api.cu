@@ -43,6 +43,17 @@ static int fail_arg(const char* why) {
 
 int arg_error(const char* why) { return fail_arg(why); }
 
+// Loop mechanism of the sweeps: a CUDA-graph while node (default) or plain
+// launches (EGPR_GRAPH_LOOP=0; profilers cannot capture kernels of conditional
+// graphs).
+bool graph_loop_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("EGPR_GRAPH_LOOP");
+        return !(v && (v[0] == '0' || v[0] == 'n' || v[0] == 'N' || v[0] == 'f' || v[0] == 'F'));
+    }();
+    return on;
+}
+
 double wall_seconds() {
     using clock = std::chrono::steady_clock;
     return std::chrono::duration<double>(clock::now().time_since_epoch()).count();

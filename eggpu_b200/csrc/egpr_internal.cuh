@@ -219,6 +219,7 @@ cudaMemPool_t device_pool();
 // Status helpers.
 int set_cuda_error(cudaError_t e, const char* what);
 int arg_error(const char* why);  // EGPR_INVALID_ARGUMENT with a message
+bool graph_loop_enabled();       // sweeps loop in a CUDA-graph while node (EGPR_GRAPH_LOOP != 0)
 int check_device(const egpr_graph* g);
 double wall_seconds();
 

@@ -97,6 +97,8 @@ struct SpmmParams {
     ColState* cols;
     double alpha;
     double tol_n;
+    float alpha_hi, alpha_lo;  // alpha = alpha_hi + alpha_lo (FP32 sweep)
+    float oma_hi, oma_lo;      // 1 - alpha, likewise
     void* parts;              // [panel][chunk][2][32] pieces of cut rows (Real)
     uint32_t* span_cnt;       // [panel][chunk] arrivals per span (reset by the last)
     unsigned long long* gacc; // [panel][kAccQ][32] fixed-point column sums
@@ -142,7 +144,8 @@ __device__ __forceinline__ double fx64_join(unsigned long long hi, unsigned long
     return (double)(long long)hi * (1.0 / 4294967296.0) + (double)lo * (1.0 / 18446744073709551616.0);
 }
 
-// Adds a lane's two columns of (err, dsum, xsum) to the CTA's accumulators of
+// Adds a lane's two columns of (err, dsum) (FP32 sweep) or (err, xsum) (FP64
+// sweep) to the CTA's accumulators of
 // panel p (lanes of the lower half-warp; each holds columns c2, c2 + 1).
 template <bool kF64>
 __device__ __forceinline__ void acc_add(SpSmem<kF64>& S, int32_t p, int c2, double e0, double e1, double d0,
@@ -153,8 +156,6 @@ __device__ __forceinline__ void acc_add(SpSmem<kF64>& S, int32_t p, int c2, doub
         if (e1 != 0.0) atomicAdd(a + 0 * kLanes + c2 + 1, fx40(e1));
         if (d0 != 0.0) atomicAdd(a + 1 * kLanes + c2, fx40(d0));
         if (d1 != 0.0) atomicAdd(a + 1 * kLanes + c2 + 1, fx40(d1));
-        if (x0 != 0.0) atomicAdd(a + 2 * kLanes + c2, fx40(x0));
-        if (x1 != 0.0) atomicAdd(a + 2 * kLanes + c2 + 1, fx40(x1));
     } else {
         unsigned long long h, l;
         fx64_split(e0, h, l);
@@ -180,9 +181,11 @@ struct Lane {
     const float* xb;  // FP64 sweep: of column c2 + 1
     float* xout;      // FP32 sweep: the next iterate (panel base)
     double* out64;    // FP64 sweep: the result (panel base)
-    RealT<kF64> dm0, dm1;  // dangling term of the two columns
+    double dm0, dm1;  // FP64 sweep: dangling term of the two columns
+    float df0, df1;   // FP32 sweep: the same in FP32
     int32_t p;
     bool live0, live1;
+    bool all;         // every column of the panel takes part
 };
 
 // Reads the lane's two column states for panel p; skip = no column of the
@@ -199,88 +202,120 @@ __device__ Lane<kF64> make_lane(const SpmmParams& P, int32_t p, bool& skip) {
     L.p = p;
     L.xout = nullptr;
     L.out64 = nullptr;
+    L.dm0 = L.dm1 = 0.0;
+    L.df0 = L.df1 = 0.f;
     if (!kF64) {
         L.live0 = a0 && !d0;
         L.live1 = a1 && !d1;
         const unsigned lm = __ballot_sync(kAll, L.live0 || L.live1);
         skip = lm == 0u;
+        L.all = __all_sync(kAll, L.live0 && L.live1);
         // live columns of a panel have taken the same number of sweeps
         const int32_t it = __shfl_sync(kAll, L.live0 ? i0 : i1, lm ? __ffs(lm) - 1 : 0);
         const int par = it & 1;
         L.xa = P.X[par] + pbase;
         L.xb = L.xa;
         L.xout = P.X[par ^ 1] + pbase;
-        L.dm0 = (RealT<kF64>)__ldcg(&cs[0].dmass);
-        L.dm1 = (RealT<kF64>)__ldcg(&cs[1].dmass);
+        L.df0 = (float)__ldcg(&cs[0].dmass);
+        L.df1 = (float)__ldcg(&cs[1].dmass);
     } else {
         // each column's x_{k-1}, recomputed to x_k in FP64
         L.live0 = a0 != 0;
         L.live1 = a1 != 0;
         skip = __ballot_sync(kAll, L.live0 || L.live1) == 0u;
+        L.all = __all_sync(kAll, L.live0 && L.live1);
         L.xa = P.X[(i0 - 1) & 1] + pbase;
         L.xb = P.X[(i1 - 1) & 1] + pbase;
         L.out64 = P.out64 + pbase;
-        L.dm0 = (RealT<kF64>)__ldcg(&cs[0].dmass_prev);
-        L.dm1 = (RealT<kF64>)__ldcg(&cs[1].dmass_prev);
+        L.dm0 = __ldcg(&cs[0].dmass_prev);
+        L.dm1 = __ldcg(&cs[1].dmass_prev);
     }
     return L;
 }
 
-// Per-lane sums of a chunk (at most a few thousand rows) for its two columns,
-// in the sweep's precision; each chunk's sums are then added as fixed point.
+// Per-lane sums of a chunk for its two columns; each chunk's sums are then
+// added as fixed point.  The dangling mass is kept in FP64 even in the FP32
+// sweep: many rows carry exactly the same value (every vertex without inbound
+// entries holds the teleport and dangling terms only), and an FP32 running sum
+// of equal terms rounds the same way at every step, a bias of about 1e-6
+// relative that the dangling term would feed back into every row.  The FP32
+// sweep keeps no rank sum (the result is normalised from an exact sum).
 template <bool kF64>
 struct LaneSums {
-    RealT<kF64> e0 = 0, e1 = 0;  // residual
-    RealT<kF64> d0 = 0, d1 = 0;  // dangling mass (FP32 sweep)
-    RealT<kF64> x0 = 0, x1 = 0;  // rank sum
+    RealT<kF64> e0 = 0, e1 = 0;  // residual (steers the stop rule)
+    double d0 = 0.0, d1 = 0.0;   // FP32 sweep: dangling mass
+    double x0 = 0.0, x1 = 0.0;   // FP64 sweep: rank sum
 };
 
 // One finished row v of the lane's two columns: rs = sum of the inbound
 // terms without alpha, pa/pb = previous value of the columns, mt = row meta.
+// FP32 sweep: alpha and 1 - alpha enter as FP32 pairs (high + low part), since
+// alpha rounded to FP32 would move the fixed point by about its rounding
+// error / (1 - alpha)^2 in L1.
 template <bool kF64>
 __device__ __forceinline__ void row_out(const SpmmParams& P, const Lane<kF64>& L, int c2, int32_t v,
                                         RealT<kF64> rsx, RealT<kF64> rsy, RealT<kF64> pa, RealT<kF64> pb,
                                         uint32_t mt, LaneSums<kF64>& A) {
-    using Real = RealT<kF64>;
-    const Real alpha = (Real)P.alpha, oma = (Real)(1.0 - P.alpha);
-    Real tx = Real(0), ty = Real(0);
     const uint32_t t = mt & ~kDangBit;
-    if (t) {  // a teleport row (seed vertices only)
-        const float2 tl =
-            __ldg(reinterpret_cast<const float2*>(P.tele + (size_t)(t - 1) * (size_t)P.tele_ld + L.p * kLanes + c2));
-        tx = (Real)tl.x;
-        ty = (Real)tl.y;
-    }
-    const Real vx = fma(alpha, rsx, fma(oma, tx, L.dm0));
-    const Real vy = fma(alpha, rsy, fma(oma, ty, L.dm1));
     const size_t off = (size_t)v * kLanes + c2;
-    if (!kF64) {
+    if constexpr (!kF64) {
+        float bx = L.df0, by = L.df1;
+        if (t) {  // a teleport row (seed vertices only)
+            const float2 tl = __ldg(
+                reinterpret_cast<const float2*>(P.tele + (size_t)(t - 1) * (size_t)P.tele_ld + L.p * kLanes + c2));
+            bx = fmaf(P.oma_hi, tl.x, fmaf(P.oma_lo, tl.x, bx));
+            by = fmaf(P.oma_hi, tl.y, fmaf(P.oma_lo, tl.y, by));
+        }
+        const float vx = fmaf(P.alpha_hi, rsx, fmaf(P.alpha_lo, rsx, bx));
+        const float vy = fmaf(P.alpha_hi, rsy, fmaf(P.alpha_lo, rsy, by));
         float* o = L.xout + off;
-        if (L.live0 && L.live1) {
-            __stcs(reinterpret_cast<float2*>(o), make_float2((float)vx, (float)vy));
+        const bool dang = (mt & kDangBit) != 0u;
+        if (L.all) {
+            __stcs(reinterpret_cast<float2*>(o), make_float2(vx, vy));
+            A.e0 += fabsf(vx - pa);
+            A.e1 += fabsf(vy - pb);
+            if (dang) {
+                A.d0 += (double)vx;
+                A.d1 += (double)vy;
+            }
         } else {
-            if (L.live0) __stcs(o, (float)vx);
-            if (L.live1) __stcs(o + 1, (float)vy);
+            if (L.live0) {
+                __stcs(o, vx);
+                A.e0 += fabsf(vx - pa);
+                if (dang) A.d0 += (double)vx;
+            }
+            if (L.live1) {
+                __stcs(o + 1, vy);
+                A.e1 += fabsf(vy - pb);
+                if (dang) A.d1 += (double)vy;
+            }
         }
     } else {
+        const double alpha = P.alpha, oma = 1.0 - P.alpha;
+        double tx = 0.0, ty = 0.0;
+        if (t) {
+            const float2 tl = __ldg(
+                reinterpret_cast<const float2*>(P.tele + (size_t)(t - 1) * (size_t)P.tele_ld + L.p * kLanes + c2));
+            tx = (double)tl.x;
+            ty = (double)tl.y;
+        }
+        const double vx = fma(alpha, rsx, fma(oma, tx, L.dm0));
+        const double vy = fma(alpha, rsy, fma(oma, ty, L.dm1));
         double* o = L.out64 + off;
         if (L.live0 && L.live1) {
-            *reinterpret_cast<double2*>(o) = make_double2((double)vx, (double)vy);
+            *reinterpret_cast<double2*>(o) = make_double2(vx, vy);
         } else {
-            if (L.live0) o[0] = (double)vx;
-            if (L.live1) o[1] = (double)vy;
+            if (L.live0) o[0] = vx;
+            if (L.live1) o[1] = vy;
         }
-    }
-    const bool dang = (mt & kDangBit) != 0u;
-    if (L.live0) {
-        A.e0 += fabs(vx - pa);
-        A.x0 += vx;
-        if (!kF64 && dang) A.d0 += vx;
-    }
-    if (L.live1) {
-        A.e1 += fabs(vy - pb);
-        A.x1 += vy;
-        if (!kF64 && dang) A.d1 += vy;
+        if (L.live0) {
+            A.e0 += fabs(vx - pa);
+            A.x0 += vx;
+        }
+        if (L.live1) {
+            A.e1 += fabs(vy - pb);
+            A.x1 += vy;
+        }
     }
 }
 
@@ -361,7 +396,7 @@ __device__ void span_arrive(const SpmmParams& P, SpSmem<kF64>& S, const Lane<kF6
     prev_of<kF64>(L, c2, v, pa, pb);
     LaneSums<kF64> A;
     row_out<kF64>(P, L, c2, v, s.x, s.y, pa, pb, __ldg(P.meta + v), A);
-    acc_add<kF64>(S, p, c2, (double)A.e0, (double)A.e1, (double)A.d0, (double)A.d1, (double)A.x0, (double)A.x1);
+    acc_add<kF64>(S, p, c2, (double)A.e0, (double)A.e1, A.d0, A.d1, A.x0, A.x1);
 }
 
 // One (panel, chunk) unit.
@@ -384,7 +419,8 @@ __device__ void process_unit(const SpmmParams& P, SpSmem<kF64>& S, int32_t p, in
                                          : reinterpret_cast<const Coef*>(P.coef32);
     const float* __restrict__ xa = L.xa;
     const float* __restrict__ xb = L.xb;
-    Real ax = Real(0), ay = Real(0);  // this half-warp's part of the open row
+    using Acc = Real;
+    Acc ax = Acc(0), ay = Acc(0);  // this half-warp's part of the open row
     LaneSums<kF64> A;
     int32_t rb = ck.r0;  // the row the next row end finishes
     bool head_pending = (ck.flags & kHasHead) && !(ck.flags & kInterior);
@@ -402,10 +438,10 @@ __device__ void process_unit(const SpmmParams& P, SpSmem<kF64>& S, int32_t p, in
         uint32_t mt = 0u;  // meta of the batch's rows, lane k: row rb + k
         if (lane < nr) mt = __ldg(P.meta + rb + lane);
         int ord = 0;
-        auto emit = [&](Real tx, Real ty) {
-            const Real sx = tx + __shfl_xor_sync(kAll, tx, 16);
-            const Real sy = ty + __shfl_xor_sync(kAll, ty, 16);
-            if (g == 0) *reinterpret_cast<V2<Real>*>(&rows[ord][c2]) = V2<Real>{sx, sy};
+        auto emit = [&](Acc tx, Acc ty) {
+            const Acc sx = tx + __shfl_xor_sync(kAll, tx, 16);
+            const Acc sy = ty + __shfl_xor_sync(kAll, ty, 16);
+            if (g == 0) *reinterpret_cast<V2<Real>*>(&rows[ord][c2]) = V2<Real>{(Real)sx, (Real)sy};
             ++ord;
         };
 #pragma unroll
@@ -429,22 +465,22 @@ __device__ void process_unit(const SpmmParams& P, SpSmem<kF64>& S, int32_t p, in
                 const Coef q = __shfl_sync(kAll, cc, 16 * h + 2 * s + g);
                 const uint32_t mp = (m >> (16 * h + 2 * s)) & 3u;  // row ends at the even / odd entry
                 if (mp == 0u) {
-                    ax = fma(q, gx[s], ax);
-                    ay = fma(q, gy[s], ay);
+                    ax = fma((Acc)q, (Acc)gx[s], ax);
+                    ay = fma((Acc)q, (Acc)gy[s], ay);
                 } else {
-                    const Real px = q * gx[s], py = q * gy[s];
+                    const Acc px = (Acc)q * (Acc)gx[s], py = (Acc)q * (Acc)gy[s];
                     if (mp & 1u) {
                         emit(g == 0 ? ax + px : ax, g == 0 ? ay + py : ay);
-                        ax = g == 0 ? Real(0) : px;
-                        ay = g == 0 ? Real(0) : py;
+                        ax = g == 0 ? Acc(0) : px;
+                        ay = g == 0 ? Acc(0) : py;
                     } else {
                         ax += px;
                         ay += py;
                     }
                     if (mp & 2u) {
                         emit(ax, ay);
-                        ax = Real(0);
-                        ay = Real(0);
+                        ax = Acc(0);
+                        ay = Acc(0);
                     }
                 }
             }
@@ -479,18 +515,22 @@ __device__ void process_unit(const SpmmParams& P, SpSmem<kF64>& S, int32_t p, in
     // the row still open at the end of the chunk: the chunk's piece of a span
     const int32_t f = ck.flags;
     if (f & kHasTail) {
-        const Real tx = ax + __shfl_xor_sync(kAll, ax, 16);
-        const Real ty = ay + __shfl_xor_sync(kAll, ay, 16);
-        if (g == 0) store_part<kF64>(P, p, c, (f & kInterior) ? 0 : 1, c2, tx, ty);
+        const Acc tx = ax + __shfl_xor_sync(kAll, ax, 16);
+        const Acc ty = ay + __shfl_xor_sync(kAll, ay, 16);
+        if (g == 0) store_part<kF64>(P, p, c, (f & kInterior) ? 0 : 1, c2, (Real)tx, (Real)ty);
     }
     // the chunk's column sums (both half-warps, fixed order)
     {
         const double e0 = (double)A.e0 + (double)__shfl_xor_sync(kAll, A.e0, 16);
         const double e1 = (double)A.e1 + (double)__shfl_xor_sync(kAll, A.e1, 16);
-        const double d0 = (double)A.d0 + (double)__shfl_xor_sync(kAll, A.d0, 16);
-        const double d1 = (double)A.d1 + (double)__shfl_xor_sync(kAll, A.d1, 16);
-        const double x0 = (double)A.x0 + (double)__shfl_xor_sync(kAll, A.x0, 16);
-        const double x1 = (double)A.x1 + (double)__shfl_xor_sync(kAll, A.x1, 16);
+        double d0 = 0.0, d1 = 0.0, x0 = 0.0, x1 = 0.0;
+        if (!kF64) {
+            d0 = A.d0 + __shfl_xor_sync(kAll, A.d0, 16);
+            d1 = A.d1 + __shfl_xor_sync(kAll, A.d1, 16);
+        } else {
+            x0 = A.x0 + __shfl_xor_sync(kAll, A.x0, 16);
+            x1 = A.x1 + __shfl_xor_sync(kAll, A.x1, 16);
+        }
         if (g == 0) acc_add<kF64>(S, p, c2, e0, e1, d0, d1, x0, x1);
     }
     if (f & (kHasHead | kHasTail)) {
@@ -568,10 +608,9 @@ k_spmm(const SpmmParams* __restrict__ Pd, cudaGraphConditionalHandle cond, int32
         ColState* cs = P.cols + j;
         if (!kF64) {
             if (cs->active && !cs->done) {
-                const double e = fx40_join(w[0]), d = fx40_join(w[1]), x = fx40_join(w[2]);
+                const double e = fx40_join(w[0]), d = fx40_join(w[1]);
                 cs->residual = e;
                 cs->dsum = d;
-                cs->xsum = x;
                 cs->dmass_prev = cs->dmass;
                 cs->dmass = P.alpha * d / (double)P.n;
                 const int32_t it = cs->iter + 1;
@@ -726,6 +765,32 @@ __global__ void k_sp_init(float* X0, float* X1, ColState* cols, int32_t n, int32
     }
 }
 
+// Rank sum of each column's final FP32 iterate (runs when the FP64 correction
+// sweep, which sums its own result, is switched off): FP64 partial sums per
+// warp, added as two-word fixed point so the total is independent of order.
+__global__ void k_sp_colsum(const float* __restrict__ X0, const float* __restrict__ X1,
+                            const ColState* __restrict__ cols, int32_t n, unsigned long long* __restrict__ words) {
+    const int32_t p = blockIdx.y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const ColState& cs = cols[p * kLanes + lane];
+    const float* x = ((cs.iter & 1) ? X1 : X0) + (size_t)p * ((size_t)n + 1) * kLanes;
+    double sum = 0.0;
+    for (int64_t v = (int64_t)blockIdx.x * nw + warp; v < n; v += (int64_t)gridDim.x * nw)
+        sum += (double)x[(size_t)v * kLanes + lane];
+    unsigned long long h, l;
+    fx64_split(sum, h, l);
+    atomicAdd(words + ((size_t)p * 2) * kLanes + lane, h);
+    atomicAdd(words + ((size_t)p * 2 + 1) * kLanes + lane, l);
+}
+
+__global__ void k_sp_colsum_set(ColState* __restrict__ cols, const unsigned long long* __restrict__ words,
+                                int32_t npanels) {
+    const int32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= npanels * kLanes) return;
+    const int32_t p = j / kLanes, lane = j - p * kLanes;
+    cols[j].xsum = fx64_join(words[((size_t)p * 2) * kLanes + lane], words[((size_t)p * 2 + 1) * kLanes + lane]);
+}
+
 // out[j*n + v] = final iterate / its sum (panel-major FP64 or FP32 source),
 // transposed through shared memory so both sides are coalesced.
 __global__ void k_sp_normalize(const double* __restrict__ out64, const float* X0, const float* X1,
@@ -803,7 +868,7 @@ struct SpmmWork {
     int64_t epad = 0;
     DevBuf src, c32, c64, chunks;
     int32_t cap_panels = 0;
-    DevBuf X0, X1, out64, cols, parts, span_cnt, gacc, ctl, meta, params, out, tele, tele_v;
+    DevBuf X0, X1, out64, cols, parts, span_cnt, gacc, colsum, ctl, meta, params, out, tele, tele_v;
     cudaGraph_t cg = nullptr;
     cudaGraphExec_t cg_exec = nullptr;
     cudaGraphConditionalHandle cond = 0;
@@ -861,6 +926,7 @@ int ensure_capacity(egpr_graph* g, SpmmWork& w, int32_t npanels, cudaStream_t s)
         (rc = w.parts.alloc(units * 2 * kLanes * sizeof(double))) ||
         (rc = w.span_cnt.alloc(units * sizeof(uint32_t))) ||
         (rc = w.gacc.alloc((size_t)npanels * kAccQ * kLanes * sizeof(unsigned long long))) ||
+        (rc = w.colsum.alloc((size_t)npanels * 2 * kLanes * sizeof(unsigned long long))) ||
         (rc = w.ctl.alloc(sizeof(Ctl))) || (rc = w.params.alloc(sizeof(SpmmParams))) ||
         (rc = w.meta.alloc(((size_t)n + 1) * sizeof(uint32_t))))
         return rc;
@@ -972,6 +1038,10 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     P.out64 = w.out64.as<double>();
     P.cols = w.cols.as<ColState>();
     P.alpha = alpha;
+    P.alpha_hi = (float)alpha;
+    P.alpha_lo = (float)(alpha - (double)P.alpha_hi);
+    P.oma_hi = (float)(1.0 - alpha);
+    P.oma_lo = (float)((1.0 - alpha) - (double)P.oma_hi);
     P.tol_n = tol * (double)n;
     P.parts = w.parts.p;
     P.span_cnt = w.span_cnt.as<uint32_t>();
@@ -992,8 +1062,8 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     k_sp_init<<<grid_1d((int64_t)npanels * (n + 1) * kLanes), 256, 0, s>>>(
         w.X0.as<float>(), w.X1.as<float>(), w.cols.as<ColState>(), n, npanels, kg, alpha, g->n_dangling_solve);
     int32_t launches = nt > 0 ? 3 : 2;
-    build_loop_graph(w, grid);
-    if (w.cg_exec) {
+    if (graph_loop_enabled()) build_loop_graph(w, grid);
+    if (w.cg_exec && graph_loop_enabled()) {
         if ((rc = cuda_ok(cudaGraphLaunch(w.cg_exec, s), "graph launch"))) return rc;
     } else {
         for (int32_t it = 0; it < max_iter; ++it) k_spmm<false><<<grid, sp_threads<false>(), smem_bytes(false), s>>>(Pd, 0, 0);
@@ -1003,6 +1073,17 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     if (correction) {
         k_spmm<true><<<grid64, sp_threads<true>(), smem_bytes(true), s>>>(Pd, 0, 0);
         launches += 1;
+    }
+    if (!correction) {
+        if ((rc = cuda_ok(cudaMemsetAsync(w.colsum.p, 0, (size_t)npanels * 2 * kLanes * sizeof(unsigned long long), s),
+                          "memset")))
+            return rc;
+        k_sp_colsum<<<dim3(148, (unsigned)npanels), 256, 0, s>>>(w.X0.as<float>(), w.X1.as<float>(),
+                                                                 w.cols.as<ColState>(), n,
+                                                                 w.colsum.as<unsigned long long>());
+        k_sp_colsum_set<<<(npanels * kLanes + 255) / 256, 256, 0, s>>>(w.cols.as<ColState>(),
+                                                                       w.colsum.as<unsigned long long>(), npanels);
+        launches += 2;
     }
     {
         dim3 gr((unsigned)((n + 31) / 32), (unsigned)npanels);

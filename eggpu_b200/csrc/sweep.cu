@@ -790,15 +790,6 @@ int vertex_grid(int32_t max_n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 8));
 }
 
-// Loop mechanism: a CUDA-graph while node (default) or plain launches
-// (EGPR_GRAPH_LOOP=0; profilers cannot capture kernels of conditional graphs).
-bool graph_loop_enabled() {
-    static const bool on = [] {
-        const char* v = std::getenv("EGPR_GRAPH_LOOP");
-        return !(v && (v[0] == '0' || v[0] == 'n' || v[0] == 'N' || v[0] == 'f' || v[0] == 'F'));
-    }();
-    return on;
-}
 
 cudaLaunchAttributeValue l2_window(const Plan& plan) {
     cudaLaunchAttributeValue v = {};
