@@ -239,28 +239,38 @@ class PreparedGraph:
         check(lib.egpr_pagerank_collect(self.handle, _ptr(res), ctypes.byref(st)), "egpr_pagerank_collect")
         return res, st.as_dict()
 
-    def pagerank_batch(self, teleport, alpha=0.85, max_iter=100, tol=1e-6, correction=True):
-        """teleport: (k, n) array of non-negative vectors. Returns ((k, n) ranks, [stats])."""
+    def _batch_out(self, k, out):
+        if out is None:
+            return np.empty((k, self.n), np.float64)
+        if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (k, self.n)
+                or not out.flags.c_contiguous or not out.flags.writeable):
+            raise ValueError(f"out must be a writeable C-contiguous float64 array of shape ({k}, {self.n})")
+        return out
+
+    def pagerank_batch(self, teleport, alpha=0.85, max_iter=100, tol=1e-6, correction=True, out=None):
+        """teleport: (k, n) array of non-negative vectors. Returns ((k, n) ranks, [stats]).
+        out: optional (k, n) float64 result array (page-locked memory makes the copy back faster)."""
         T = _f64(teleport)
         if T.ndim != 2 or T.shape[1] != self.n:
             raise ValueError("teleport must have shape (k, n)")
         k = T.shape[0]
-        res = np.empty((k, self.n), np.float64)
+        res = self._batch_out(k, out)
         sts = (EgprStats * k)()
         flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
         check(lib.egpr_pagerank_batch(self.handle, float(alpha), int(max_iter), float(tol), k, _ptr(T), flags,
                                       _ptr(res), ctypes.cast(sts, c_void_p)), "egpr_pagerank_batch")
         return res, [s.as_dict() for s in sts]
 
-    def pagerank_seeds(self, seed_sets, alpha=0.85, max_iter=100, tol=1e-6, correction=True):
-        """seed_sets: list of vertex-id sequences (uniform teleport over each)."""
+    def pagerank_seeds(self, seed_sets, alpha=0.85, max_iter=100, tol=1e-6, correction=True, out=None):
+        """seed_sets: list of vertex-id sequences (uniform teleport over each).
+        out: optional (k, n) float64 result array, as for pagerank_batch."""
         k = len(seed_sets)
         ptr = np.zeros(k + 1, np.int32)
         for j, s in enumerate(seed_sets):
             ptr[j + 1] = ptr[j] + len(s)
         seeds = np.concatenate([np.asarray(s, np.int32) for s in seed_sets]) if k else np.zeros(0, np.int32)
         seeds = _i32(seeds)
-        res = np.empty((k, self.n), np.float64)
+        res = self._batch_out(k, out)
         sts = (EgprStats * k)()
         flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
         check(lib.egpr_pagerank_seeds(self.handle, float(alpha), int(max_iter), float(tol), k, _ptr(ptr),
@@ -278,6 +288,32 @@ class PreparedGraph:
             self.close()
         except Exception:
             pass
+
+
+def pinned_empty(shape, dtype=np.float64):
+    """A page-locked host array (CUDA copies into it run at full link speed);
+    a plain array where page-locked memory cannot be had.  Keep the array
+    alive for as long as its data is used (it keeps the memory)."""
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            t = torch.empty(tuple(int(x) for x in np.atleast_1d(shape)), dtype=_TORCH_DTYPES[np.dtype(dtype)],
+                            pin_memory=True)
+            return t.numpy()  # the array's base holds the page-locked storage
+    except Exception:
+        pass
+    return np.empty(shape, dtype)
+
+
+_TORCH_DTYPES = {}
+try:
+    import torch as _torch
+
+    _TORCH_DTYPES = {np.dtype(np.float64): _torch.float64, np.dtype(np.float32): _torch.float32,
+                     np.dtype(np.int32): _torch.int32, np.dtype(np.int64): _torch.int64}
+except Exception:  # torch is optional here
+    pass
 
 
 def pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6, correction=True):

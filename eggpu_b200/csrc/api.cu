@@ -159,6 +159,49 @@ void DevBuf::release() {
     pooled = false;
 }
 
+int DevBuf::grow_on(size_t b, cudaStream_t s) {
+    if (b == 0) b = 16;
+    const int d = current_device();
+    if (p && b <= bytes && dev == d) return EGPR_SUCC;
+    release_on(s);
+    cudaMemPool_t pool = device_pool();
+    cudaError_t e;
+    if (pool) {
+        e = cudaMallocFromPoolAsync(&p, b, pool, s);
+        pooled = true;
+    } else {
+        e = cudaMalloc(&p, b);
+        pooled = false;
+    }
+    if (e != cudaSuccess) {
+        p = nullptr;
+        pooled = false;
+        cudaGetLastError();
+        set_cuda_error(e, "device allocation");
+        return EGPR_FAILED_TO_ALLOCATE_DEVICE_MEM;
+    }
+    dev = d;
+    bytes = b;
+    g_live_bytes += (int64_t)b;
+    return EGPR_SUCC;
+}
+
+void DevBuf::release_on(cudaStream_t s) {
+    if (p) {
+        if (pooled) {
+            cudaFreeAsync(p, s);  // after the work already queued on s
+        } else {
+            cudaStreamSynchronize(s);
+            cudaFree(p);
+        }
+        g_live_bytes -= (int64_t)bytes;
+    }
+    p = nullptr;
+    bytes = 0;
+    dev = -1;
+    pooled = false;
+}
+
 Plan::~Plan() { release(); }
 
 void Plan::release() {
@@ -177,6 +220,18 @@ void Plan::release() {
     d_span_acc.release();
     d_span_cnt.release();
     d_span_list.release();
+    ngraphs = nchunks = grid = any_weighted = max_n = nspans = nacc = 0;
+}
+
+void Plan::release_on(cudaStream_t s) {
+    if (cg_exec) cudaGraphExecDestroy(cg_exec);
+    if (cg) cudaGraphDestroy(cg);
+    cg_exec = nullptr;
+    cg = nullptr;
+    cond = 0;
+    cg_failed = false;
+    for (DevBuf* b : {&d_chunks, &d_graphs, &d_states, &d_ndang, &d_ctl, &d_acc, &d_span_acc, &d_span_cnt, &d_span_list})
+        b->release_on(s);
     ngraphs = nchunks = grid = any_weighted = max_n = nspans = nacc = 0;
 }
 
@@ -311,7 +366,7 @@ struct MultiPlan {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ~MultiPlan() {
-        plan.release();
+        plan.release_on(stream);  // the plan's buffers serve this stream only
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);

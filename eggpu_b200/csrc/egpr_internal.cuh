@@ -142,6 +142,11 @@ struct DevBuf {
     bool pooled = false;  // from device_pool() (else cudaMalloc)
     int alloc(size_t b);
     void release();
+    // Stream-ordered forms for buffers used by one stream only: grow_on keeps
+    // a large enough buffer and otherwise frees and allocates in the order of
+    // stream s; neither waits for the device.
+    int grow_on(size_t b, cudaStream_t s);
+    void release_on(cudaStream_t s);
     template <typename T>
     T* as() const { return static_cast<T*>(p); }
 };
@@ -169,6 +174,7 @@ struct Plan {
     float l2_hit_ratio = 0.f;
     ~Plan();
     void release();
+    void release_on(cudaStream_t s);  // buffers used by stream s only: freed in its order
 };
 
 struct SpmmWork;  // batched personalised PageRank workspace (spmm.cu)
@@ -232,6 +238,7 @@ int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
 // Plans and sweeps (sweep.cu).
 int sweep_grid();
 int sweep_resident_warps();
+int work_grid(int64_t entries, int full);  // CTAs of a launch over that many entries
 int32_t hub_stride(int32_t nhub);  // floats per parity of the hub copy (zero slot included)
 int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_t stream);
 int plan_capture_loop(Plan& plan, cudaStream_t stream);

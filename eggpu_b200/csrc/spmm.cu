@@ -186,6 +186,7 @@ struct Lane {
     int32_t p;
     bool live0, live1;
     bool all;         // every column of the panel takes part
+    bool same;        // FP64 sweep: every column's x_{k-1} is in the same buffer (xa)
 };
 
 // Reads the lane's two column states for panel p; skip = no column of the
@@ -204,6 +205,7 @@ __device__ Lane<kF64> make_lane(const SpmmParams& P, int32_t p, bool& skip) {
     L.out64 = nullptr;
     L.dm0 = L.dm1 = 0.0;
     L.df0 = L.df1 = 0.f;
+    L.same = true;
     if (!kF64) {
         L.live0 = a0 && !d0;
         L.live1 = a1 && !d1;
@@ -224,8 +226,17 @@ __device__ Lane<kF64> make_lane(const SpmmParams& P, int32_t p, bool& skip) {
         L.live1 = a1 != 0;
         skip = __ballot_sync(kAll, L.live0 || L.live1) == 0u;
         L.all = __all_sync(kAll, L.live0 && L.live1);
-        L.xa = P.X[(i0 - 1) & 1] + pbase;
-        L.xb = P.X[(i1 - 1) & 1] + pbase;
+        const int par0 = (i0 - 1) & 1, par1 = (i1 - 1) & 1;
+        const unsigned odd = __ballot_sync(kAll, (L.live0 && par0) || (L.live1 && par1));
+        const unsigned even = __ballot_sync(kAll, (L.live0 && !par0) || (L.live1 && !par1));
+        L.same = odd == 0u || even == 0u;
+        if (L.same) {
+            L.xa = P.X[odd ? 1 : 0] + pbase;
+            L.xb = L.xa;
+        } else {
+            L.xa = P.X[par0] + pbase;
+            L.xb = P.X[par1] + pbase;
+        }
         L.out64 = P.out64 + pbase;
         L.dm0 = __ldcg(&cs[0].dmass_prev);
         L.dm1 = __ldcg(&cs[1].dmass_prev);
@@ -356,6 +367,10 @@ __device__ __forceinline__ void prev_of(const Lane<kF64>& L, int c2, int32_t v, 
         const float2 q = __ldg(reinterpret_cast<const float2*>(L.xa + off));
         a = q.x;
         b = q.y;
+    } else if (L.same) {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(L.xa + off));
+        a = (double)q.x;
+        b = (double)q.y;
     } else {
         a = (double)__ldg(L.xa + off);
         b = (double)__ldg(L.xb + off + 1);
@@ -451,10 +466,10 @@ __device__ void process_unit(const SpmmParams& P, SpSmem<kF64>& S, int32_t p, in
             for (int s = 0; s < 8; ++s) {
                 const int32_t u = __shfl_sync(kAll, ec, 16 * h + 2 * s + g) & 0x7fffffff;
                 const size_t off = (size_t)u * kLanes + c2;
-                if (!kF64) {
+                if (!kF64 || L.same) {
                     const float2 v = __ldg(reinterpret_cast<const float2*>(xa + off));
-                    gx[s] = v.x;
-                    gy[s] = v.y;
+                    gx[s] = (Real)v.x;
+                    gy[s] = (Real)v.y;
                 } else {
                     gx[s] = (Real)__ldg(xa + off);
                     gy[s] = (Real)__ldg(xb + off + 1);
@@ -872,10 +887,14 @@ struct SpmmWork {
     cudaGraph_t cg = nullptr;
     cudaGraphExec_t cg_exec = nullptr;
     cudaGraphConditionalHandle cond = 0;
+    int cg_grid = 0;
     bool cg_failed = false;
     ~SpmmWork() {
         if (cg_exec) cudaGraphExecDestroy(cg_exec);
         if (cg) cudaGraphDestroy(cg);
+        for (DevBuf* b : {&src, &c32, &c64, &chunks, &X0, &X1, &out64, &cols, &parts, &span_cnt, &gacc, &colsum, &ctl,
+                          &meta, &params, &out, &tele, &tele_v})
+            b->release();
     }
 };
 
@@ -897,8 +916,8 @@ int build_spmm_layout(egpr_graph* g, SpmmWork& w, cudaStream_t s) {
     const int32_t nch = (int32_t)((g->sw_nnz + C - 1) / C);
     const int64_t epad = (int64_t)nch * C;
     int rc;
-    if ((rc = w.src.alloc((size_t)epad * sizeof(int32_t))) || (rc = w.c32.alloc((size_t)epad * sizeof(float))) ||
-        (rc = w.c64.alloc((size_t)epad * sizeof(double))) || (rc = w.chunks.alloc((size_t)nch * sizeof(SpChunk))))
+    if ((rc = w.src.grow_on((size_t)epad * sizeof(int32_t), s)) || (rc = w.c32.grow_on((size_t)epad * sizeof(float), s)) ||
+        (rc = w.c64.grow_on((size_t)epad * sizeof(double), s)) || (rc = w.chunks.grow_on((size_t)nch * sizeof(SpChunk), s)))
         return rc;
     k_sp_entries<<<grid_1d(epad), 256, 0, s>>>(g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr,
                                                g->sw_nnz, epad, g->hub_ids.as<int32_t>(), g->nhub,
@@ -920,15 +939,15 @@ int ensure_capacity(egpr_graph* g, SpmmWork& w, int32_t npanels, cudaStream_t s)
     const size_t xs = (size_t)npanels * ((size_t)n + 1) * kLanes;
     const size_t units = (size_t)npanels * w.nchunks;
     int rc;
-    if ((rc = w.X0.alloc(xs * sizeof(float))) || (rc = w.X1.alloc(xs * sizeof(float))) ||
-        (rc = w.out64.alloc(xs * sizeof(double))) ||
-        (rc = w.cols.alloc((size_t)npanels * kLanes * sizeof(ColState))) ||
-        (rc = w.parts.alloc(units * 2 * kLanes * sizeof(double))) ||
-        (rc = w.span_cnt.alloc(units * sizeof(uint32_t))) ||
-        (rc = w.gacc.alloc((size_t)npanels * kAccQ * kLanes * sizeof(unsigned long long))) ||
-        (rc = w.colsum.alloc((size_t)npanels * 2 * kLanes * sizeof(unsigned long long))) ||
-        (rc = w.ctl.alloc(sizeof(Ctl))) || (rc = w.params.alloc(sizeof(SpmmParams))) ||
-        (rc = w.meta.alloc(((size_t)n + 1) * sizeof(uint32_t))))
+    if ((rc = w.X0.grow_on(xs * sizeof(float), s)) || (rc = w.X1.grow_on(xs * sizeof(float), s)) ||
+        (rc = w.out64.grow_on(xs * sizeof(double), s)) ||
+        (rc = w.cols.grow_on((size_t)npanels * kLanes * sizeof(ColState), s)) ||
+        (rc = w.parts.grow_on(units * 2 * kLanes * sizeof(double), s)) ||
+        (rc = w.span_cnt.grow_on(units * sizeof(uint32_t), s)) ||
+        (rc = w.gacc.grow_on((size_t)npanels * kAccQ * kLanes * sizeof(unsigned long long), s)) ||
+        (rc = w.colsum.grow_on((size_t)npanels * 2 * kLanes * sizeof(unsigned long long), s)) ||
+        (rc = w.ctl.grow_on(sizeof(Ctl), s)) || (rc = w.params.grow_on(sizeof(SpmmParams), s)) ||
+        (rc = w.meta.grow_on(((size_t)n + 1) * sizeof(uint32_t), s)))
         return rc;
     if ((rc = cuda_ok(cudaMemsetAsync(w.X1.p, 0, xs * sizeof(float), s), "memset")) ||
         (rc = cuda_ok(cudaMemsetAsync(w.span_cnt.p, 0, units * sizeof(uint32_t), s), "memset")) ||
@@ -947,6 +966,12 @@ int ensure_capacity(egpr_graph* g, SpmmWork& w, int32_t npanels, cudaStream_t s)
 
 // The sweep loop as a CUDA-graph while node whose body is one k_spmm launch.
 void build_loop_graph(SpmmWork& w, int grid) {
+    if (w.cg_exec && w.cg_grid != grid) {  // built for another launch size
+        cudaGraphExecDestroy(w.cg_exec);
+        cudaGraphDestroy(w.cg);
+        w.cg_exec = nullptr;
+        w.cg = nullptr;
+    }
     if (w.cg_exec || w.cg_failed) return;
     const SpmmParams* Pd = w.params.as<SpmmParams>();
     cudaGraph_t cg = nullptr;
@@ -979,6 +1004,7 @@ void build_loop_graph(SpmmWork& w, int grid) {
         w.cg = cg;
         w.cg_exec = ex;
         w.cond = h;
+        w.cg_grid = grid;
     } else {
         cudaGetLastError();
         if (cg) cudaGraphDestroy(cg);
@@ -1010,9 +1036,9 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     std::vector<float> tt((size_t)std::max(nt, 1) * ld, 0.f);
     for (int32_t jj = 0; jj < kg; ++jj)
         for (const auto& pr : per_col[(size_t)(j0 + jj)]) tt[(size_t)tidx[(size_t)pr.first] * ld + jj] = pr.second;
-    if ((rc = w.tele.alloc(tt.size() * sizeof(float))) ||
-        (rc = w.tele_v.alloc((size_t)std::max(nt, 1) * sizeof(int32_t))) ||
-        (rc = w.out.alloc((size_t)kg * n * sizeof(double))))
+    if ((rc = w.tele.grow_on(tt.size() * sizeof(float), s)) ||
+        (rc = w.tele_v.grow_on((size_t)std::max(nt, 1) * sizeof(int32_t), s)) ||
+        (rc = w.out.grow_on((size_t)kg * n * sizeof(double), s)))
         return rc;
     if ((rc = cuda_ok(cudaMemcpyAsync(w.tele.p, tt.data(), tt.size() * sizeof(float), cudaMemcpyHostToDevice, s),
                       "H2D teleport")) ||
@@ -1054,8 +1080,10 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
         (rc = cuda_ok(cudaMemcpyAsync(w.ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D ctl")))
         return rc;
     const SpmmParams* Pd = w.params.as<SpmmParams>();
-    const int grid = spmm_grid(false);
-    const int grid64 = spmm_grid(true);
+    // the SpMM does about four times the work of a single-vector sweep per entry and panel
+    const int64_t work = 4 * (int64_t)npanels * w.epad;
+    const int grid = work_grid(work, spmm_grid(false));
+    const int grid64 = work_grid(work, spmm_grid(true));
     if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event"))) return rc;
     k_sp_meta<<<grid_1d(n), 256, 0, s>>>(g->outw.as<double>(), n, w.meta.as<uint32_t>());
     if (nt > 0) k_sp_tele_rows<<<(nt + 255) / 256, 256, 0, s>>>(w.tele_v.as<int32_t>(), nt, w.meta.as<uint32_t>());

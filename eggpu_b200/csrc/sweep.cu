@@ -807,6 +807,21 @@ int32_t hub_stride(int32_t nhub) { return (nhub + 1 + 31) & ~31; }
 
 int sweep_resident_warps() { return sweep_grid() * kCtaWarps; }
 
+// CTAs for a persistent launch over `entries` inbound entries: one per
+// EGPR_CTA_ENTRIES entries (default 32768), at most `full`.  A small graph
+// then holds a few SMs instead of all of them, so solves of other graphs on
+// other streams run beside it (0: always the full grid).
+int work_grid(int64_t entries, int full) {
+    static const int64_t per = [] {
+        const char* e = std::getenv("EGPR_CTA_ENTRIES");
+        const long long x = e ? std::atoll(e) : 32768;
+        return (int64_t)(x >= 0 ? x : 32768);
+    }();
+    if (per == 0) return std::max(1, full);
+    const int64_t want = (entries + per - 1) / per;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, full));
+}
+
 // One persistent CTA per SM.
 int sweep_grid() {
     static int cache[64] = {};
@@ -910,7 +925,9 @@ int plan_build(Plan& plan, egpr_graph* const* graphs, int32_t count, cudaStream_
     plan.max_n = max_n;
     plan.any_weighted = any_w;
     plan.hub_count = count == 1 ? hub_stride(graphs[0]->nhub) : 0;
-    plan.grid = std::max(1, std::min(plan.nchunks, sweep_grid()));
+    int64_t entries = 0;
+    for (int32_t gi = 0; gi < count; ++gi) entries += graphs[gi]->sw_nnz;
+    plan.grid = std::max(1, std::min(plan.nchunks, work_grid(entries, sweep_grid())));
     // accumulator slots: 64 per graph (few for the launch's last CTA to read,
     // enough that concurrent chunks rarely add to the same address), fewer
     // for many graphs

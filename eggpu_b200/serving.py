@@ -48,12 +48,13 @@ class Request:
     future: Future = field(default_factory=Future)
     done_at: float = 0.0
     iterations: int = 0
+    keep_result: bool = True  # False: the future gets (None, stats) once the ranks are on the host
 
 
 class GraphRegistry:
     """Device-resident prepared graphs, admitted by HBM bytes (LRU eviction of idle graphs)."""
 
-    def __init__(self, sources, budget_bytes):
+    def __init__(self, sources, budget_bytes, priority_max_n=1_000_000):
         self.sources = dict(sources)  # graph id -> (V, E, W)
         self.budget = int(budget_bytes)
         self.resident = collections.OrderedDict()  # id -> PreparedGraph
@@ -61,9 +62,15 @@ class GraphRegistry:
         self.lock = threading.Condition()
         self.evictions = 0
         self.admissions = 0
+        self.loading = {}  # id -> bytes reserved while its graph is prepared (outside the lock)
+        # graphs of at most priority_max_n vertices solve on high-priority
+        # streams: their kernels take the SMs first whenever a long launch of
+        # a large graph ends
+        self.priority_max_n = int(priority_max_n)
+        self.streams = {}
 
     def _bytes(self):
-        return sum(pg.info()["device_bytes"] for pg in self.resident.values())
+        return sum(pg.info()["device_bytes"] for pg in self.resident.values()) + sum(self.loading.values())
 
     @staticmethod
     def estimate_bytes(V, E, W):
@@ -71,8 +78,30 @@ class GraphRegistry:
         m = len(E)
         return 4 * (n + 1) + 4 * m * (2 if W is not None else 1) + 8 * n + 4 * n + 24 * n + 16 * n + 64 * 1024
 
+    def _prioritize(self, gid, pg):
+        if pg.n > self.priority_max_n:
+            return
+        try:
+            import torch
+
+            if not torch.cuda.is_available():
+                return
+            lo, hi = torch.cuda.Stream.priority_range()
+            st = torch.cuda.Stream(priority=min(lo, hi))  # the numerically lowest value is the highest priority
+            pg.set_stream(st.cuda_stream)
+            self.streams[gid] = st
+        except Exception:  # priorities are an optimisation only
+            pass
+
+    def _evict(self, gid):
+        self.resident.pop(gid).close()
+        self.streams.pop(gid, None)
+        self.evictions += 1
+
     def acquire(self, gid):
-        """The prepared graph for gid, marked busy; waits for HBM room if needed."""
+        """The prepared graph for gid, marked busy; waits for HBM room if needed.
+        A graph is prepared outside the lock, so requests for resident graphs
+        go on meanwhile."""
         with self.lock:
             while True:
                 pg = self.resident.get(gid)
@@ -80,6 +109,9 @@ class GraphRegistry:
                     self.resident.move_to_end(gid)
                     self.busy[gid] += 1
                     return pg
+                if gid in self.loading:  # another thread prepares it
+                    self.lock.wait(0.01)
+                    continue
                 V, E, W = self.sources[gid]
                 need = self.estimate_bytes(V, E, W)
                 used = self._bytes()
@@ -88,15 +120,35 @@ class GraphRegistry:
                         break
                     if self.busy[victim] == 0:
                         used -= self.resident[victim].info()["device_bytes"]
-                        self.resident.pop(victim).close()
-                        self.evictions += 1
-                if used + need <= self.budget or not any(self.busy.values()):
-                    pg = _native.PreparedGraph(V, E, W)
-                    self.resident[gid] = pg
-                    self.admissions += 1
-                    self.busy[gid] += 1
-                    return pg
+                        self._evict(victim)
+                if used + need <= self.budget or not (any(self.busy.values()) or self.loading):
+                    self.loading[gid] = need
+                    break
                 self.lock.wait(0.01)
+        try:
+            pg = _native.PreparedGraph(V, E, W)
+        except BaseException:
+            with self.lock:
+                self.loading.pop(gid, None)
+                self.lock.notify_all()
+            raise
+        with self.lock:
+            self._prioritize(gid, pg)
+            self.loading.pop(gid, None)
+            self.resident[gid] = pg
+            self.admissions += 1
+            self.busy[gid] += 1
+            self.lock.notify_all()
+        return pg
+
+    def warm(self, gids):
+        """Prepares the given graphs ahead of traffic (as a server loads its
+        graphs before it takes requests); returns the seconds it took."""
+        t0 = time.perf_counter()
+        for gid in gids:
+            self.acquire(gid)
+            self.release(gid)
+        return time.perf_counter() - t0
 
     def release(self, gid):
         with self.lock:
@@ -108,13 +160,26 @@ class GraphRegistry:
             for pg in self.resident.values():
                 pg.close()
             self.resident.clear()
+            self.streams.clear()
 
 
 class Server:
     """Serves Request objects; submit() returns a Future resolving to (ranks, stats)."""
 
-    def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True):
+    def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True, pinned=True,
+                 multi_min=8, ppr_min_batch=6):
         self.registry = registry
+        # a batched solve gathers one 32-column panel per inbound entry, about
+        # seven single-vector sweeps' worth: fewer PPR requests than this for
+        # one graph are solved one by one
+        self.ppr_min_batch = int(ppr_min_batch)
+        # plain requests of small graphs share one multi-graph launch once at
+        # least multi_min such graphs wait (a launch plan over a new set of
+        # graphs costs more than a few single solves)
+        self.multi_min = int(multi_min)
+        # results land in page-locked host arrays (copied at full link speed;
+        # the allocator reuses the memory once a result is dropped)
+        self.pinned = bool(pinned)
         self.max_columns = int(max_columns)
         self.multi_max_n = int(multi_max_n)
         self.fold_multi = fold_multi
@@ -157,10 +222,10 @@ class Server:
         reqs = list(self.queues.pop(best))
         work = [(best, reqs)]
         if self.fold_multi and all(r.kind == "pr" for r in reqs) and self._small(best):
-            for gid, q in list(self.queues.items()):
-                if len(work) >= 64:
-                    break
-                if q and gid not in self.running and all(r.kind == "pr" for r in q) and self._small(gid):
+            more = [gid for gid, q in self.queues.items()
+                    if q and gid not in self.running and all(r.kind == "pr" for r in q) and self._small(gid)]
+            if len(more) + 1 >= self.multi_min:
+                for gid in more[:63]:
                     self.running.add(gid)
                     work.append((gid, list(self.queues.pop(gid))))
         return work
@@ -196,7 +261,10 @@ class Server:
     def _finish(self, req, ranks, stats):
         req.done_at = time.perf_counter()
         req.iterations = int(stats["iterations"])
-        req.future.set_result((ranks, stats))
+        req.future.set_result((ranks if req.keep_result else None, stats))
+
+    def _out(self, shape):
+        return _native.pinned_empty(shape) if self.pinned else None
 
     def _run(self, work):
         if len(work) > 1:
@@ -210,15 +278,21 @@ class Server:
                 by_params[(r.kind, r.alpha, r.max_iter, r.tol)].append(r)
             for (kind, alpha, max_iter, tol), group in by_params.items():
                 if kind == "pr":
-                    ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol)
+                    ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol, out=self._out(pg.n))
                     self.stats["pr_solves"] += 1
                     for r in group:
+                        self._finish(r, ranks, st)
+                elif len(group) < self.ppr_min_batch:
+                    for r in group:
+                        ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol,
+                                                personalization=_teleport(pg.n, r.seeds), out=self._out(pg.n))
+                        self.stats["ppr_single"] += 1
                         self._finish(r, ranks, st)
                 else:
                     for s in range(0, len(group), self.max_columns):
                         part = group[s:s + self.max_columns]
                         ranks, sts = pg.pagerank_seeds([r.seeds for r in part], alpha=alpha, max_iter=max_iter,
-                                                       tol=tol)
+                                                       tol=tol, out=self._out((len(part), pg.n)))
                         self.stats["ppr_batches"] += 1
                         self.stats["ppr_columns"] += len(part)
                         for j, r in enumerate(part):
@@ -248,6 +322,13 @@ class Server:
         finally:
             for gid in gids[:len(pgs)]:
                 self.registry.release(gid)
+
+
+def _teleport(n, seeds):
+    """Uniform teleport vector over a seed set (the batched solve's column)."""
+    p = np.zeros(n)
+    p[np.unique(np.asarray(seeds, np.int64))] = 1.0
+    return p / p.sum()
 
 
 def poisson_arrivals(rate, count, seed):

@@ -335,6 +335,11 @@ def test_ppr_batch_is_deterministic_and_columns_independent():
     a, _ = pg.pagerank_seeds(sets, alpha=0.85, max_iter=30, tol=1e-6)
     b, _ = pg.pagerank_seeds(sets, alpha=0.85, max_iter=30, tol=1e-6)
     assert np.array_equal(a, b)
+    held = _native.pinned_empty(a.shape)  # a caller's reused (page-locked) result array
+    c, _ = pg.pagerank_seeds(sets, alpha=0.85, max_iter=30, tol=1e-6, out=held)
+    assert c is held and np.array_equal(a, c)
+    with pytest.raises(ValueError):
+        pg.pagerank_seeds(sets, alpha=0.85, max_iter=30, tol=1e-6, out=np.empty((3, g.n)))
     sub, _ = pg.pagerank_seeds(sets[5:9], alpha=0.85, max_iter=30, tol=1e-6)
     assert np.abs(sub - a[5:9]).sum(axis=1).max() <= L1_TOL
 

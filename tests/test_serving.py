@@ -27,13 +27,17 @@ class FakePrepared:
     def info(self):
         return {"device_bytes": serving.GraphRegistry.estimate_bytes(self.V, self.E, self.W)}
 
-    def pagerank(self, alpha, max_iter, tol, personalization=None):
+    def pagerank(self, alpha, max_iter, tol, personalization=None, out=None):
         FakePrepared.calls.append(("pr", self.n))
         time.sleep(0.002)
-        r, it, res = oracle.pagerank_push(self.V, self.E, self.W, alpha=alpha, max_iter=max_iter, tol=tol)
+        r, it, res = oracle.pagerank_push(self.V, self.E, self.W, alpha=alpha, max_iter=max_iter, tol=tol,
+                                          teleport=personalization)
+        if out is not None:
+            out[:] = r
+            r = out
         return r, {"iterations": it}
 
-    def pagerank_seeds(self, seed_sets, alpha, max_iter, tol):
+    def pagerank_seeds(self, seed_sets, alpha, max_iter, tol, out=None):
         FakePrepared.calls.append(("ppr", self.n, len(seed_sets)))
         time.sleep(0.002)
         outs, sts = [], []
@@ -44,6 +48,9 @@ class FakePrepared:
                                             teleport=p / p.sum())
             outs.append(r)
             sts.append({"iterations": it})
+        if out is not None:
+            out[:] = np.array(outs)
+            return out, sts
         return np.array(outs), sts
 
     def close(self):
@@ -81,7 +88,7 @@ def _sources(k=5):
 def test_requests_are_folded_and_answers_match_standalone(fake_engine):
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=2)
+    srv = serving.Server(reg, workers=2, ppr_min_batch=2)
     rng = np.random.default_rng(0)
     reqs = []
     for i in range(60):
@@ -110,6 +117,56 @@ def test_requests_are_folded_and_answers_match_standalone(fake_engine):
     assert lat["count"] == 60 and lat["p99_ms"] >= lat["p50_ms"]
 
 
+@pytest.mark.parametrize("multi_min,expect_multi", [(2, True), (100, False)])
+def test_plain_requests_of_small_graphs_share_a_launch_past_a_threshold(fake_engine, multi_min, expect_multi):
+    src = _sources()
+    reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
+    srv = serving.Server(reg, workers=1, multi_min=multi_min)
+    gate = threading.Event()
+    first = serving.Request(0, "pr")
+    orig = srv._run
+
+    def held(work):  # the first solve waits until the others have queued up
+        gate.wait(10)
+        orig(work)
+
+    srv._run = held
+    srv.submit(first)
+    time.sleep(0.05)
+    reqs = [serving.Request(gid, "pr") for gid in (1, 2, 3, 4)]
+    for r in reqs:
+        srv.submit(r)
+    gate.set()
+    for r in [first] + reqs:
+        ranks, st = r.future.result(timeout=60)
+        alone, it, _ = oracle.pagerank_push(*src[r.graph])
+        assert np.array_equal(ranks, alone) and st["iterations"] == it
+    srv.close()
+    assert any(c[0] == "multi" for c in FakePrepared.calls) == expect_multi
+    reg.close()
+
+
+def test_a_few_ppr_requests_are_solved_one_by_one(fake_engine):
+    src = _sources()
+    reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
+    srv = serving.Server(reg, workers=1, ppr_min_batch=4)
+    rng = np.random.default_rng(1)
+    reqs = [serving.Request(2, "ppr", seeds=rng.choice(src[2][0].shape[0] - 1, 3, replace=False)) for _ in range(3)]
+    for r in reqs:
+        srv.submit(r)
+    for r in reqs:
+        ranks, st = r.future.result(timeout=60)
+        V, E, W = src[2]
+        p = np.zeros(V.shape[0] - 1)
+        p[np.unique(r.seeds)] = 1.0
+        alone, it, _ = oracle.pagerank_push(V, E, W, teleport=p / p.sum())
+        assert np.array_equal(ranks, alone) and st["iterations"] == it
+    srv.close()
+    assert not any(c[0] == "ppr" for c in FakePrepared.calls)
+    assert srv.stats["ppr_single"] == 3
+    reg.close()
+
+
 def test_admission_by_bytes_evicts_idle_graphs(fake_engine):
     src = _sources()
     sizes = [serving.GraphRegistry.estimate_bytes(*src[i]) for i in src]
@@ -136,7 +193,7 @@ def test_served_results_equal_standalone_results_on_gpu():
         c = synth.rmat(scale=scale, edgefactor=ef, seed=2000 + i)
         src[i] = (c.V, c.E, None)
     reg = serving.GraphRegistry(src, budget_bytes=1 << 34)
-    srv = serving.Server(reg, workers=3)
+    srv = serving.Server(reg, workers=3, ppr_min_batch=2)  # batched and single PPR solves both occur
     rng = np.random.default_rng(1)
     reqs = []
     for i in range(300):
