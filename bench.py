@@ -449,6 +449,11 @@ def run_serving(args):
     wall = serving.replay(srv, reqs, times)
     srv.close()
     lat = serving.latency_summary(reqs)
+    # capacity: the same requests all at once (queued requests fold into batched solves)
+    burst = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
+    srv2 = serving.Server(reg, workers=int(os.environ.get("EGPR_SERVING_WORKERS", "4")))
+    burst_wall = serving.replay(srv2, burst, np.zeros(n_req))
+    srv2.close()
     # plain unbatched per-request solves of a sample, on the same GPU
     sample = reqs[:: max(1, n_req // 200)]
     plain_lat = []
@@ -474,6 +479,8 @@ def run_serving(args):
                        "total_nnz": int(sum(len(v[1]) for v in src.values()))},
             "serving": {"latency": lat, "solves_per_s": n_req / wall, "offered_req_per_s": 1000.0,
                         "server_stats": dict(srv.stats), "admissions": reg.admissions, "evictions": reg.evictions,
+                        "capacity_burst": {"solves_per_s": n_req / burst_wall, "wall_s": burst_wall,
+                                           "server_stats": dict(srv2.stats)},
                         "plain_unbatched_service_ms": {"p50": float(np.percentile(plain, 50) * 1e3),
                                                        "p99": float(np.percentile(plain, 99) * 1e3),
                                                        "mean": float(plain.mean() * 1e3)},

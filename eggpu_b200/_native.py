@@ -77,6 +77,24 @@ class EgprCacheStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class EgprTuning(ctypes.Structure):
+    _fields_ = [
+        ("chunks_per_warp", c_int32),
+        ("row_cost", c_int32),
+        ("spmm_chunk", c_int32),
+        ("configs_tried", c_int32),
+        ("sweep_ms", c_double),
+        ("spmm_sweep_ms", c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+EGPR_TUNE_SWEEP = 1
+EGPR_TUNE_SPMM = 2
+
+
 # (name, restype, argtypes) for every entry point of include/egpr.h.
 _SIGNATURES = [
     ("egpr_status_string", c_char_p, [c_int]),
@@ -86,6 +104,9 @@ _SIGNATURES = [
     ("egpr_graph_info_get", c_int, [c_void_p, POINTER(EgprGraphInfo)]),
     ("egpr_graph_export_inbound", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("egpr_graph_set_stream", c_int, [c_void_p, c_void_p]),
+    ("egpr_graph_autotune", c_int, [c_void_p, c_uint32, POINTER(EgprTuning)]),
+    ("egpr_graph_get_tuning", c_int, [c_void_p, POINTER(EgprTuning)]),
+    ("egpr_graph_set_tuning", c_int, [c_void_p, POINTER(EgprTuning)]),
     ("egpr_pagerank", c_int, [c_void_p, c_double, c_int32, c_double, c_void_p, c_uint32, c_void_p, POINTER(EgprStats)]),
     ("egpr_pagerank_enqueue", c_int, [c_void_p, c_double, c_int32, c_double, c_uint32]),
     ("egpr_pagerank_collect", c_int, [c_void_p, c_void_p, POINTER(EgprStats)]),
@@ -209,6 +230,29 @@ class PreparedGraph:
         check(lib.egpr_graph_export_inbound(self.handle, _ptr(in_row), _ptr(in_col), _ptr(in_w), _ptr(dang), _ptr(outw)),
               "egpr_graph_export_inbound")
         return in_row, in_col[:nnz], in_w[:nnz], dang, outw
+
+    def autotune(self, sweep=True, spmm=True) -> dict:
+        """Times candidate work layouts on this graph and keeps the fastest
+        (egpr_graph_autotune); returns the chosen parameters and timings."""
+        what = (EGPR_TUNE_SWEEP if sweep else 0) | (EGPR_TUNE_SPMM if spmm else 0)
+        if what == 0:
+            return self.tuning()
+        t = EgprTuning()
+        check(lib.egpr_graph_autotune(self.handle, what, ctypes.byref(t)), "egpr_graph_autotune")
+        return t.as_dict()
+
+    def tuning(self) -> dict:
+        t = EgprTuning()
+        check(lib.egpr_graph_get_tuning(self.handle, ctypes.byref(t)), "egpr_graph_get_tuning")
+        return {k: v for k, v in t.as_dict().items() if k in ("chunks_per_warp", "row_cost", "spmm_chunk")}
+
+    def set_tuning(self, chunks_per_warp=None, row_cost=None, spmm_chunk=None) -> None:
+        cur = self.tuning()
+        t = EgprTuning()
+        t.chunks_per_warp = cur["chunks_per_warp"] if chunks_per_warp is None else int(chunks_per_warp)
+        t.row_cost = cur["row_cost"] if row_cost is None else int(row_cost)
+        t.spmm_chunk = cur["spmm_chunk"] if spmm_chunk is None else int(spmm_chunk)
+        check(lib.egpr_graph_set_tuning(self.handle, ctypes.byref(t)), "egpr_graph_set_tuning")
 
     def set_stream(self, stream_ptr: int | None) -> None:
         check(lib.egpr_graph_set_stream(self.handle, None if not stream_ptr else c_void_p(int(stream_ptr))),

@@ -478,6 +478,79 @@ static void destroy_graph_object(egpr_graph* g) {
     delete g;
 }
 
+// ---- layout tuning ----------------------------------------------------------
+namespace {
+
+bool tuning_valid(const egpr_tuning& t) {
+    return t.chunks_per_warp >= 1 && t.chunks_per_warp <= 64 && t.row_cost >= 0 && t.row_cost <= 64 &&
+           t.spmm_chunk >= 64 && t.spmm_chunk <= (1 << 16) && (t.spmm_chunk % 32) == 0;
+}
+
+// Rebuilds the sweep layout and the single-graph plan for the graph's current
+// parameters (the inbound CSR and the hub codes stay as prepared).
+int rebuild_sweep(egpr_graph* g) {
+    cudaStream_t s = g->own_stream;
+    int rc;
+    if ((rc = cuda_ok(cudaStreamSynchronize(g->stream), "tuning")) ||
+        (rc = cuda_ok(cudaStreamSynchronize(s), "tuning")))
+        return rc;
+    drop_multi_plans_with(g);  // they hold copies of the graph's chunk table
+    if ((rc = build_sweep_layout(g, sweep_resident_warps(), nullptr, s))) return rc;
+    egpr_graph* self = g;
+    if ((rc = plan_build(g->plan, &self, 1, s))) return rc;
+    const size_t nf = ((size_t)g->n + 8) * sizeof(float);
+    plan_set_l2_window(g->plan, g->z0.p, 2 * nf);
+    return EGPR_SUCC;
+}
+
+// Device time of one sweep of the graph's current layout: fixed-count solves
+// of S and S + L sweeps (no correction sweep), best of three, difference / L
+// (the candidates differ by a few percent, about the spread of one sample).
+int time_sweep(egpr_graph* g, double* ms) {
+    cudaStream_t s = g->stream;
+    const int32_t S = 3, L = 24;
+    double best[2] = {1e30, 1e30};
+    for (int rep = 0; rep < 3; ++rep)
+        for (int i = 0; i < 2; ++i) {
+            int32_t launches = 0;
+            int rc;
+            if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event")) ||
+                (rc = enqueue_plan(g->plan, 0.85, i ? S + L : S, 0.0, false, EGPR_FLAG_NO_CORRECTION, s, &launches)) ||
+                (rc = cuda_ok(cudaEventRecord(g->ev1, s), "event")) ||
+                (rc = cuda_ok(cudaStreamSynchronize(s), "tuning")))
+                return rc;
+            float t = 0.f;
+            cudaEventElapsedTime(&t, g->ev0, g->ev1);
+            best[i] = std::min(best[i], (double)t);
+        }
+    *ms = std::max(0.0, (best[1] - best[0]) / L);
+    return EGPR_SUCC;
+}
+
+// Device time of one batched sweep (one panel: 32 single-vertex seed sets).
+int time_spmm(egpr_graph* g, double* ms) {
+    const int32_t k = 32, S = 2, L = 8;
+    std::vector<int32_t> ptr(k + 1), seeds(k);
+    for (int32_t j = 0; j < k; ++j) {
+        ptr[(size_t)j] = j;
+        seeds[(size_t)j] = (int32_t)(((int64_t)j * 2654435761LL) % g->n);
+    }
+    ptr[(size_t)k] = k;
+    std::vector<egpr_stats> st((size_t)k);
+    double best[2] = {1e30, 1e30};
+    for (int rep = 0; rep < 2; ++rep)
+        for (int i = 0; i < 2; ++i) {
+            int rc = ppr_batch_solve(g, 0.85, i ? S + L : S, 0.0, k, nullptr, ptr.data(), seeds.data(),
+                                     EGPR_FLAG_NO_CORRECTION, nullptr, st.data());
+            if (rc) return rc;
+            best[i] = std::min(best[i], st[0].kernel_seconds * 1e3);
+        }
+    *ms = std::max(0.0, (best[1] - best[0]) / L);
+    return EGPR_SUCC;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* egpr_status_string(int status) {
@@ -525,6 +598,9 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
         return rc;
     }
     g->stream = g->own_stream;
+    g->tune_cpw = default_chunks_per_warp();
+    g->tune_rc = default_row_cost();
+    g->tune_spmm_chunk = default_spmm_chunk();
     if ((rc = prepare_graph(g, V, E, W))) {
         destroy_graph_object(g);
         return rc;
@@ -596,6 +672,95 @@ int egpr_graph_export_inbound(const egpr_graph* gc, int32_t* in_row, int32_t* in
         }
     }
     return cuda_ok(cudaStreamSynchronize(s), "export");
+}
+
+int egpr_graph_get_tuning(const egpr_graph* g, egpr_tuning* out) {
+    if (!g || !out) return fail_arg("NULL argument");
+    std::memset(out, 0, sizeof(*out));
+    out->chunks_per_warp = g->tune_cpw;
+    out->row_cost = g->tune_rc;
+    out->spmm_chunk = g->tune_spmm_chunk;
+    return EGPR_SUCC;
+}
+
+int egpr_graph_set_tuning(egpr_graph* g, const egpr_tuning* in) {
+    if (!g || !in) return fail_arg("NULL argument");
+    if (!tuning_valid(*in))
+        return fail_arg("tuning out of range: chunks_per_warp 1..64, row_cost 0..64, spmm_chunk 64..65536 in steps of 32");
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->pending) return fail_arg("a solve is pending on this graph");
+    int rc;
+    if ((rc = check_device(g))) return rc;
+    const bool sweep = in->chunks_per_warp != g->tune_cpw || in->row_cost != g->tune_rc;
+    const bool spmm = in->spmm_chunk != g->tune_spmm_chunk;
+    g->tune_cpw = in->chunks_per_warp;
+    g->tune_rc = in->row_cost;
+    g->tune_spmm_chunk = in->spmm_chunk;
+    if (spmm) {
+        cudaStreamSynchronize(g->stream);
+        spmm_work_release(g);  // rebuilt for the new tile by the next batched solve
+    }
+    if (sweep && g->nnz > 0 && (rc = rebuild_sweep(g))) return rc;
+    return EGPR_SUCC;
+}
+
+int egpr_graph_autotune(egpr_graph* g, uint32_t what, egpr_tuning* out) {
+    if (!g) return fail_arg("NULL graph");
+    if (what == 0) what = EGPR_TUNE_SWEEP | EGPR_TUNE_SPMM;
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->pending) return fail_arg("a solve is pending on this graph");
+    int rc;
+    if ((rc = check_device(g))) return rc;
+    egpr_tuning res;
+    std::memset(&res, 0, sizeof(res));
+    if (g->nnz > 0 && (what & EGPR_TUNE_SWEEP)) {
+        double best = 1e30;
+        int32_t bc = g->tune_cpw, br = g->tune_rc;
+        for (int32_t cpw : {4, 8, 16})
+            for (int32_t rcost : {2, 4, 8}) {
+                g->tune_cpw = cpw;
+                g->tune_rc = rcost;
+                double ms = 0.0;
+                if ((rc = rebuild_sweep(g)) || (rc = time_sweep(g, &ms))) return rc;
+                res.configs_tried += 1;
+                if (ms < best) {
+                    best = ms;
+                    bc = cpw;
+                    br = rcost;
+                }
+            }
+        g->tune_cpw = bc;
+        g->tune_rc = br;
+        if ((rc = rebuild_sweep(g))) return rc;
+        res.sweep_ms = best;
+    }
+    if (g->nnz > 0 && (what & EGPR_TUNE_SPMM)) {
+        double best = 1e30;
+        int32_t bc = g->tune_spmm_chunk;
+        for (int32_t c : {512, 1024, 2048}) {
+            cudaStreamSynchronize(g->stream);
+            spmm_work_release(g);
+            g->tune_spmm_chunk = c;
+            double ms = 0.0;
+            if ((rc = time_spmm(g, &ms))) return rc;
+            res.configs_tried += 1;
+            if (ms < best) {
+                best = ms;
+                bc = c;
+            }
+        }
+        if (bc != g->tune_spmm_chunk) {
+            cudaStreamSynchronize(g->stream);
+            spmm_work_release(g);
+            g->tune_spmm_chunk = bc;
+        }
+        res.spmm_sweep_ms = best;
+    }
+    res.chunks_per_warp = g->tune_cpw;
+    res.row_cost = g->tune_rc;
+    res.spmm_chunk = g->tune_spmm_chunk;
+    if (out) *out = res;
+    return EGPR_SUCC;
 }
 
 int egpr_graph_set_stream(egpr_graph* g, void* stream) {

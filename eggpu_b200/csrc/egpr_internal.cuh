@@ -201,6 +201,10 @@ struct egpr_graph {
     int64_t sw_nnz = 0;
     int32_t ntiles = 0;
     int32_t nhub = 0;
+    // layout parameters (egpr_tuning); defaults from the environment
+    int32_t tune_cpw = 8;           // sweep: work-queue chunks per resident warp
+    int32_t tune_rc = 4;            // sweep: cost of finishing a row, in entries
+    int32_t tune_spmm_chunk = 1024; // batched solve: entries per work unit
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
     egpr::Plan plan;               // single-graph plan
@@ -233,6 +237,9 @@ double wall_seconds();
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
 int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
 int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* sorted_dst, cudaStream_t s);
+int default_chunks_per_warp();  // EGPR_CHUNKS_PER_WARP, else 8
+int default_row_cost();         // EGPR_ROW_COST, else 4
+int32_t default_spmm_chunk();   // EGPR_SPMM_CHUNK, else 1024
 int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
 
 // Plans and sweeps (sweep.cu).

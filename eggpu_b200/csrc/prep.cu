@@ -558,11 +558,11 @@ __global__ void k_sweep_placeholders(const int32_t* __restrict__ in_row, int32_t
     }
 }
 
-namespace {
-
-int chunks_per_warp() {
+// Defaults of a graph's layout parameters (egpr_graph_set_tuning and
+// egpr_graph_autotune change them per graph).
+int default_chunks_per_warp() {
     static const int v = [] {
-        const char* e = std::getenv("EGPR_CHUNKS_PER_WARP");  // tuning: queue granularity
+        const char* e = std::getenv("EGPR_CHUNKS_PER_WARP");  // queue granularity
         const int x = e ? std::atoi(e) : 8;
         return x >= 1 && x <= 64 ? x : 8;
     }();
@@ -570,23 +570,21 @@ int chunks_per_warp() {
 }
 
 // Cost of finishing one row, in entries (a row costs its entries plus this).
-int row_cost() {
+int default_row_cost() {
     static const int v = [] {
-        const char* e = std::getenv("EGPR_ROW_COST");  // tuning
+        const char* e = std::getenv("EGPR_ROW_COST");
         const int x = e ? std::atoi(e) : 4;
         return x >= 0 && x <= 64 ? x : 4;
     }();
     return v;
 }
 
-}  // namespace
-
 // The sweep's work layout, built on the device (the host only sees the chunk
 // boundaries):
 //   * sw_row / sw_col / sw_w: the inbound CSR with a placeholder entry in every
 //     empty row, so that every row ends on an entry of its own;
 //   * chunks: boundaries at multiples of a cost cap along the rows, where a
-//     row costs its entries plus row_cost(); a boundary moves back to the
+//     row costs its entries plus the graph's row cost; a boundary moves back to the
 //     start of its row unless that row began before the previous boundary (a
 //     row longer than a chunk), which is then cut (a span: its chunks add
 //     pieces to the span's accumulator and the sweep finishes the row when the
@@ -615,10 +613,11 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
     const int32_t nnz = (int32_t)nnz_u;
     g->sw_nnz = nnz;
     // chunk boundaries at ideal costs d_i = i * cap
-    const int64_t R = row_cost();
+    const int64_t R = g->tune_rc;
     const int64_t warps = std::max(1, resident_warps);
     const int64_t total = (int64_t)nnz + R * (int64_t)n;
-    int64_t cap = (total + warps * chunks_per_warp() - 1) / (warps * chunks_per_warp());
+    const int64_t cpw = std::max(1, g->tune_cpw);
+    int64_t cap = (total + warps * cpw - 1) / (warps * cpw);
     cap = std::min<int64_t>(std::max<int64_t>(kTileItems + R + 1, cap), 1 << 24);
     const int64_t ideal = std::max<int64_t>(1, (total + cap - 1) / cap);
     int4* d_cut = tmp.get<int4>((size_t)ideal + 1, &rc);

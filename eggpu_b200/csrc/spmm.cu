@@ -862,8 +862,10 @@ int spmm_grid(bool f64) {
     return c;
 }
 
-// Entries per chunk (a multiple of 32).
-int32_t chunk_entries() {
+}  // namespace
+
+// Default entries per chunk (a multiple of 32).
+int32_t default_spmm_chunk() {
     static const int32_t v = [] {
         const char* e = std::getenv("EGPR_SPMM_CHUNK");
         const int x = e ? std::atoi(e) : 1024;
@@ -871,8 +873,6 @@ int32_t chunk_entries() {
     }();
     return v;
 }
-
-}  // namespace
 
 // Per-graph SpMM workspace: the layout (entry stream and chunks, built on the
 // first batched solve) and the solve buffers, grown to the largest group of
@@ -911,7 +911,7 @@ int grid_1d(int64_t work) {
 
 int build_spmm_layout(egpr_graph* g, SpmmWork& w, cudaStream_t s) {
     const int32_t n = g->n;
-    const int32_t C = chunk_entries();
+    const int32_t C = std::max(64, g->tune_spmm_chunk & ~31);
     if (g->sw_nnz <= 0 || g->sw_nnz > (int64_t)INT32_MAX - 2 * C) return arg_error("graph too large for the batched solve");
     const int32_t nch = (int32_t)((g->sw_nnz + C - 1) / C);
     const int64_t epad = (int64_t)nch * C;
@@ -1121,8 +1121,8 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     }
     if ((rc = cuda_ok(cudaGetLastError(), "spmm finish"))) return rc;
     if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
-    if ((rc = cuda_ok(cudaMemcpyAsync(out, w.out.p, (size_t)kg * n * sizeof(double), cudaMemcpyDeviceToHost, s),
-                      "D2H ranks")))
+    if (out && (rc = cuda_ok(cudaMemcpyAsync(out, w.out.p, (size_t)kg * n * sizeof(double), cudaMemcpyDeviceToHost, s),
+                             "D2H ranks")))  // out == NULL: device timing only (the tuner)
         return rc;
     std::vector<ColState> hc((size_t)npanels * kLanes);
     Ctl ctl;
@@ -1190,7 +1190,8 @@ int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, i
         }
     }
     if (g->nnz == 0) {  // pagerank.py:96-98: no edges -> uniform
-        for (size_t i = 0; i < (size_t)k * n; ++i) out[i] = 1.0 / n;
+        if (out)
+            for (size_t i = 0; i < (size_t)k * n; ++i) out[i] = 1.0 / n;
         if (stats)
             for (int32_t j = 0; j < k; ++j) {
                 std::memset(&stats[j], 0, sizeof(egpr_stats));
@@ -1206,7 +1207,7 @@ int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, i
     constexpr int32_t kGroup = kMaxPanels * kLanes;
     for (int32_t j0 = 0; j0 < k; j0 += kGroup) {
         const int32_t kg = std::min(kGroup, k - j0);
-        if ((rc = solve_group(g, w, alpha, max_iter, tol, j0, kg, per_col, flags, out + (size_t)j0 * n,
+        if ((rc = solve_group(g, w, alpha, max_iter, tol, j0, kg, per_col, flags, out ? out + (size_t)j0 * n : nullptr,
                               stats ? stats + j0 : nullptr)))
             return rc;
     }

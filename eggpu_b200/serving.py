@@ -180,6 +180,7 @@ class Server:
         # results land in page-locked host arrays (copied at full link speed;
         # the allocator reuses the memory once a result is dropped)
         self.pinned = bool(pinned)
+        self.pinned_max_bytes = 64 << 20
         self.max_columns = int(max_columns)
         self.multi_max_n = int(multi_max_n)
         self.fold_multi = fold_multi
@@ -264,7 +265,10 @@ class Server:
         req.future.set_result((ranks if req.keep_result else None, stats))
 
     def _out(self, shape):
-        return _native.pinned_empty(shape) if self.pinned else None
+        # page-locked up to pinned_max_bytes: pinning a fresh multi-GB block
+        # costs more than the faster copy saves
+        nbytes = 8 * int(np.prod(shape))
+        return _native.pinned_empty(shape) if self.pinned and nbytes <= self.pinned_max_bytes else None
 
     def _run(self, work):
         if len(work) > 1:

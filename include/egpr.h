@@ -133,6 +133,38 @@ EGPR_API int egpr_graph_export_inbound(const egpr_graph* g, int32_t* in_row /* n
  */
 EGPR_API int egpr_graph_set_stream(egpr_graph* g, void* stream);
 
+/* ---- layout tuning (no counterpart in the reference) ------------------- */
+
+/*
+ * The work-layout parameters of a prepared graph.  The reference has no such
+ * layer: its PageRank kernel takes one thread per row with fixed launch
+ * shapes (pagerank.cu), so nothing there is tuned per graph.
+ */
+typedef struct egpr_tuning {
+    int32_t chunks_per_warp; /* single-vector sweep: work-queue chunks per resident warp */
+    int32_t row_cost;        /* single-vector sweep: cost of finishing a row, in entries, when cutting chunks */
+    int32_t spmm_chunk;      /* batched solve: inbound entries per work unit (the tile along the entries) */
+    int32_t configs_tried;   /* egpr_graph_autotune: layouts measured */
+    double sweep_ms;         /* egpr_graph_autotune: per-sweep device time of the chosen sweep layout */
+    double spmm_sweep_ms;    /* egpr_graph_autotune: per-sweep device time of the chosen batched layout
+                                (one 32-column panel) */
+} egpr_tuning;
+
+#define EGPR_TUNE_SWEEP 1u /* tune the single-vector sweep layout */
+#define EGPR_TUNE_SPMM 2u  /* tune the batched solve's tile */
+
+/*
+ * Measures candidate layouts on this graph (a few fixed-count sweeps each,
+ * timed on the device) and keeps the fastest: chunks_per_warp in {4, 8, 16}
+ * x row_cost in {2, 4, 8} for the sweep, spmm_chunk in {512, 1024, 2048} for
+ * the batched solve.  Results do not depend on the layout beyond FP32
+ * rounding.  out (nullable) receives the chosen parameters and timings.
+ */
+EGPR_API int egpr_graph_autotune(egpr_graph* g, uint32_t what, egpr_tuning* out);
+/* Reads / applies layout parameters (values outside their ranges are refused). */
+EGPR_API int egpr_graph_get_tuning(const egpr_graph* g, egpr_tuning* out);
+EGPR_API int egpr_graph_set_tuning(egpr_graph* g, const egpr_tuning* in);
+
 /* ---- solves ---------------------------------------------------------- */
 
 /*
