@@ -509,19 +509,31 @@ __device__ void process_unit(const SpmmParams& P, SpSmem<kF64>& S, int32_t p, in
             k0 = 1;
         }
         // the batch's rows: half-warp g takes rows k0 + g, k0 + g + 2, ...
-        for (int kk = k0; kk < nr; kk += 8) {
+        // four rows per half-warp at a time (their loads issued together) while
+        // eight or more remain, then one at a time: the cost follows the row count
+        int kk = k0;
+        for (; kk + 8 <= nr; kk += 8) {
             Real pa[4], pb[4];
             uint32_t mr[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int k = kk + 2 * i + g;
-                mr[i] = __shfl_sync(kAll, mt, k & 31);
-                if (k < nr) prev_of<kF64>(L, c2, rb + k, pa[i], pb[i]);
+                mr[i] = __shfl_sync(kAll, mt, k);
+                prev_of<kF64>(L, c2, rb + k, pa[i], pb[i]);
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int k = kk + 2 * i + g;
-                if (k < nr) row_out<kF64>(P, L, c2, rb + k, rows[k][c2], rows[k][c2 + 1], pa[i], pb[i], mr[i], A);
+                row_out<kF64>(P, L, c2, rb + k, rows[k][c2], rows[k][c2 + 1], pa[i], pb[i], mr[i], A);
+            }
+        }
+        for (; kk < nr; kk += 2) {
+            const int k = kk + g;
+            const uint32_t m1 = __shfl_sync(kAll, mt, k & 31);
+            if (k < nr) {
+                Real pa, pb;
+                prev_of<kF64>(L, c2, rb + k, pa, pb);
+                row_out<kF64>(P, L, c2, rb + k, rows[k][c2], rows[k][c2 + 1], pa, pb, m1, A);
             }
         }
         rb += nr;
