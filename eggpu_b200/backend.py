@@ -289,16 +289,37 @@ def _weight_of(attr, weight):
         return 1.0
 
 
+try:  # the native walk (eggpu_b200/csrc/graph_walk.cpp); same arrays as _graph_csr_py
+    from . import _graph_walk
+except ImportError:  # not built: the Python walk below gives the same result
+    _graph_walk = None
+
+
 def graph_csr(G, prepared, weight=None):
     """Out-edge CSR (V int32, E int32, W float64 or None) of G in prepared["nodes"] order.
 
     Directed graphs keep every arc (self-loops included); undirected graphs
     drop self-loops and store each pair once per direction, the rules of
     build_digraph / build_graph (cpp_easygraph/classes/graph_convert.cpp:72-134).
-    Rows are sorted by destination index as gen_CSR does.
+    Rows are sorted by destination index as gen_CSR does.  The walk over the
+    adjacency dicts runs in native code when the extension is built.
     """
     if is_bulk_graph(G):
         return G.csr_arrays(weight)
+    if _graph_walk is not None:
+        adj = _adj_dict(G)
+        index = prepared["node_to_idx"]
+        if isinstance(adj, dict) and isinstance(index, dict):
+            res = _graph_walk.out_csr(adj, index, len(prepared["nodes"]), bool(prepared["directed"]), weight)
+            if res is not None:
+                V, E, W = res
+                return (np.frombuffer(V, dtype=np.int32), np.frombuffer(E, dtype=np.int32),
+                        None if W is None else np.frombuffer(W, dtype=np.float64))
+    return _graph_csr_py(G, prepared, weight)
+
+
+def _graph_csr_py(G, prepared, weight=None):
+    """graph_csr's walk in Python (the specification of the native walk)."""
     index = prepared["node_to_idx"]
     n = len(prepared["nodes"])
     if n >= 2**31 - 1:

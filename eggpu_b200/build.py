@@ -2,6 +2,7 @@
 
 * ``libegpr.so``       the CUDA engine (sm_100a) behind the C ABI in include/egpr.h
 * ``libegpr_synth.so`` the seeded synthetic graph generators (host C++/OpenMP)
+* ``_graph_walk*.so``  Python graph -> out-edge CSR (CPython extension, host C++)
 
 Run ``python -m eggpu_b200.build`` (or call :func:`build`).  Objects go to
 ``eggpu_b200/_build/``; a library is rebuilt when any of its sources or headers
@@ -83,9 +84,23 @@ def build_synth(verbose: bool = False) -> Path:
     return SYNTH
 
 
+def build_graph_walk(verbose: bool = False) -> Path:
+    """The CPython extension that turns a Python graph's adjacency into the out-edge CSR."""
+    import sysconfig
+
+    src = CSRC / "graph_walk.cpp"
+    out = PKG / ("_graph_walk" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if _newer(out, [src]):
+        inc = sysconfig.get_paths()["include"]
+        _run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden", f"-I{inc}", src, "-o", out],
+             verbose)
+    return out
+
+
 def build(verbose: bool = False) -> None:
     build_engine(verbose)
     build_synth(verbose)
+    build_graph_walk(verbose)
 
 
 if __name__ == "__main__":

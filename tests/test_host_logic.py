@@ -76,6 +76,37 @@ def test_graph_csr_matches_restated_gen_csr(case):
         assert np.array_equal(W, W2)
 
 
+@pytest.mark.skipif(backend._graph_walk is None, reason="native graph walk not built")
+@pytest.mark.parametrize("directed", [True, False])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_native_graph_walk_equals_the_python_walk(directed, weighted):
+    rng = np.random.default_rng(7 + 2 * directed + weighted)
+    n = 1500
+    nodes = [("v", int(i)) for i in rng.permutation(n)]
+    adj = {u: {} for u in nodes}
+    for _ in range(12000):
+        a, b = rng.integers(0, n, 2)
+        r = rng.random()
+        # odd attributes: missing, None, numeric strings, junk strings, empty dicts
+        attr = ({} if r > 0.95 else {"w": None} if r > 0.9 else {"w": str(r)} if r < 0.1 else
+                {"w": "x"} if r < 0.12 else {"w": r, "other": 1})
+        adj[nodes[a]][nodes[b]] = attr
+        if not directed:
+            adj[nodes[b]][nodes[a]] = attr
+    G = types.SimpleNamespace(_adj=adj)
+    prepared = {"node_to_idx": {u: i for i, u in enumerate(nodes)}, "nodes": nodes, "directed": directed}
+    w = "w" if weighted else None
+    V, E, W = backend.graph_csr(G, prepared, w)
+    V2, E2, W2 = backend._graph_csr_py(G, prepared, w)
+    assert V.dtype == V2.dtype == np.int32 and E.dtype == E2.dtype == np.int32
+    assert np.array_equal(V, V2) and np.array_equal(E, E2)
+    assert (W is None and W2 is None) or np.array_equal(W, W2)
+    # a neighbour missing from the node index fails the same way
+    adj[nodes[0]][("v", -1)] = {}
+    with pytest.raises(KeyError):
+        backend.graph_csr(G, prepared, w)
+
+
 def test_prepared_context_reuse_and_mutation_invalidation():
     G = DiGraph()
     G.add_edge(0, 1, weight=8.0)
