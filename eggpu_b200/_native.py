@@ -374,13 +374,20 @@ def pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6, correction=True):
     return outs, [s.as_dict() for s in sts]
 
 
-def pagerank_csr(V, E, W, graph_id, alpha, max_iter, threshold):
-    """Drop-in for gpu_easygraph::pagerank: returns (PR float64[n], kernel_seconds)."""
+def pagerank_csr(V, E, W, graph_id, alpha, max_iter, threshold, out=None):
+    """Drop-in for gpu_easygraph::pagerank: returns (PR float64[n], kernel_seconds).
+    out: optional caller-owned float64[n] result (page-locked memory copies back faster)."""
     V = _i32(V)
     E = _i32(E)
     W = None if W is None or len(W) == 0 else _f64(W)
     n = int(V.shape[0]) - 1
-    PR = np.empty(max(n, 0), np.float64)
+    if out is None:
+        PR = np.empty(max(n, 0), np.float64)
+    else:
+        if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (max(n, 0),)
+                or not out.flags.c_contiguous or not out.flags.writeable):
+            raise ValueError(f"out must be a writeable contiguous float64 array of {max(n, 0)} entries")
+        PR = out
     ks = c_double(0.0)
     check(lib.egpr_pagerank_csr(_ptr(V), int(V.shape[0]), _ptr(E), int(E.shape[0]), _ptr(W), int(graph_id) & (2**64 - 1),
                                 float(alpha), int(max_iter), float(threshold), _ptr(PR), ctypes.byref(ks)),

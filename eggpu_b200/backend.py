@@ -392,8 +392,20 @@ def cpp_gpu_pagerank_dense(csr, alpha, max_iterator, threshold, weight=None, per
 
     pg = csr if isinstance(csr, PreparedGraph) else PreparedGraph(*csr)
     ranks, stats = pg.pagerank(alpha=float(alpha), max_iter=int(max_iterator), tol=float(threshold),
-                               personalization=personalization)
+                               personalization=personalization, out=_result_vector(pg.n))
     return {"values_dense": ranks, "kernel_seconds": stats["kernel_seconds"], "stats": stats}
+
+
+_PINNED_RESULT_MAX = 256 << 20
+
+
+def _result_vector(n):
+    """The array the ranks are copied into, which the result Mapping then
+    wraps without a copy: page-locked (faster copy; the allocator reuses it
+    once the result is dropped) up to 256 MiB."""
+    from ._native import pinned_empty
+
+    return pinned_empty(n) if 8 * n <= _PINNED_RESULT_MAX else None
 
 
 def _personalization_vector(personalization, prepared):
