@@ -579,8 +579,15 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
     if (!V) return fail_arg("V is NULL");
     if (m > 0 && !E) return fail_arg("E is NULL");
     if (V[0] != 0 || (int64_t)V[n] != m) return fail_arg("CSR offsets must start at 0 and end at m");
-    for (int32_t i = 0; i < n; ++i)
-        if (V[i + 1] < V[i]) return fail_arg("CSR offsets must be non-decreasing");
+    {
+        // branch-free over blocks of 4096 (the compiler vectorises it), checked per block
+        int bad = 0;
+        for (int32_t b = 0; b < n && !bad; b += 4096) {
+            const int32_t e = std::min(n, b + 4096);
+            for (int32_t i = b; i < e; ++i) bad |= V[i + 1] < V[i];
+        }
+        if (bad) return fail_arg("CSR offsets must be non-decreasing");
+    }
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaGetDevice");

@@ -37,8 +37,6 @@ namespace {
 
 constexpr int kScanPerThread = 8;
 constexpr int kScanTile = kThreads * kScanPerThread;
-constexpr int kRadixBits = 8;
-constexpr int kDigits = 1 << kRadixBits;
 constexpr int kSortPerLane = 16;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSortTile = kThreads * kSortPerLane;
@@ -100,34 +98,42 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, int64_t len, const uint32
 }
 
 // -------------------------------------------------------------- radix ------
+// LSD radix sort of (key, value) pairs with digits of kBits bits (8 to 11):
+// a key of B bits takes ceil(B / 11) passes of equal digits.
+template <int kBits>
 __global__ void __launch_bounds__(kThreads)
 k_radix_hist(const uint32_t* __restrict__ keys, int64_t len, int shift, int64_t ntiles,
              uint32_t* __restrict__ hist) {
-    __shared__ uint32_t h[kDigits];
-    for (int d = threadIdx.x; d < kDigits; d += kThreads) h[d] = 0;
+    constexpr int kD = 1 << kBits;
+    __shared__ uint32_t h[kD];
+    for (int d = threadIdx.x; d < kD; d += kThreads) h[d] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSortTile;
     for (int i = threadIdx.x; i < kSortTile; i += kThreads) {
         int64_t idx = base + i;
-        if (idx < len) atomicAdd(&h[(keys[idx] >> shift) & (kDigits - 1)], 1u);
+        if (idx < len) atomicAdd(&h[(keys[idx] >> shift) & (kD - 1)], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < kDigits; d += kThreads) hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
+    for (int d = threadIdx.x; d < kD; d += kThreads) hist[(int64_t)d * ntiles + blockIdx.x] = h[d];
 }
 
 // Stable scatter: within a tile, warp w owns items [w*32*kSortPerLane, ...) in
 // order; inside a warp, rounds of 32 consecutive items rank equal digits by
 // lane order.  Global order = tile order (digit-major scanned histogram),
-// then warp order, then item order.
+// then warp order, then item order.  keys_out may be NULL (last pass: only
+// the values are needed).
+template <int kBits>
 __global__ void __launch_bounds__(kThreads)
 k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t len,
                 int shift, int64_t ntiles, const uint32_t* __restrict__ offsets) {
-    __shared__ uint32_t warp_hist[kWarps][kDigits];
-    __shared__ uint32_t tile_off[kDigits];
+    constexpr int kD = 1 << kBits;
+    extern __shared__ uint32_t radix_smem[];
+    uint32_t (*warp_hist)[kD] = reinterpret_cast<uint32_t (*)[kD]>(radix_smem);  // [kWarps][kD]
+    uint32_t* tile_off = radix_smem + kWarps * kD;                               // [kD]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < kWarps * kDigits; i += kThreads) (&warp_hist[0][0])[i] = 0;
-    for (int d = tid; d < kDigits; d += kThreads) tile_off[d] = offsets[(int64_t)d * ntiles + blockIdx.x];
+    for (int i = tid; i < kWarps * kD; i += kThreads) radix_smem[i] = 0;
+    for (int d = tid; d < kD; d += kThreads) tile_off[d] = offsets[(int64_t)d * ntiles + blockIdx.x];
     __syncthreads();
     const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortPerLane;
     uint32_t key[kSortPerLane], val[kSortPerLane], rank[kSortPerLane];
@@ -138,8 +144,8 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         const bool valid = idx < len;
         key[r] = valid ? keys_in[idx] : 0u;
         val[r] = valid ? vals_in[idx] : 0u;
-        const uint32_t d = (key[r] >> shift) & (kDigits - 1);
-        const uint32_t tag = valid ? d : (uint32_t)(kDigits + lane);
+        const uint32_t d = (key[r] >> shift) & (kD - 1);
+        const uint32_t tag = valid ? d : (uint32_t)(kD + lane);
         const uint32_t peers = __match_any_sync(0xffffffffu, tag);
         const uint32_t before = valid ? warp_hist[warp][d] : 0u;
         __syncwarp();
@@ -148,7 +154,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         rank[r] = before + __popc(peers & lt_mask);
     }
     __syncthreads();
-    for (int d = tid; d < kDigits; d += kThreads) {
+    for (int d = tid; d < kD; d += kThreads) {
         uint32_t run = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
@@ -162,9 +168,9 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
     for (int r = 0; r < kSortPerLane; ++r) {
         const int64_t idx = wbase + (int64_t)r * 32 + lane;
         if (idx < len) {
-            const uint32_t d = (key[r] >> shift) & (kDigits - 1);
+            const uint32_t d = (key[r] >> shift) & (kD - 1);
             const uint32_t dst = tile_off[d] + warp_hist[warp][d] + rank[r];
-            keys_out[dst] = key[r];
+            if (keys_out) keys_out[dst] = key[r];
             vals_out[dst] = val[r];
         }
     }
@@ -392,24 +398,53 @@ struct TmpAlloc {
     }
 };
 
+template <int kBits>
+int radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t len, int shift,
+               bool last, int64_t ntiles, uint32_t* hist, cudaStream_t s) {
+    constexpr int kD = 1 << kBits;
+    const size_t smem = (size_t)(kWarps + 1) * kD * sizeof(uint32_t);
+    static bool attr_set = false;  // per process; the attribute is per function and harmless to repeat
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_radix_scatter<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    k_radix_hist<kBits><<<(unsigned)ntiles, kThreads, 0, s>>>(kin, len, shift, ntiles, hist);
+    int rc = exclusive_scan_u32(hist, hist, ntiles * kD, s);
+    if (rc) return rc;
+    k_radix_scatter<kBits><<<(unsigned)ntiles, kThreads, smem, s>>>(kin, vin, last ? nullptr : kout, vout, len, shift,
+                                                                    ntiles, hist);
+    return EGPR_SUCC;
+}
+
+// Sorts (keys, vals) by the low `bits` bits of the keys, stable.  After the
+// call the values are in the buffer *result_in_alt names; the keys are sorted
+// alongside except in the last pass, which writes values only.
 int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
-                     int64_t len, int bits, cudaStream_t s, TmpAlloc& tmp, bool* result_in_alt) {
+                     int64_t len, int bits, cudaStream_t s, TmpAlloc& tmp, bool* result_in_alt,
+                     bool keys_needed = true) {
     *result_in_alt = false;
     if (len <= 1 || bits <= 0) return EGPR_SUCC;
     int rc = EGPR_SUCC;
+    const int passes = (bits + 10) / 11;
+    const int dbits = std::max(8, (bits + passes - 1) / passes);
     const int64_t ntiles = (len + kSortTile - 1) / kSortTile;
-    uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles * kDigits, &rc);
+    uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles << dbits, &rc);
     if (!hist) return rc;
     uint32_t *kin = keys, *vin = vals, *kout = keys_alt, *vout = vals_alt;
-    for (int shift = 0; shift < bits; shift += kRadixBits) {
-        k_radix_hist<<<(unsigned)ntiles, kThreads, 0, s>>>(kin, len, shift, ntiles, hist);
-        rc = exclusive_scan_u32(hist, hist, ntiles * kDigits, s);
+    for (int p = 0; p < passes; ++p) {
+        const int shift = p * dbits;
+        const bool last = p == passes - 1 && !keys_needed;
+        switch (dbits) {
+            case 8: rc = radix_pass<8>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
+            case 9: rc = radix_pass<9>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
+            case 10: rc = radix_pass<10>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
+            default: rc = radix_pass<11>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
+        }
         if (rc) return rc;
-        k_radix_scatter<<<(unsigned)ntiles, kThreads, 0, s>>>(kin, vin, kout, vout, len, shift, ntiles, hist);
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
-    *result_in_alt = (kin == keys_alt);
+    *result_in_alt = (vin == vals_alt);
     return cuda_ok(cudaGetLastError(), "radix sort");
 }
 
@@ -713,10 +748,22 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
             else if (k.flags & kHasHead) hparts[(size_t)c] = c - k.head_ta + 1;
             if ((k.flags & kHasTail) && !(k.flags & kInterior)) tparts[(size_t)c] = k.tail_tb - c + 1;
         }
+        // costliest first: a stable counting sort over 4096 cost classes (the
+        // order only needs to be roughly by cost, and a comparison sort of the
+        // ~28K records costs milliseconds of host time)
         std::vector<int32_t> perm((size_t)nch), pos_of((size_t)nch);
-        for (int32_t c = 0; c < nch; ++c) perm[(size_t)c] = c;
-        std::stable_sort(perm.begin(), perm.end(),
-                         [&](int32_t a, int32_t b) { return ch[(size_t)a].pad > ch[(size_t)b].pad; });
+        {
+            int64_t cmax = 1;
+            for (int32_t c = 0; c < nch; ++c) cmax = std::max<int64_t>(cmax, ch[(size_t)c].pad);
+            constexpr int kClasses = 4096;
+            std::vector<int32_t> start(kClasses + 1, 0);
+            auto cls = [&](int32_t c) {
+                return kClasses - 1 - (int32_t)(((int64_t)ch[(size_t)c].pad * (kClasses - 1)) / cmax);
+            };
+            for (int32_t c = 0; c < nch; ++c) start[(size_t)cls(c) + 1] += 1;
+            for (int i = 0; i < kClasses; ++i) start[(size_t)i + 1] += start[(size_t)i];
+            for (int32_t c = 0; c < nch; ++c) perm[(size_t)start[(size_t)cls(c)]++] = c;
+        }
         for (int32_t i = 0; i < nch; ++i) pos_of[(size_t)perm[(size_t)i]] = i;
         std::vector<Chunk> sorted((size_t)nch);
         for (int32_t i = 0; i < nch; ++i) {
@@ -877,7 +924,7 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             return rc;
         if (g->nhub > 0) {
             bool alt = false;
-            if ((rc = radix_sort_pairs(hkey, hval, hkey2, hval2, n, 32, s, tmp, &alt))) return rc;
+            if ((rc = radix_sort_pairs(hkey, hval, hkey2, hval2, n, 32, s, tmp, &alt, false))) return rc;
             k_hub_slots<<<grid_for(g->nhub), kThreads, 0, s>>>(alt ? hval2 : hval, g->nhub, g->hub_ids.as<int32_t>(),
                                                                g->hub_slot.as<int32_t>());
             if (nnz > 0)
