@@ -325,6 +325,12 @@ def run_ppr(args):
     g = synth.rmat(scale=20, edgefactor=16, seed=3)
     sets = synth.seed_sets(g.n, 256, 1, 64, seed=3)
     pg = _native.PreparedGraph(g.V, g.E)
+    if args.ppr_profile:  # a short case for a profiler: warm-up solve, then the profiled one
+        k = int(args.ppr_profile)
+        for _ in range(2):
+            _, sts = pg.pagerank_seeds(sets[:k], alpha=0.85, max_iter=4, tol=0.0)
+        print(json.dumps({"ppr_profile": {"k": k, "sweeps": 4, "device_ms": sts[0]["kernel_seconds"] * 1e3}}))
+        return
     out = {}
     res = _native.pinned_empty((len(sets), g.n))  # the result array a serving caller keeps and reuses
     for label, max_iter, tol in (("rule", 100, 1e-6), ("fixed20", 20, 0.0)):
@@ -535,6 +541,8 @@ def main():
     ap.add_argument("--serving-max-n", type=float, default=1e7)
     ap.add_argument("--serving-requests", type=int, default=10000)
     ap.add_argument("--serving-hbm-gb", type=float, default=64.0)
+    ap.add_argument("--ppr-profile", type=int, default=0, metavar="K",
+                    help="ppr workload: only two batched solves of K columns and 4 sweeps (a case for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -902,8 +902,11 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         if (W && (rc = g->in_w.alloc((size_t)std::max<int64_t>(nnz, 1) * sizeof(float) + pad)))
             return rc;
         if (m > 0) {
+            // keys are destinations in [0, n), and n for an out-of-range one:
+            // the key width covers n only when such an entry exists
+            const uint64_t kmax = nnz < m ? (uint64_t)n : (uint64_t)n - 1;
             int bits = 0;
-            while (bits < 32 && ((uint64_t)n >> bits) != 0) ++bits;
+            while (bits < 32 && (kmax >> bits) != 0) ++bits;
             bool alt = false;
             if ((rc = radix_sort_pairs(keys, vals, keys2, vals2, m, bits, s, tmp, &alt))) return rc;
             const uint32_t* sorted_ids = alt ? vals2 : vals;
