@@ -372,3 +372,36 @@ def test_ppr_through_the_api_batch():
     for r, p in zip(res, ([1, 0, 0, 0], [0, 0.5, 0, 0.5])):
         ref, _, _ = oracle.pagerank_push(V, E, None, teleport=np.array(p, float))
         assert np.allclose(r.to_numpy(), ref, rtol=2e-5, atol=1e-7)
+
+
+def test_ppr_config_full_size_k256_rmat20():
+    # configs[4a]: R-MAT scale 20, seed 3, k = 256 seed sets of 1-64 vertices, at full size
+    g = synth.rmat(scale=20, edgefactor=16, seed=3)
+    sets = synth.seed_sets(g.n, 256, 1, 64, seed=3)
+    pg = _native.PreparedGraph(g.V, g.E)
+    for max_iter, tol in ((100, 1e-6), (20, 0.0)):
+        ranks, stats = pg.pagerank_seeds(sets, alpha=0.85, max_iter=max_iter, tol=tol)
+        assert ranks.shape == (256, g.n) and ranks.min() >= 0.0
+        assert np.abs(ranks.sum(axis=1) - 1.0).max() <= 1e-12
+        again, _ = pg.pagerank_seeds(sets, alpha=0.85, max_iter=max_iter, tol=tol)
+        assert np.array_equal(ranks, again)
+        for j in (0, 127, 255):
+            _check_against_oracle(g.V, g.E, None, ranks[j], stats[j], 0.85, max_iter, tol,
+                                  teleport=_seed_teleport(g.n, sets[j]))
+
+
+def test_many_graphs_config_full_size_512_er():
+    # configs[4b]: 512 directed Erdos-Renyi graphs (n log-uniform in [1e3, 2e5], mean out-degree U[8, 32])
+    rng = np.random.Generator(np.random.PCG64(1000))
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(2e5), size=512)).astype(np.int64)
+    ds = rng.uniform(8.0, 32.0, size=512)
+    csrs = [synth.erdos_renyi(int(ns[i]), float(ds[i]), seed=1000 + i) for i in range(512)]
+    graphs = [_native.PreparedGraph(c.V, c.E) for c in csrs]
+    outs, sts = _native.pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6)
+    for o in outs:
+        assert o.min() >= 0.0 and abs(o.sum() - 1.0) <= 1e-12
+    for i in (0, 1, 255, 510, 511):
+        c = csrs[i]
+        _check_against_oracle(c.V, c.E, None, outs[i], sts[i], 0.85, 100, 1e-6)
+        single, st = graphs[i].pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+        assert st["iterations"] == sts[i]["iterations"] and np.abs(single - outs[i]).sum() <= L1_TOL
