@@ -445,7 +445,7 @@ static uint64_t bits_of(double x) {
 }  // namespace egpr
 
 int64_t egpr_graph::device_bytes() const {
-    return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes + sub_coord.bytes +
+    return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes +
                      sw_row.bytes + sw_col.bytes + sw_w.bytes + tile_bits.bytes + tile_row.bytes +
                      hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_acc.bytes + plan.d_span_acc.bytes + plan.d_span_cnt.bytes +
                      plan.d_span_list.bytes +
@@ -465,7 +465,7 @@ static void destroy_graph_object(egpr_graph* g) {
     if (g->own_stream) cudaStreamSynchronize(g->own_stream);
     spmm_work_release(g);
     g->plan.release();
-    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sub_coord, &g->sw_row,
+    for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sw_row,
                       &g->sw_col, &g->sw_w, &g->tile_bits, &g->tile_row,
                       &g->hub_ids, &g->hub_slot, &g->hubz, &g->scale, &g->tele,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})

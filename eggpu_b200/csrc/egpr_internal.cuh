@@ -13,19 +13,16 @@
 namespace egpr {
 
 // ---------------------------------------------------------------------------
-// Work decomposition.
+// Work decomposition of the single-vector sweep.
 //
-// A graph's merge path has n + nnz items (one "row end" per vertex plus one
-// item per inbound entry).  It is cut into sub-tiles of kSubItems items; a
-// CTA processes one sub-tile at a time entirely in shared memory.  Runs of
-// consecutive sub-tiles form chunks, the unit of the persistent work queue.
-// A row cut by a chunk boundary is a "span": each chunk it touches leaves a
-// partial sum, and the last of them to finish combines the partials in
-// chunk order (no waiting, deterministic).
+// The sweep reads the inbound CSR with one placeholder entry in every empty
+// row, in warp tiles of kTileItems entries.  Runs of tiles form chunks, cut at
+// equal cost (entries plus a weight per row), the unit of the persistent work
+// queue.  A row cut by a chunk boundary is a "span": each chunk it touches
+// adds its piece, and the last of them to arrive finishes the row (no
+// waiting; the pieces are exact fixed point, so the order does not matter).
 // ---------------------------------------------------------------------------
-constexpr int kThreads = 256;
-constexpr int kItemsPerThread = 8;
-constexpr int kSubItems = kThreads * kItemsPerThread;
+constexpr int kThreads = 256;  // threads of the preparation and helper kernels
 
 // Chunk flags.
 constexpr int32_t kHasHead = 1;    // the chunk's first row began in an earlier chunk
@@ -33,8 +30,8 @@ constexpr int32_t kHasTail = 2;    // the chunk's last row continues into a late
 constexpr int32_t kInterior = 4;   // the chunk lies inside one row (head and tail are that row)
 
 struct Chunk {
-    int32_t sub_begin;   // SpMM: first sub-tile; sweep stage: first row touched
-    int32_t sub_end;     // SpMM: one past the last sub-tile; sweep stage: one past the last row touched
+    int32_t tile_begin;  // first warp tile of the chunk
+    int32_t tile_end;    // one past its last warp tile
     int32_t graph;       // slot in the plan's graph table
     int32_t flags;
     int32_t head_ta;     // global chunk id where the head row's span starts
@@ -192,10 +189,8 @@ struct egpr_graph {
     int32_t n_dangling = 0;        // out-weight <= 0 (reference mask)
     int32_t n_dangling_solve = 0;  // out-weight <= 1e-15 (EasyGraph CPU rule)
     double prep_seconds = 0.0;
-    int32_t nsub = 0;              // SpMM merge-path sub-tiles
-    int32_t chunk_subs = 1;        // sub-tiles per SpMM chunk
     // prepared graph
-    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, sub_coord, hub_ids, hub_slot, hubz;
+    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, hub_ids, hub_slot, hubz;
     // the sweep's layout (see build_sweep_layout)
     egpr::DevBuf sw_row, sw_col, sw_w, tile_bits, tile_row;
     int64_t sw_nnz = 0;
@@ -235,7 +230,6 @@ double wall_seconds();
 
 // Preparation (prep.cu).
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W);
-int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& out, cudaStream_t s);
 int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* sorted_dst, cudaStream_t s);
 int default_chunks_per_warp();  // EGPR_CHUNKS_PER_WARP, else 8
 int default_row_cost();         // EGPR_ROW_COST, else 4

@@ -15,7 +15,6 @@
 //   k_gather_inbound in_col / in_w from the sorted entry ids
 //   k_dangling       dangling mask outw <= 0 (:323-326) and the counts used by
 //                    the solver
-//   k_sub_coord      merge-path coordinates of every sub-tile start
 //
 // The results are bit-identical to build_inbound_from_csr for in_row, in_col,
 // the dangling mask and the FP64 out-weight sums.  The engine stores raw
@@ -335,30 +334,6 @@ __device__ __forceinline__ int2 merge_search(const int32_t* __restrict__ in_row,
         else hi = mid;
     }
     return make_int2((int32_t)lo, (int32_t)(d - lo));
-}
-
-__global__ void k_sub_coord(const int32_t* __restrict__ in_row, int32_t n, int64_t nnz, int32_t nsub,
-                            int2* __restrict__ coord) {
-    const int64_t total = (int64_t)n + nnz;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s <= nsub;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        int64_t d = s * (int64_t)kSubItems;
-        if (d > total) d = total;
-        coord[s] = merge_search(in_row, n, nnz, d);
-    }
-}
-
-// (row, entry, in_row[row]) at each chunk boundary, for the host-side span table.
-__global__ void k_chunk_bounds(const int2* __restrict__ coord, const int32_t* __restrict__ in_row,
-                               int32_t nsub, int32_t chunk_subs, int32_t nchunks, int32_t n,
-                               int4* __restrict__ out) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= nchunks; c += gridDim.x * blockDim.x) {
-        int s = c * chunk_subs;
-        if (s > nsub) s = nsub;
-        const int2 rc = coord[s];
-        const int32_t start = rc.x < n ? in_row[rc.x] : in_row[n];
-        out[c] = make_int4(rc.x, rc.y, start, 0);
-    }
 }
 
 inline int grid_for(int64_t work, int per_block = kThreads) {
@@ -696,8 +671,8 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
         if (tail) f |= kHasTail;
         if (head && tail && a.r == b.r) f |= kInterior;
         k.flags = f;
-        k.sub_begin = (int32_t)ntiles;
-        k.sub_end = (int32_t)(ntiles + nt);
+        k.tile_begin = (int32_t)ntiles;
+        k.tile_end = (int32_t)(ntiles + nt);
         k.nnz_begin = a.k;
         k.nnz_end = b.k;
         k.row_end = b.r;
@@ -802,50 +777,6 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
     return cuda_ok(cudaStreamSynchronize(s), "sweep layout");
 }
 
-// Chunk table over a graph's sub-tiles: runs of chunk_subs sub-tiles, with the
-// span links of rows cut by chunk boundaries (chunk ids local to the graph).
-int build_chunk_table(egpr_graph* g, int32_t chunk_subs, std::vector<Chunk>& ch, cudaStream_t s) {
-    const int32_t n = g->n;
-    const int32_t nch = (g->nsub + chunk_subs - 1) / chunk_subs;
-    int4* bounds = nullptr;
-    int rc = cuda_ok(cudaMallocAsync(&bounds, ((size_t)nch + 1) * sizeof(int4), s), "cudaMallocAsync (chunks)");
-    if (rc) return rc;
-    k_chunk_bounds<<<grid_for((int64_t)nch + 1), kThreads, 0, s>>>(g->sub_coord.as<int2>(), g->in_row.as<int32_t>(),
-                                                                  g->nsub, chunk_subs, nch, n, bounds);
-    std::vector<int4> hb((size_t)nch + 1);
-    rc = cuda_ok(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int4), cudaMemcpyDeviceToHost, s), "D2H chunk bounds");
-    cudaFreeAsync(bounds, s);
-    if (rc || (rc = cuda_ok(cudaStreamSynchronize(s), "chunk table"))) return rc;
-    ch.assign((size_t)nch, Chunk{});
-    for (int32_t c = 0; c < nch; ++c) {
-        Chunk& k = ch[(size_t)c];
-        k.sub_begin = c * chunk_subs;
-        k.sub_end = std::min(g->nsub, (c + 1) * chunk_subs);
-        k.graph = 0;
-        const int4 a = hb[(size_t)c], b = hb[(size_t)c + 1];
-        const bool head = a.y > a.z;             // first row began earlier
-        const bool tail = b.x < n && b.y > b.z;  // last row continues
-        int32_t f = 0;
-        if (head) f |= kHasHead;
-        if (tail) f |= kHasTail;
-        if (head && tail && a.x == b.x) f |= kInterior;
-        k.flags = f;
-        k.tail_row = tail ? b.x : -1;
-        k.head_ta = -1;
-        k.tail_tb = -1;
-        k.pad2 = 0;
-    }
-    for (int32_t c = 0; c < nch; ++c) {
-        Chunk& k = ch[(size_t)c];
-        if (k.flags & kHasHead) k.head_ta = (ch[(size_t)c - 1].flags & kInterior) ? ch[(size_t)c - 1].head_ta : c - 1;
-    }
-    for (int32_t c = nch - 1; c >= 0; --c) {
-        Chunk& k = ch[(size_t)c];
-        if (k.flags & kHasTail) k.tail_tb = (ch[(size_t)c + 1].flags & kInterior) ? ch[(size_t)c + 1].tail_tb : c + 1;
-    }
-    return EGPR_SUCC;
-}
-
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W) {
     const int32_t n = g->n;
     const int64_t m = g->m_input;
@@ -942,13 +873,6 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         unsigned long long hc[2] = {0, 0};
         if ((rc = cuda_ok(cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s), "D2H counts")))
             return rc;
-        // merge-path sub-tiles and chunks
-        const int64_t total = (int64_t)n + nnz;
-        g->nsub = (int32_t)((total + kSubItems - 1) / kSubItems);
-        if (g->nsub < 1) g->nsub = 1;
-        if ((rc = g->sub_coord.alloc(((size_t)g->nsub + 1) * sizeof(int2)))) return rc;
-        k_sub_coord<<<grid_for((int64_t)g->nsub + 1), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, nnz, g->nsub,
-                                                                       g->sub_coord.as<int2>());
         g->n_dangling = (int32_t)hc[0];
         g->n_dangling_solve = (int32_t)hc[1];
         if ((rc = build_sweep_layout(g, sweep_resident_warps(), sorted_dst, s))) return rc;

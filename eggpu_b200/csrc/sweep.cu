@@ -352,14 +352,14 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
     int4 ca, cb;
     uint32_t bits, below;
     int32_t row;
-    fetch_tile(cols, tbits, trows, ck.sub_begin, T0, lane, ca, cb, bits, below, row);
-    for (int32_t t = ck.sub_begin; t < ck.sub_end; ++t) {
-        const int32_t T = T0 + (t - ck.sub_begin) * kTileItems;
+    fetch_tile(cols, tbits, trows, ck.tile_begin, T0, lane, ca, cb, bits, below, row);
+    for (int32_t t = ck.tile_begin; t < ck.tile_end; ++t) {
+        const int32_t T = T0 + (t - ck.tile_begin) * kTileItems;
         const int32_t cc[kLaneItems] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
         const uint32_t mb = bits;
         const int32_t pre = (int32_t)below;
         const int32_t r0 = row;
-        if (t + 1 < ck.sub_end) fetch_tile(cols, tbits, trows, t + 1, T + kTileItems, lane, ca, cb, bits, below, row);
+        if (t + 1 < ck.tile_end) fetch_tile(cols, tbits, trows, t + 1, T + kTileItems, lane, ca, cb, bits, below, row);
         // 1. gathers of this tile's entries (only a chunk's first and last
         //    tiles hold entries of other chunks)
         const int32_t p0 = T + kLaneItems * lane;
