@@ -326,8 +326,36 @@ static int upload_teleport(egpr_graph* g, const double* p, cudaStream_t s, std::
     return cuda_ok(cudaStreamSynchronize(s), "H2D teleport");
 }
 
+// Seed-set teleport on the device: g->tele = 0, then 1/|S| at the seeds
+// (sorted, duplicates removed, checked to lie in [0, n)).
+__global__ void k_tele_seeds(float* __restrict__ tele, int32_t n, const int32_t* __restrict__ ids, int32_t count) {
+    const float val = 1.0f / (float)count;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) tele[ids[i]] = val;
+}
+
+static int upload_teleport_seeds(egpr_graph* g, const int32_t* seeds, int32_t count, cudaStream_t s) {
+    std::vector<int32_t> sv(seeds, seeds + count);
+    std::sort(sv.begin(), sv.end());
+    sv.erase(std::unique(sv.begin(), sv.end()), sv.end());
+    if (sv.empty() || sv.front() < 0 || sv.back() >= g->n) return fail_arg("seed ids must lie in [0, n)");
+    int rc = g->seed_ids.grow_on(sv.size() * sizeof(int32_t), s);  // the graph's own buffer, kept
+    if (rc) return rc;
+    rc = cuda_ok(cudaMemcpyAsync(g->seed_ids.p, sv.data(), sv.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s),
+                 "H2D seeds");
+    if (!rc) rc = cuda_ok(cudaMemsetAsync(g->tele.p, 0, (size_t)g->n * sizeof(float), s), "memset");
+    if (!rc) {
+        k_tele_seeds<<<(unsigned)std::min<size_t>((sv.size() + 255) / 256, 1024), 256, 0, s>>>(
+            g->tele.as<float>(), g->n, g->seed_ids.as<int32_t>(), (int32_t)sv.size());
+        rc = cuda_ok(cudaGetLastError(), "seed teleport");
+    }
+    if (rc) return rc;
+    return cuda_ok(cudaStreamSynchronize(s), "seed teleport");  // sv is freed on return
+}
+
+// One single-vector solve; the teleport is the uniform vector, a dense host
+// vector (pers) or one already on the device (tele_on_device).
 static int solve_single(egpr_graph* g, double alpha, int32_t max_iter, double tol, const double* pers,
-                        uint32_t flags, double* out, egpr_stats* stats) {
+                        uint32_t flags, double* out, egpr_stats* stats, bool tele_on_device = false) {
     const double t0 = wall_seconds();
     int rc;
     if ((rc = check_device(g))) return rc;
@@ -343,7 +371,9 @@ static int solve_single(egpr_graph* g, double alpha, int32_t max_iter, double to
     if (pers && (rc = upload_teleport(g, pers, s, staging))) return rc;
     if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event"))) return rc;
     int32_t host_launches = 0;
-    if ((rc = enqueue_plan(g->plan, alpha, max_iter, tol, pers != nullptr, flags, s, &host_launches))) return rc;
+    if ((rc = enqueue_plan(g->plan, alpha, max_iter, tol, pers != nullptr || tele_on_device, flags, s,
+                           &host_launches)))
+        return rc;
     if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
     if ((rc = cuda_ok(cudaMemcpyAsync(out, g->out.p, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ranks")))
         return rc;
@@ -467,7 +497,7 @@ static void destroy_graph_object(egpr_graph* g) {
     g->plan.release();
     for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sw_row,
                       &g->sw_col, &g->sw_w, &g->tile_bits, &g->tile_row,
-                      &g->hub_ids, &g->hub_slot, &g->hubz, &g->scale, &g->tele,
+                      &g->hub_ids, &g->hub_slot, &g->hubz, &g->scale, &g->tele, &g->seed_ids,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})
         b->release();
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -836,6 +866,14 @@ int egpr_pagerank_batch(egpr_graph* g, double alpha, int32_t max_iter, double to
     if (k < 1 || !teleport || !out) return fail_arg("k >= 1, teleport and out are required");
     std::lock_guard<std::mutex> lk(g->mu);
     if (g->pending) return fail_arg("a solve is pending on this graph");
+    if (k < kSpmmMinColumns) {  // a few columns: single-vector solves cost less than a 32-column panel
+        for (int32_t j = 0; j < k; ++j) {
+            int rc = solve_single(g, alpha, max_iter, tol, teleport + (size_t)j * g->n, flags, out + (size_t)j * g->n,
+                                  stats ? stats + j : nullptr);
+            if (rc) return rc;
+        }
+        return EGPR_SUCC;
+    }
     return ppr_batch_solve(g, alpha, max_iter, tol, k, teleport, nullptr, nullptr, flags, out, stats);
 }
 
@@ -845,6 +883,19 @@ int egpr_pagerank_seeds(egpr_graph* g, double alpha, int32_t max_iter, double to
     if (k < 1 || !seed_ptr || !out) return fail_arg("k >= 1, seed_ptr and out are required");
     std::lock_guard<std::mutex> lk(g->mu);
     if (g->pending) return fail_arg("a solve is pending on this graph");
+    if (k < kSpmmMinColumns) {  // a few columns: single-vector solves with the seed sets uploaded sparse
+        int rc;
+        if ((rc = check_device(g))) return rc;
+        for (int32_t j = 0; j < k; ++j) {
+            const int32_t b = seed_ptr[j], e = seed_ptr[j + 1];
+            if (e <= b || b < 0) return fail_arg("every seed set needs at least one seed");
+            if (g->nnz > 0 && (rc = upload_teleport_seeds(g, seeds + b, e - b, g->stream))) return rc;
+            if ((rc = solve_single(g, alpha, max_iter, tol, nullptr, flags, out + (size_t)j * g->n,
+                                   stats ? stats + j : nullptr, true)))
+                return rc;
+        }
+        return EGPR_SUCC;
+    }
     return ppr_batch_solve(g, alpha, max_iter, tol, k, nullptr, seed_ptr, seeds, flags, out, stats);
 }
 

@@ -202,6 +202,7 @@ struct egpr_graph {
     int32_t tune_spmm_chunk = 1024; // batched solve: entries per work unit
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
+    egpr::DevBuf seed_ids;         // seed set of a single-vector PPR solve
     egpr::Plan plan;               // single-graph plan
     egpr::SpmmWork* spmm = nullptr; // batched personalised PageRank workspace
     cudaStream_t own_stream = nullptr;
@@ -250,7 +251,10 @@ int launch_init(Plan& plan, double alpha, int32_t max_iter, double tol, bool per
 int launch_loop(Plan& plan, int32_t max_iter, cudaStream_t stream, int32_t* launches);
 int launch_finish(Plan& plan, bool correction, cudaStream_t stream, int32_t* launches);
 
-// SpMM personalised PageRank (spmm.cu).
+// SpMM personalised PageRank (spmm.cu).  A batched sweep gathers a whole
+// 32-column panel per entry, about seven single-vector sweeps' worth, so
+// batches of fewer columns run as single-vector solves.
+constexpr int32_t kSpmmMinColumns = 6;
 void spmm_work_release(egpr_graph* g);
 int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, int32_t k,
                     const double* teleport_dense, const int32_t* seed_ptr, const int32_t* seeds,

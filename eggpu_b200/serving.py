@@ -7,9 +7,9 @@ idle graphs, and serves requests as they arrive:
 
 * every graph has at most one solve in flight; requests that arrive while it
   runs queue up and are folded into that graph's next solve: all queued PPR
-  requests become the columns of one batched SpMM solve
-  (``egpr_pagerank_seeds``), all queued plain requests share one solve (their
-  answer is identical);
+  requests go to one ``egpr_pagerank_seeds`` call (one batched SpMM solve
+  from six columns on, single-vector solves below), all queued plain requests
+  share one solve (their answer is identical);
 * solves on different graphs run concurrently from a pool of worker threads,
   each prepared graph on its own CUDA stream, so their kernels overlap on the
   device;
@@ -167,11 +167,12 @@ class Server:
     """Serves Request objects; submit() returns a Future resolving to (ranks, stats)."""
 
     def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True, pinned=True,
-                 multi_min=8, ppr_min_batch=6):
+                 multi_min=8, ppr_min_batch=1):
         self.registry = registry
-        # a batched solve gathers one 32-column panel per inbound entry, about
-        # seven single-vector sweeps' worth: fewer PPR requests than this for
-        # one graph are solved one by one
+        # PPR groups smaller than this go through the dense single-vector
+        # entry one request at a time; otherwise through egpr_pagerank_seeds,
+        # which itself solves fewer than six columns as single-vector solves
+        # with the seed sets uploaded sparse
         self.ppr_min_batch = int(ppr_min_batch)
         # plain requests of small graphs share one multi-graph launch once at
         # least multi_min such graphs wait (a launch plan over a new set of

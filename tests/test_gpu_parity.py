@@ -405,3 +405,19 @@ def test_many_graphs_config_full_size_512_er():
         _check_against_oracle(c.V, c.E, None, outs[i], sts[i], 0.85, 100, 1e-6)
         single, st = graphs[i].pagerank(alpha=0.85, max_iter=100, tol=1e-6)
         assert st["iterations"] == sts[i]["iterations"] and np.abs(single - outs[i]).sum() <= L1_TOL
+
+
+def test_ppr_few_columns_are_single_vector_solves():
+    # fewer than six columns: egpr_pagerank_seeds / _batch run single-vector solves (seed sets uploaded sparse)
+    g = synth.rmat(scale=13, edgefactor=16, seed=35)
+    sets = synth.seed_sets(g.n, 3, 1, 16, seed=8)
+    pg = _native.PreparedGraph(g.V, g.E)
+    ranks, stats = pg.pagerank_seeds(sets, alpha=0.85, max_iter=100, tol=1e-6)
+    dense, dstats = pg.pagerank_batch(np.stack([_seed_teleport(g.n, s) for s in sets]), alpha=0.85, max_iter=100,
+                                      tol=1e-6)
+    for j in range(3):
+        single, st = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6, personalization=_seed_teleport(g.n, sets[j]))
+        assert np.array_equal(ranks[j], single) and np.array_equal(dense[j], single)
+        assert stats[j]["iterations"] == st["iterations"] == dstats[j]["iterations"]
+        _check_against_oracle(g.V, g.E, None, ranks[j], stats[j], 0.85, 100, 1e-6,
+                              teleport=_seed_teleport(g.n, sets[j]))
