@@ -48,7 +48,7 @@ namespace {
 
 constexpr unsigned kAll = 0xffffffffu;
 constexpr int kLanes = 32;          // columns per panel
-constexpr int kSpWarps = 24;        // warps per CTA of the FP32 sweep (one CTA per SM)
+constexpr int kSpWarps = 28;        // warps per CTA of the FP32 sweep (one CTA per SM)
 constexpr int kSpWarps64 = 16;      // of the FP64 sweep (its row buffers are twice as large)
 template <bool kF64>
 __host__ __device__ constexpr int sp_threads() { return 32 * (kF64 ? kSpWarps64 : kSpWarps); }
