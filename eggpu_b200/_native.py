@@ -360,11 +360,23 @@ except Exception:  # torch is optional here
     pass
 
 
-def pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6, correction=True):
-    """Solves many prepared graphs in one persistent launch per sweep."""
+def pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6, correction=True, out=None):
+    """Solves many prepared graphs in one persistent launch per sweep.
+    out: optional list of caller-owned float64[n_i] result arrays; by default
+    the results are views of one page-locked block (up to 256 MiB)."""
     count = len(graphs)
     handles = (c_void_p * count)(*[g.handle for g in graphs])
-    outs = [np.empty(g.n, np.float64) for g in graphs]
+    if out is not None:
+        outs = list(out)
+        if len(outs) != count or any(
+                not isinstance(o, np.ndarray) or o.dtype != np.float64 or o.shape != (g.n,)
+                or not o.flags.c_contiguous or not o.flags.writeable for o, g in zip(outs, graphs)):
+            raise ValueError("out must hold one writeable contiguous float64[n] array per graph")
+    else:
+        total = sum(g.n for g in graphs)
+        block = pinned_empty(total) if 8 * total <= (256 << 20) else np.empty(total, np.float64)
+        offs = np.concatenate([[0], np.cumsum([g.n for g in graphs])])
+        outs = [block[offs[i]:offs[i + 1]] for i in range(count)]
     out_ptrs = (c_void_p * count)(*[o.ctypes.data for o in outs])
     sts = (EgprStats * count)()
     flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
