@@ -99,8 +99,16 @@ cudaMemPool_t device_pool() {
             cudaGetLastError();
             return nullptr;
         }
+        // freed memory the pool keeps for reuse: EGPR_POOL_KEEP_MB, else a
+        // quarter of the device (a scale-25 preparation frees ~17 GB of
+        // scratch; mapping it again on every graph would cost ~1 s)
         const char* e = std::getenv("EGPR_POOL_KEEP_MB");
-        const long long mb = e ? std::atoll(e) : 8192;
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            total_b = 32ull << 30;
+        }
+        const long long mb = e ? std::atoll(e) : (long long)(total_b >> 22);  // total / 4, in MiB
         unsigned long long keep = (unsigned long long)std::max(0LL, mb) << 20;
         cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
         g_pools[dev] = p;

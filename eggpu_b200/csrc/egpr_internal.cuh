@@ -219,7 +219,8 @@ namespace egpr {
 
 // The library's memory pool of the current device: device buffers and
 // preparation scratch come from it, and it keeps up to EGPR_POOL_KEEP_MB
-// (default 8192) MiB of freed memory for reuse (null if pools are unavailable).
+// (default: a quarter of the device) MiB of freed memory for reuse (null if
+// pools are unavailable).
 cudaMemPool_t device_pool();
 
 // Status helpers.
