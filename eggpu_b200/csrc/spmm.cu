@@ -757,38 +757,37 @@ __global__ void k_sp_tele_rows(const int32_t* __restrict__ tv, int32_t nt, uint3
 }
 
 // X0 = 1/n on live columns, 0 on padding columns and on row n of both
-// iterates; column states.
+// iterates (grid.y = panel, 16-byte stores); column states.
 __global__ void k_sp_init(float* X0, float* X1, ColState* cols, int32_t n, int32_t npanels, int32_t k, double alpha,
                           int32_t ndang) {
     const float x0 = (float)(1.0 / (double)n);
-    const int64_t rowsz = ((int64_t)n + 1) * kLanes;
-    const int64_t total = (int64_t)npanels * rowsz;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t lane = (int32_t)(i & 31);
-        const int32_t p = (int32_t)(i / rowsz);
-        const int64_t v = (i - p * rowsz) >> 5;
-        if (v == n) {
-            X0[i] = 0.f;
-            X1[i] = 0.f;
+    const int32_t p = blockIdx.y;
+    const int64_t quads = ((int64_t)n + 1) * (kLanes / 4);
+    float4* a = reinterpret_cast<float4*>(X0 + (size_t)p * ((size_t)n + 1) * kLanes);
+    float4* b = reinterpret_cast<float4*>(X1 + (size_t)p * ((size_t)n + 1) * kLanes);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = p * kLanes + 4 * (int32_t)(q & 7);  // first column of the quad
+        if ((q >> 3) == n) {
+            a[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+            b[q] = make_float4(0.f, 0.f, 0.f, 0.f);
         } else {
-            X0[i] = (p * kLanes + lane) < k ? x0 : 0.f;
+            a[q] = make_float4(c < k ? x0 : 0.f, c + 1 < k ? x0 : 0.f, c + 2 < k ? x0 : 0.f, c + 3 < k ? x0 : 0.f);
         }
     }
-    const int32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < npanels * kLanes) {
-        ColState c;
-        c.dsum = (double)ndang * (double)x0;
-        c.dmass = alpha * c.dsum / (double)n;
-        c.dmass_prev = c.dmass;
-        c.residual = 0.0;
-        c.residual64 = 0.0;
-        c.xsum = 0.0;
-        c.iter = 0;
-        c.active = j < k ? 1 : 0;
-        c.done = j < k ? 0 : 1;
-        c.converged = 0;
-        cols[j] = c;
+    const int32_t j = p * kLanes + (int32_t)threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x < kLanes) {
+        ColState cs;
+        cs.dsum = (double)ndang * (double)x0;
+        cs.dmass = alpha * cs.dsum / (double)n;
+        cs.dmass_prev = cs.dmass;
+        cs.residual = 0.0;
+        cs.residual64 = 0.0;
+        cs.xsum = 0.0;
+        cs.iter = 0;
+        cs.active = j < k ? 1 : 0;
+        cs.done = j < k ? 0 : 1;
+        cs.converged = 0;
+        cols[j] = cs;
     }
 }
 
@@ -819,34 +818,37 @@ __global__ void k_sp_colsum_set(ColState* __restrict__ cols, const unsigned long
 }
 
 // out[j*n + v] = final iterate / its sum (panel-major FP64 or FP32 source),
-// transposed through shared memory so both sides are coalesced.
-__global__ void k_sp_normalize(const double* __restrict__ out64, const float* X0, const float* X1,
-                               const ColState* __restrict__ cols, int32_t n, int32_t k, int32_t from_fp32,
-                               double* __restrict__ out) {
-    __shared__ double tile[32][33];
+// transposed through shared memory 128 vertices at a time so that both sides
+// are coalesced.
+constexpr int kNormRows = 128;
+__global__ void __launch_bounds__(256) k_sp_normalize(const double* __restrict__ out64, const float* X0, const float* X1,
+                                                      const ColState* __restrict__ cols, int32_t n, int32_t k,
+                                                      int32_t from_fp32, double* __restrict__ out) {
+    __shared__ double tile[kNormRows][kLanes + 1];
     const int32_t p = blockIdx.y;
-    const int32_t v0 = blockIdx.x * 32;
+    const int32_t v0 = blockIdx.x * kNormRows;
     const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
     const int32_t col = p * kLanes + lane;
     const ColState cs = cols[col];
-    const float* xl = (cs.iter & 1) ? X1 : X0;
+    const float* xl = ((cs.iter & 1) ? X1 : X0) + (size_t)p * ((size_t)n + 1) * kLanes;
+    const double* ol = out64 + (size_t)p * ((size_t)n + 1) * kLanes;
     const double inv = cs.xsum > 0.0 ? 1.0 / cs.xsum : 0.0;
     const double uni = 1.0 / (double)n;
-    for (int r = row; r < 32; r += blockDim.x / 32) {
+    for (int r = row; r < kNormRows; r += (int)(blockDim.x >> 5)) {
         const int32_t v = v0 + r;
         double val = 0.0;
         if (v < n) {
-            const size_t off = ((size_t)p * ((size_t)n + 1) + v) * kLanes + lane;
-            const double raw = from_fp32 ? (double)xl[off] : out64[off];
+            const size_t off = (size_t)v * kLanes + lane;
+            const double raw = from_fp32 ? (double)xl[off] : ol[off];
             val = cs.xsum > 0.0 ? raw * inv : uni;
         }
         tile[r][lane] = val;
     }
     __syncthreads();
-    for (int r = row; r < 32; r += blockDim.x / 32) {
-        const int32_t j = p * kLanes + r;
-        const int32_t v = v0 + lane;
-        if (j < k && v < n) out[(size_t)j * n + v] = tile[lane][r];
+    for (int idx = threadIdx.x; idx < kLanes * kNormRows; idx += blockDim.x) {
+        const int jj = idx / kNormRows, i = idx - jj * kNormRows;
+        const int32_t j = p * kLanes + jj, v = v0 + i;
+        if (j < k && v < n) out[(size_t)j * n + v] = tile[i][jj];
     }
 }
 
@@ -1099,7 +1101,8 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event"))) return rc;
     k_sp_meta<<<grid_1d(n), 256, 0, s>>>(g->outw.as<double>(), n, w.meta.as<uint32_t>());
     if (nt > 0) k_sp_tele_rows<<<(nt + 255) / 256, 256, 0, s>>>(w.tele_v.as<int32_t>(), nt, w.meta.as<uint32_t>());
-    k_sp_init<<<grid_1d((int64_t)npanels * (n + 1) * kLanes), 256, 0, s>>>(
+    k_sp_init<<<dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 1) * 8 / 256 + 1, 148 * 8)),
+                     (unsigned)npanels), 256, 0, s>>>(
         w.X0.as<float>(), w.X1.as<float>(), w.cols.as<ColState>(), n, npanels, kg, alpha, g->n_dangling_solve);
     int32_t launches = nt > 0 ? 3 : 2;
     if (graph_loop_enabled()) build_loop_graph(w, grid);
@@ -1126,7 +1129,7 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
         launches += 2;
     }
     {
-        dim3 gr((unsigned)((n + 31) / 32), (unsigned)npanels);
+        dim3 gr((unsigned)((n + kNormRows - 1) / kNormRows), (unsigned)npanels);
         k_sp_normalize<<<gr, 256, 0, s>>>(w.out64.as<double>(), w.X0.as<float>(), w.X1.as<float>(),
                                           w.cols.as<ColState>(), n, kg, correction ? 0 : 1, w.out.as<double>());
         launches += 1;
