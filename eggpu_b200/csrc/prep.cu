@@ -605,7 +605,9 @@ int default_row_cost() {
 //     of the tile ends (the k-th mark of a tile ends row tile_row + k, since
 //     every row has an entry).
 // Chunks are stored costliest first, which is their queue order.
-int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* sorted_dst, cudaStream_t s) {
+// The layout's tables (row offsets, chunks, tile masks, span links), which
+// need in_row only; the entries follow in build_sweep_entries.
+int build_sweep_tables(egpr_graph* g, int32_t resident_warps, cudaStream_t s) {
     const int32_t n = g->n;
     TmpAlloc tmp(s);
     int rc = EGPR_SUCC;
@@ -757,6 +759,17 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
     if ((rc = g->sw_col.alloc((size_t)nnz * sizeof(int32_t) + pad)) ||
         (g->weighted && (rc = g->sw_w.alloc((size_t)nnz * sizeof(float) + pad))))
         return rc;
+    return cuda_ok(cudaGetLastError(), "sweep tables");
+}
+
+// The layout's entries: in_col (hub codes already in place) copied behind the
+// row offsets, with a placeholder in every empty row.  Stream-ordered; the
+// tables must be complete on the device.
+int build_sweep_entries(egpr_graph* g, const uint32_t* sorted_dst, cudaStream_t s) {
+    const int32_t n = g->n;
+    const int32_t nnz = (int32_t)g->sw_nnz;
+    const size_t pad = (size_t)(kTileItems + 16) * sizeof(int32_t);
+    int rc;
     // every entry is written below; only the padding past the last one is cleared
     if ((rc = cuda_ok(cudaMemsetAsync(g->sw_col.as<int32_t>() + nnz, 0, pad, s), "memset"))) return rc;
     if (g->weighted && (rc = cuda_ok(cudaMemsetAsync(g->sw_w.as<float>() + nnz, 0, pad, s), "memset"))) return rc;
@@ -774,6 +787,12 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
             g->sw_row.as<int32_t>(), g->sw_col.as<int32_t>(), g->weighted ? g->sw_w.as<float>() : nullptr,
             -(g->nhub + 1));
     }
+    return cuda_ok(cudaGetLastError(), "sweep entries");
+}
+
+int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* sorted_dst, cudaStream_t s) {
+    int rc;
+    if ((rc = build_sweep_tables(g, resident_warps, s)) || (rc = build_sweep_entries(g, sorted_dst, s))) return rc;
     return cuda_ok(cudaStreamSynchronize(s), "sweep layout");
 }
 
@@ -870,12 +889,30 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                                           cudaMemcpyHostToDevice, s), "H2D zero slot")))
             return rc;
         k_dangling<<<grid_for(n), kThreads, 0, s>>>(g->outw.as<double>(), n, g->dangling01.as<int32_t>(), counts);
+        // The layout's tables need in_row only (complete since the nnz read
+        // above): they are built on a second stream while the inbound sort, the
+        // gather and the hub ranking run on s; the entries then follow on s.
+        cudaStream_t s2 = nullptr;
+        cudaEvent_t e2 = nullptr;
+        if ((rc = cuda_ok(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking), "stream")) ||
+            (rc = cuda_ok(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming), "event"))) {
+            if (s2) cudaStreamDestroy(s2);
+            return rc;
+        }
+        rc = build_sweep_tables(g, sweep_resident_warps(), s2);
+        if (!rc) rc = cuda_ok(cudaEventRecord(e2, s2), "event");
+        if (!rc) rc = cuda_ok(cudaStreamWaitEvent(s, e2, 0), "event");
+        if (!rc) rc = build_sweep_entries(g, sorted_dst, s);
+        if (rc) cudaStreamSynchronize(s2);  // nothing of s2 may outlive an early return
+        cudaEventDestroy(e2);
+        cudaStreamDestroy(s2);  // released once its work is done
+        if (rc) return rc;
         unsigned long long hc[2] = {0, 0};
+        // a copy into pageable memory returns once it is done, after all of s above
         if ((rc = cuda_ok(cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, s), "D2H counts")))
             return rc;
         g->n_dangling = (int32_t)hc[0];
         g->n_dangling_solve = (int32_t)hc[1];
-        if ((rc = build_sweep_layout(g, sweep_resident_warps(), sorted_dst, s))) return rc;
     }
     cudaEventRecord(g->ev1, s);
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "preparation"))) return rc;
