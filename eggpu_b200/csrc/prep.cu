@@ -183,9 +183,10 @@ __device__ __forceinline__ double sanitize_w(double w) {
 // FP64 out-weight sum per source in entry order (pagerank.cu:301-316).  For
 // unit weights the sum is a count, which is exact in any order.
 __global__ void k_out_weight(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
-                             const double* __restrict__ W, int32_t n, double* __restrict__ outw,
-                             uint32_t* __restrict__ hub_key, uint32_t* __restrict__ hub_val) {
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+                             const double* __restrict__ W, int32_t n, int32_t r0, int32_t r1,
+                             double* __restrict__ outw, uint32_t* __restrict__ hub_key,
+                             uint32_t* __restrict__ hub_val) {
+    for (int64_t u = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < r1;
          u += (int64_t)gridDim.x * blockDim.x) {
         const int32_t b = V[u], e = V[u + 1];
         double s = 0.0;
@@ -214,13 +215,13 @@ __global__ void k_out_weight(const int32_t* __restrict__ V, const int32_t* __res
 
 // Unit weights: the out-weight sum is the count of valid entries, exact in any
 // order, so one warp counts a row.
-__global__ void k_out_degree(const int32_t* __restrict__ V, const int32_t* __restrict__ E, int32_t n,
-                             double* __restrict__ outw, uint32_t* __restrict__ hub_key,
+__global__ void k_out_degree(const int32_t* __restrict__ V, const int32_t* __restrict__ E, int32_t n, int32_t r0,
+                             int32_t r1, double* __restrict__ outw, uint32_t* __restrict__ hub_key,
                              uint32_t* __restrict__ hub_val) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t u = warp; u < n; u += nwarps) {
+    for (int64_t u = r0 + warp; u < r1; u += nwarps) {
         const int32_t b = V[u], e = V[u + 1];
         int32_t c = 0;
         for (int32_t p = b + lane; p < e; p += 32) {
@@ -265,10 +266,10 @@ __global__ void k_decode_hubs(const int32_t* __restrict__ in_col, int64_t nnz, c
 
 // In-degree histogram and the sort keys: destination, or n for an entry whose
 // destination is outside [0, n) (those sort last and are dropped).
-__global__ void k_in_degree_keys(const int32_t* __restrict__ E, int64_t m, int32_t n,
+__global__ void k_in_degree_keys(const int32_t* __restrict__ E, int64_t p0, int64_t p1, int32_t n,
                                  uint32_t* __restrict__ indeg, uint32_t* __restrict__ keys,
                                  uint32_t* __restrict__ vals) {
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < m;
+    for (int64_t p = p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < p1;
          p += (int64_t)gridDim.x * blockDim.x) {
         const int32_t v = E[p];
         const bool ok = v >= 0 && v < n;
@@ -827,15 +828,64 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             return rc;
         if ((rc = cuda_ok(cudaMemcpyAsync(dV, V, ((size_t)n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D offsets")))
             return rc;
-        if (m > 0 && (rc = cuda_ok(cudaMemcpyAsync(dE, E, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D indices")))
-            return rc;
-        if (W && m > 0 && (rc = cuda_ok(cudaMemcpyAsync(dW, W, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s), "H2D weights")))
-            return rc;
         cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * sizeof(uint32_t), s);
         cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s);
-        if (dW) k_out_weight<<<grid_for(n), kThreads, 0, s>>>(dV, dE, dW, n, g->outw.as<double>(), hkey, hval);
-        else k_out_degree<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, dE, n, g->outw.as<double>(), hkey, hval);
-        if (m > 0) k_in_degree_keys<<<grid_for(m), kThreads, 0, s>>>(dE, m, n, indeg, keys, vals);
+        {
+            // E (and W) arrive in pieces on a copy stream; the degree passes of
+            // each piece run on s while the next one is in flight.  A piece's
+            // out-degree pass covers the rows whose entries have all arrived.
+            const int pieces = m >= (int64_t)(8 << 20) ? 4 : 1;
+            cudaStream_t sc = nullptr;
+            std::vector<cudaEvent_t> ev((size_t)pieces, nullptr);
+            if (pieces > 1) {
+                rc = cuda_ok(cudaStreamCreateWithFlags(&sc, cudaStreamNonBlocking), "stream");
+                for (int i = 0; i < pieces && !rc; ++i)
+                    rc = cuda_ok(cudaEventCreateWithFlags(&ev[(size_t)i], cudaEventDisableTiming), "event");
+                // the copy stream starts after the memsets and the offsets above
+                cudaEvent_t start = nullptr;
+                if (!rc) rc = cuda_ok(cudaEventCreateWithFlags(&start, cudaEventDisableTiming), "event");
+                if (!rc) rc = cuda_ok(cudaEventRecord(start, s), "event");
+                if (!rc) rc = cuda_ok(cudaStreamWaitEvent(sc, start, 0), "event");
+                if (start) cudaEventDestroy(start);
+            }
+            int32_t r_done = 0;
+            for (int i = 0; i < pieces && !rc; ++i) {
+                const int64_t a = m * i / pieces, b = m * (i + 1) / pieces;
+                cudaStream_t cs = pieces > 1 ? sc : s;
+                if (b > a) {
+                    rc = cuda_ok(cudaMemcpyAsync(dE + a, E + a, (size_t)(b - a) * sizeof(int32_t), cudaMemcpyHostToDevice, cs),
+                                 "H2D indices");
+                    if (!rc && W)
+                        rc = cuda_ok(cudaMemcpyAsync(dW + a, W + a, (size_t)(b - a) * sizeof(double),
+                                                     cudaMemcpyHostToDevice, cs), "H2D weights");
+                }
+                if (!rc && pieces > 1) {
+                    rc = cuda_ok(cudaEventRecord(ev[(size_t)i], sc), "event");
+                    if (!rc) rc = cuda_ok(cudaStreamWaitEvent(s, ev[(size_t)i], 0), "event");
+                }
+                if (rc) break;
+                // rows [r_done, r_end): V[r_end] <= b, all of them when this is the last piece
+                int32_t r_end = n;
+                if (i + 1 < pieces) r_end = (int32_t)(std::upper_bound(V, V + n + 1, (int32_t)b) - V) - 1;
+                if (r_end > r_done) {
+                    if (dW)
+                        k_out_weight<<<grid_for(r_end - r_done), kThreads, 0, s>>>(dV, dE, dW, n, r_done, r_end,
+                                                                                   g->outw.as<double>(), hkey, hval);
+                    else
+                        k_out_degree<<<grid_for((int64_t)(r_end - r_done) * 32), kThreads, 0, s>>>(
+                            dV, dE, n, r_done, r_end, g->outw.as<double>(), hkey, hval);
+                    r_done = r_end;
+                }
+                if (b > a) k_in_degree_keys<<<grid_for(b - a), kThreads, 0, s>>>(dE, a, b, n, indeg, keys, vals);
+            }
+            if (sc) {
+                if (rc) cudaStreamSynchronize(sc);
+                cudaStreamDestroy(sc);  // released once its copies are done
+            }
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+            if (rc) return rc;
+        }
         if ((rc = exclusive_scan_u32(indeg, reinterpret_cast<uint32_t*>(g->in_row.as<int32_t>()), (int64_t)n + 1, s)))
             return rc;
         const uint32_t* sorted_dst = nullptr;  // destination of every inbound entry, in entry order
