@@ -97,8 +97,8 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, int64_t len, const uint32
 }
 
 // -------------------------------------------------------------- radix ------
-// LSD radix sort of (key, value) pairs with digits of kBits bits (8 to 11):
-// a key of B bits takes ceil(B / 11) passes of equal digits.
+// LSD radix sort of (key, value) pairs with digits of kBits bits (8 in use):
+// a key of B bits takes ceil(B / kBits) passes.
 template <int kBits>
 __global__ void __launch_bounds__(kThreads)
 k_radix_hist(const uint32_t* __restrict__ keys, int64_t len, int shift, int64_t ntiles,
@@ -153,6 +153,8 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         rank[r] = before + __popc(peers & lt_mask);
     }
     __syncthreads();
+    // per digit: the warps' prefix, and the tile's count (then its start in the tile)
+    uint32_t* dstart = tile_off + kD;  // [kD]
     for (int d = tid; d < kD; d += kThreads) {
         uint32_t run = 0;
 #pragma unroll
@@ -161,17 +163,47 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
             warp_hist[w][d] = run;
             run += c;
         }
+        dstart[d] = run;
     }
     __syncthreads();
+    if (warp == 0) {  // exclusive scan of the kD counts, one warp
+        uint32_t carry = 0;
+        for (int d0 = 0; d0 < kD; d0 += 32) {
+            const uint32_t c = dstart[d0 + lane];
+            uint32_t x = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            dstart[d0 + lane] = carry + x - c;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+    }
+    __syncthreads();
+    // the tile in digit order in shared memory (same order as before: digit,
+    // then warp, then item), then each digit's run written out contiguously
+    uint32_t* skey = dstart + kD;          // [kSortTile]
+    uint32_t* sval = skey + kSortTile;     // [kSortTile]
 #pragma unroll
     for (int r = 0; r < kSortPerLane; ++r) {
         const int64_t idx = wbase + (int64_t)r * 32 + lane;
         if (idx < len) {
             const uint32_t d = (key[r] >> shift) & (kD - 1);
-            const uint32_t dst = tile_off[d] + warp_hist[warp][d] + rank[r];
-            if (keys_out) keys_out[dst] = key[r];
-            vals_out[dst] = val[r];
+            const uint32_t lpos = dstart[d] + warp_hist[warp][d] + rank[r];
+            skey[lpos] = key[r];
+            sval[lpos] = val[r];
         }
+    }
+    __syncthreads();
+    const int64_t tbase = (int64_t)blockIdx.x * kSortTile;
+    const int nvalid = (int)(len - tbase < (int64_t)kSortTile ? len - tbase : (int64_t)kSortTile);
+    for (int i = tid; i < nvalid; i += kThreads) {
+        const uint32_t k = skey[i];
+        const uint32_t d = (k >> shift) & (kD - 1);
+        const uint32_t dst = tile_off[d] + ((uint32_t)i - dstart[d]);
+        if (keys_out) keys_out[dst] = k;
+        vals_out[dst] = sval[i];
     }
 }
 
@@ -378,7 +410,8 @@ template <int kBits>
 int radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t len, int shift,
                bool last, int64_t ntiles, uint32_t* hist, cudaStream_t s) {
     constexpr int kD = 1 << kBits;
-    const size_t smem = (size_t)(kWarps + 1) * kD * sizeof(uint32_t);
+    // warp histograms, tile offsets, digit starts, and the tile's keys and values
+    const size_t smem = ((size_t)(kWarps + 2) * kD + 2 * (size_t)kSortTile) * sizeof(uint32_t);
     static bool attr_set = false;  // per process; the attribute is per function and harmless to repeat
     if (!attr_set) {
         cudaFuncSetAttribute(k_radix_scatter<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -401,21 +434,18 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_
     *result_in_alt = false;
     if (len <= 1 || bits <= 0) return EGPR_SUCC;
     int rc = EGPR_SUCC;
-    const int passes = (bits + 10) / 11;
-    const int dbits = std::max(8, (bits + passes - 1) / passes);
+    // 8-bit digits: with 4096-item tiles a digit's run averages 16 items, so
+    // the runs written out are 64-byte pieces (11-bit digits, one pass fewer,
+    // leave 2-item runs and were slower in total)
+    const int passes = (bits + 7) / 8;
     const int64_t ntiles = (len + kSortTile - 1) / kSortTile;
-    uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles << dbits, &rc);
+    uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles << 8, &rc);
     if (!hist) return rc;
     uint32_t *kin = keys, *vin = vals, *kout = keys_alt, *vout = vals_alt;
     for (int p = 0; p < passes; ++p) {
-        const int shift = p * dbits;
+        const int shift = p * 8;
         const bool last = p == passes - 1 && !keys_needed;
-        switch (dbits) {
-            case 8: rc = radix_pass<8>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
-            case 9: rc = radix_pass<9>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
-            case 10: rc = radix_pass<10>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
-            default: rc = radix_pass<11>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s); break;
-        }
+        rc = radix_pass<8>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s);
         if (rc) return rc;
         std::swap(kin, kout);
         std::swap(vin, vout);
