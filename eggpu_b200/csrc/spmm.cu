@@ -29,9 +29,12 @@
 // load (two source rows per warp instruction).  Row sums go to a per-warp
 // buffer in shared memory; the rows a batch finishes are then written in one
 // pass (previous iterate, teleport, dangling term), with their loads issued
-// together.  Column sums (residual, dangling mass, rank sum) are converted to
-// fixed point per chunk and added with integer atomics, so their value does not
-// depend on which warp ran which chunk.
+// together.  Column sums (residual and dangling mass; the FP64 sweep's rank
+// sum) are converted to fixed point per chunk and added with integer atomics,
+// so their value does not depend on which warp ran which chunk.
+//
+// Batches of fewer than kSpmmMinColumns columns do not come here: the entry
+// points run them as single-vector solves (a panel costs about seven sweeps).
 #include <cuda_runtime.h>
 
 #include <algorithm>
