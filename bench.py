@@ -44,6 +44,23 @@ def _rank_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(dist, vals, device):
+    """Each value's maximum over the ranks of the process group (the values
+    themselves on a single process): a multi-GPU time is the slowest rank's."""
+    if not dist:
+        return [float(v) for v in vals]
+    import torch
+
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_rate(world, units_per_rank, seconds):
+    """Units all ranks processed (each rank does the same work) per second of the slowest rank."""
+    return world * units_per_rank / seconds
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -223,14 +240,12 @@ def run_ours(args):
         t_step, st = timed(args.steps, sweeps)
         t_step2, st2 = timed(max(1, args.steps // 2), 2 * sweeps)
     torch.cuda.synchronize()
+    t_step, t_step2 = max_over_ranks(dist, [t_step, t_step2], "cuda")
     if dist:
-        tt = torch.tensor([t_step, t_step2], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step, t_step2 = tt.tolist()
         dist.barrier()
     t_sweep = max((t_step2 - t_step) / sweeps, 1e-9)
     bytes_per_iter = st["bytes_per_iter"]
-    value = world * nnz * sweeps / t_step / 1e9
+    value = whole_job_rate(world, nnz * sweeps, t_step) / 1e9
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_iter / t_sweep / 1e9
     traffic = profile_traffic(f"k_sweep_{args.workload}.md")
@@ -252,12 +267,9 @@ def run_ours(args):
         _native.pagerank_csr(Vp, Ep, Wp, 2 * 10**9 + i, 0.85, sweeps, 0.0, out=PRp)
         _native.cache_reset()
     t_e2e = (time.perf_counter() - t0) / max(e2e_steps, 1)
-    if dist:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = tt.item()
+    (t_e2e,) = max_over_ranks(dist, [t_e2e], "cuda")
     h2d = csr.V.nbytes + csr.E.nbytes + (0 if csr.W is None else csr.W.nbytes)
-    e2e = None if not e2e_steps else {"value": world * nnz * sweeps / t_e2e / 1e9, "unit": "GTEPS/iter", "h2d_bytes_per_step": int(h2d),
+    e2e = None if not e2e_steps else {"value": whole_job_rate(world, nnz * sweeps, t_e2e) / 1e9, "unit": "GTEPS/iter", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(8 * csr.n), "ms_per_step": t_e2e * 1e3,
            "path": "egpr_pagerank_csr (drop-in for gpu_easygraph::pagerank): H2D of the out-edge CSR, GPU "
                    "preparation, solve, D2H of FP64 ranks into the caller's page-locked result vector, every "
