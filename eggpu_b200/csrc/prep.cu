@@ -12,7 +12,9 @@
 //                    one destination keep ascending entry order, i.e. the
 //                    ascending-source order of the reference's sequential
 //                    scatter (:328-346)
-//   k_gather_inbound in_col / in_w from the sorted entry ids
+//   k_gather_inbound in_col / in_w from the sorted entry ids (weighted; with
+//                    unit weights the pairs carry the source, and the sorted
+//                    values are in_col)
 //   k_dangling       dangling mask outw <= 0 (:323-326) and the counts used by
 //                    the solver
 //
@@ -307,7 +309,7 @@ __global__ void k_in_degree_keys(const int32_t* __restrict__ E, int64_t p0, int6
         const bool ok = v >= 0 && v < n;
         if (ok) atomicAdd(&indeg[v], 1u);
         keys[p] = ok ? (uint32_t)v : (uint32_t)n;
-        vals[p] = (uint32_t)p;
+        if (vals) vals[p] = (uint32_t)p;  // weighted: the entry id (its weight is gathered after the sort)
     }
 }
 
@@ -844,7 +846,7 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         uint32_t* vals = tmp.get<uint32_t>((size_t)m, &rc);
         uint32_t* keys2 = tmp.get<uint32_t>((size_t)m, &rc);
         uint32_t* vals2 = tmp.get<uint32_t>((size_t)m, &rc);
-        int32_t* src = tmp.get<int32_t>((size_t)m, &rc);
+        int32_t* src = W ? tmp.get<int32_t>((size_t)m, &rc) : nullptr;  // weighted: source of every entry
         unsigned long long* counts = tmp.get<unsigned long long>(2, &rc);
         uint32_t* hkey = tmp.get<uint32_t>((size_t)n, &rc);
         uint32_t* hval = tmp.get<uint32_t>((size_t)n, &rc);
@@ -860,6 +862,10 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             return rc;
         cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * sizeof(uint32_t), s);
         cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s);
+        // unit weights: the sort carries each entry's source (written from the
+        // offsets alone, while E is still arriving), so no gather follows it
+        if (!W && m > 0)
+            k_expand_src<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, n, reinterpret_cast<int32_t*>(vals));
         {
             // E (and W) arrive in pieces on a copy stream; the degree passes of
             // each piece run on s while the next one is in flight.  A piece's
@@ -906,7 +912,8 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                             dV, dE, n, r_done, r_end, g->outw.as<double>(), hkey, hval);
                     r_done = r_end;
                 }
-                if (b > a) k_in_degree_keys<<<grid_for(b - a), kThreads, 0, s>>>(dE, a, b, n, indeg, keys, vals);
+                if (b > a)
+                    k_in_degree_keys<<<grid_for(b - a), kThreads, 0, s>>>(dE, a, b, n, indeg, keys, W ? vals : nullptr);
             }
             if (sc) {
                 if (rc) cudaStreamSynchronize(sc);
@@ -939,12 +946,18 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             while (bits < 32 && (kmax >> bits) != 0) ++bits;
             bool alt = false;
             if ((rc = radix_sort_pairs(keys, vals, keys2, vals2, m, bits, s, tmp, &alt))) return rc;
-            const uint32_t* sorted_ids = alt ? vals2 : vals;
+            const uint32_t* sorted_vals = alt ? vals2 : vals;
             sorted_dst = alt ? keys2 : keys;
-            k_expand_src<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, n, src);
-            if (nnz > 0)
-                k_gather_inbound<<<grid_for(nnz), kThreads, 0, s>>>(sorted_ids, nnz, src, dW, g->in_col.as<int32_t>(),
-                                                                   W ? g->in_w.as<float>() : nullptr);
+            if (!W) {
+                if (nnz > 0 && (rc = cuda_ok(cudaMemcpyAsync(g->in_col.p, sorted_vals, (size_t)nnz * sizeof(int32_t),
+                                                             cudaMemcpyDeviceToDevice, s), "inbound sources")))
+                    return rc;
+            } else {
+                k_expand_src<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, n, src);
+                if (nnz > 0)
+                    k_gather_inbound<<<grid_for(nnz), kThreads, 0, s>>>(sorted_vals, nnz, src, dW,
+                                                                       g->in_col.as<int32_t>(), g->in_w.as<float>());
+            }
         }
         // Hubs: the min(n, kHubCap) sources of largest out-degree (a multiple of 4,
         // the granule of the shared-memory staging copy).
