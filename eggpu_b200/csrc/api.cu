@@ -485,7 +485,7 @@ static uint64_t bits_of(double x) {
 int64_t egpr_graph::device_bytes() const {
     return (int64_t)(in_row.bytes + in_col.bytes + in_w.bytes + outw.bytes + dangling01.bytes +
                      sw_row.bytes + sw_col.bytes + sw_w.bytes + tile_bits.bytes + tile_row.bytes +
-                     hub_ids.bytes + hub_slot.bytes + hubz.bytes + plan.d_acc.bytes + plan.d_span_acc.bytes + plan.d_span_cnt.bytes +
+                     hub_ids.bytes + hub_slot.bytes + hubz.bytes + hubz64.bytes + plan.d_acc.bytes + plan.d_span_acc.bytes + plan.d_span_cnt.bytes +
                      plan.d_span_list.bytes +
                      scale.bytes + tele.bytes + x0.bytes + x1.bytes + z0.bytes + z1.bytes + out.bytes + z64.bytes +
                      plan.d_chunks.bytes + plan.d_graphs.bytes + plan.d_states.bytes + plan.d_ndang.bytes +
@@ -505,7 +505,7 @@ static void destroy_graph_object(egpr_graph* g) {
     g->plan.release();
     for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sw_row,
                       &g->sw_col, &g->sw_w, &g->tile_bits, &g->tile_row,
-                      &g->hub_ids, &g->hub_slot, &g->hubz, &g->scale, &g->tele, &g->seed_ids,
+                      &g->hub_ids, &g->hub_slot, &g->hubz, &g->hubz64, &g->scale, &g->tele, &g->seed_ids,
                       &g->x0, &g->x1, &g->z0, &g->z1, &g->out, &g->z64})
         b->release();
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -655,6 +655,7 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
     if ((rc = g->scale.alloc(nf)) || (rc = g->tele.alloc(nf)) || (rc = g->x0.alloc(nf)) || (rc = g->x1.alloc(nf)) ||
         (rc = g->z0.alloc(2 * nf)) || (rc = g->out.alloc(nd)) || (rc = g->z64.alloc(nd + sizeof(double))) ||
         (rc = g->hubz.alloc(2 * (size_t)hub_stride(g->nhub) * sizeof(float))) ||
+        (rc = g->hubz64.alloc(((size_t)g->nhub + 1) * sizeof(double))) ||
         // zero slots: hubz[.][nhub] and z64[n] are read by placeholder entries
         (rc = (cudaMemsetAsync(g->hubz.p, 0, g->hubz.bytes, g->own_stream) == cudaSuccess &&
                cudaMemsetAsync(g->z64.p, 0, g->z64.bytes, g->own_stream) == cudaSuccess)

@@ -72,6 +72,7 @@ struct GraphDev {
     const int32_t* hub_ids;  // nhub source ids of the hub slots
     const int32_t* hub_slot; // n, slot of each vertex or -1
     float* hubz[2];          // nhub carried values of the hubs, double-buffered with z
+    double* hubz64;          // nhub + 1: the hubs' FP64 carried values for the correction sweep (slot nhub = 0)
     int32_t nhub;
     int32_t n;
     int32_t chunk_begin;     // this graph's global chunk id range
@@ -190,7 +191,7 @@ struct egpr_graph {
     int32_t n_dangling_solve = 0;  // out-weight <= 1e-15 (EasyGraph CPU rule)
     double prep_seconds = 0.0;
     // prepared graph
-    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, hub_ids, hub_slot, hubz;
+    egpr::DevBuf in_row, in_col, in_w, outw, dangling01, hub_ids, hub_slot, hubz, hubz64;
     // the sweep's layout (see build_sweep_layout)
     egpr::DevBuf sw_row, sw_col, sw_w, tile_bits, tile_row;
     int64_t sw_nnz = 0;

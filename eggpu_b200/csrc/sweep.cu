@@ -293,6 +293,7 @@ struct WarpCtx {
     const float* zsrc;      // carried values read by this sweep
     const float* hub_g;     // their hub copy (global)
     const double* z64;
+    const double* hubz64;    // the hubs' FP64 carried values (correction sweep)
     const int32_t* hub_ids;
     int32_t graph;
     int32_t iter;
@@ -368,7 +369,7 @@ __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, 
         // copy (predicated pair); a graph whose hubs are not all staged reads
         // the rest of them from its global hub copy.
         auto carried = [&](int32_t s) -> Real {
-            if (kFinal) return X.z64[s >= 0 ? s : __ldg(X.hub_ids + (-s - 1))];
+            if (kFinal) return s >= 0 ? X.z64[s] : X.hubz64[-s - 1];
             float x;
             if (hubs_local) {
                 if (s >= 0) x = __ldg(zsrc + s);
@@ -572,6 +573,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_sweep(SweepParams P) {
                         X.zsrc = G.z[iter & 1];
                         X.hub_g = G.hubz[iter & 1];
                         X.z64 = G.z64;
+                        X.hubz64 = G.hubz64;
                         X.hub_ids = G.hub_ids;
                         X.hub_slots = G.nhub + 1;
                         X.graph = gi;
@@ -693,6 +695,18 @@ __global__ void k_prep_z64(const GraphDev* graphs, const GraphState* states, int
          u += (int64_t)gridDim.x * blockDim.x) {
         const double o = G.outw[u];
         G.z64[u] = o <= 1e-15 ? 0.0 : alpha * (double)xp[u] / o;
+    }
+    // the hubs' copy, by slot (the same value, so a hub entry reads one word
+    // instead of its slot's id and then the value); slot nhub is the zero slot
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h <= G.nhub;
+         h += (int64_t)gridDim.x * blockDim.x) {
+        double z = 0.0;
+        if (h < G.nhub) {
+            const int32_t u = G.hub_ids[h];
+            const double o = G.outw[u];
+            z = o <= 1e-15 ? 0.0 : alpha * (double)xp[u] / o;
+        }
+        G.hubz64[h] = z;
     }
 }
 
@@ -884,6 +898,7 @@ GraphDev graph_dev_view(const egpr_graph* g) {
     d.hub_slot = g->hub_slot.as<int32_t>();
     d.hubz[0] = g->hubz.as<float>();
     d.hubz[1] = g->hubz.as<float>() + hub_stride(g->nhub);
+    d.hubz64 = g->hubz64.as<double>();
     d.nhub = g->nhub;
     d.n = g->n;
     d.chunk_begin = d.chunk_end = 0;
