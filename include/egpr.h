@@ -106,7 +106,8 @@ EGPR_API const char* egpr_last_error(void);
 /*
  * Uploads an out-edge CSR and prepares it on the current device: FP64
  * out-weight sums, inbound CSR with entries in ascending source order,
- * dangling mask, merge-path work tiles.  Replaces the host-side
+ * dangling mask, and the sweep's layout (rows padded to end on an entry of
+ * their own, 256-entry warp tiles, cost-balanced chunks).  Replaces the host-side
  * build_inbound_from_csr + H2D of pagerank.cu:286-347,472-518, done on the
  * GPU.  V[n+1] must be non-decreasing with V[0]==0 and V[n]==m (the CSR the
  * reference's gen_CSR / load_csr_files produce); destinations outside [0,n)
