@@ -172,7 +172,7 @@ def test_bulk_manifest_roundtrip_and_validation(tmp_path):
     meta["format"] = "bogus"
     bad = tmp_path / "bad.json"
     bad.write_text(json.dumps(meta))
-    with pytest.raises(ValueError, match="unsupported CSR artifact format"):
+    with pytest.raises(ValueError, match="unsupported EGGPU CSR format"):
         bulk.read_eggpu_csr(bad)
     with pytest.raises(ValueError, match="endpoint is outside"):
         bulk.BulkCSRGraph(V, np.array([1, 5, 0], np.int32))
@@ -183,6 +183,131 @@ def test_bulk_manifest_roundtrip_and_validation(tmp_path):
     p = backend.prepare_graph_context(G)
     assert p["bulk_csr"] and p["nodes"] == range(3)
     assert backend.prepare_graph_context(G) is p
+
+
+# the six-node graph of the reference's bulk tests (tests/test_eggpu_bulk_csr.py:12-61)
+_BULK_EDGES = [(0, 1), (1, 2), (2, 0), (2, 3), (3, 4), (4, 5), (5, 3)]
+
+
+def _write_reference_style_bulk(tmp_path, directed=False, weighted=False):
+    """The artifact the reference's test writer produces, written here with the array module as it does."""
+    from array import array
+
+    rows = [[] for _ in range(6)]
+    for u, v in _BULK_EDGES:
+        rows[u].append(v)
+        if not directed:
+            rows[v].append(u)
+    offsets, indices = [0], []
+    for row in rows:
+        indices.extend(row)
+        offsets.append(len(indices))
+    with (tmp_path / "tiny.offsets.i32").open("wb") as f:
+        array("i", offsets).tofile(f)
+    with (tmp_path / "tiny.indices.i32").open("wb") as f:
+        array("i", indices).tofile(f)
+    meta = {"format": "eggpu-csr-v1", "generation": 1, "name": "tiny", "directed": directed, "num_nodes": 6,
+            "num_edges": len(_BULK_EDGES), "num_entries": len(indices), "node_labels": "zero_based_contiguous",
+            "offset_dtype": "int32", "index_dtype": "int32", "offsets_path": "tiny.offsets.i32",
+            "indices_path": "tiny.indices.i32"}
+    if weighted:
+        weights = [1.0 + ((src * dst) % 6) for src, row in enumerate(rows) for dst in row]
+        with (tmp_path / "tiny.weights.f64").open("wb") as f:
+            array("d", weights).tofile(f)
+        meta.update(weights_path="tiny.weights.f64", weight_dtype="float64", weight_key="weight")
+    path = tmp_path / "tiny.json"
+    path.write_text(json.dumps(meta), encoding="utf-8")
+    return path, meta
+
+
+def test_bulk_graph_contract_as_the_reference_pins_it(tmp_path):
+    # tests/test_eggpu_bulk_csr.py:188-195 and :256-262
+    path, _ = _write_reference_style_bulk(tmp_path)
+    G = bulk.read_eggpu_csr(path)
+    assert isinstance(G, bulk.EGGPUBulkGraph)
+    assert len(G) == 6 and G.number_of_edges() == 7 and list(G.nodes) == list(range(6))
+    assert G.memory_estimate()["host_total_bytes"] == (7 + 14) * 4
+    assert "materialize" not in repr(G) and repr(G).startswith("EGGPUBulkGraph(name='tiny'")
+    assert 5 in G and 6 not in G and "a" not in G and G.has_node(0) and list(G) == list(range(6))
+    assert G.copy() is G and not G.is_directed() and G.weight_key is None
+    with pytest.raises(TypeError, match="immutable"):
+        G.add_edge(0, 5)
+    with pytest.raises(NotImplementedError, match="does not materialize"):
+        G.adj
+    with pytest.raises(NotImplementedError, match="per-pair"):
+        G.number_of_edges(0, 1)
+
+    wdir = tmp_path / "w"
+    wdir.mkdir()
+    Gw = bulk.read_eggpu_csr(_write_reference_style_bulk(wdir, weighted=True)[0])
+    est = Gw.memory_estimate()
+    assert est["implicit_unit_weights"] is False and est["host_weights_bytes"] == Gw.num_entries * 8
+    assert est["host_total_bytes"] == (7 + 14) * 4 + 14 * 8 and Gw.weight_key == "weight"
+    assert Gw.has_weight("weight") and not Gw.has_weight("cost")
+    # the signature follows the manifest path and generation, not the array bytes
+    assert Gw._eggpu_bulk_signature[:2] == (str(Gw.metadata_path), 1)
+
+
+def test_bulk_manifest_checks_match_the_reference_messages(tmp_path, monkeypatch):
+    # easygraph/classes/eggpu_bulk_graph.py:200-247 and graph_convert.cpp:447-516
+    path, meta = _write_reference_style_bulk(tmp_path, weighted=True)
+
+    def load_with(**changes):
+        m = dict(meta)
+        for k, v in changes.items():
+            if v is None:
+                m.pop(k, None)
+            else:
+                m[k] = v
+        p = tmp_path / "variant.json"
+        p.write_text(json.dumps(m), encoding="utf-8")
+        return bulk.read_eggpu_csr(p)
+
+    with pytest.raises(ValueError, match="requires int32 offsets and int32 indices"):
+        load_with(offset_dtype=None)
+    with pytest.raises(ValueError, match="requires int32 offsets and int32 indices"):
+        load_with(index_dtype="int64")
+    with pytest.raises(ValueError, match="zero-based contiguous node labels"):
+        load_with(node_labels=None)
+    with pytest.raises(ValueError, match="num_nodes exceeds the signed 32-bit EGGPU CSR limit"):
+        load_with(num_nodes=2**31 - 1)
+    with pytest.raises(ValueError, match="num_entries exceeds the signed 32-bit EGGPU CSR limit"):
+        load_with(num_entries=-1)
+    with pytest.raises(ValueError, match="offset file size mismatch: expected 32, found 28"):
+        load_with(num_nodes=7)
+    with pytest.raises(ValueError, match="index file size mismatch: expected 60, found 56"):
+        load_with(num_entries=15)
+    with pytest.raises(ValueError, match="explicit weights require float64"):
+        load_with(weight_dtype=None)
+    with pytest.raises(ValueError, match="weight_key must be non-empty"):
+        load_with(weight_key="")
+    # contents: offsets that do not end at num_entries, out-of-range endpoints, non-finite weights
+    idx = np.fromfile(tmp_path / "tiny.indices.i32", dtype=np.int32)
+    bad = idx.copy()
+    bad[3] = 6
+    bad.tofile(tmp_path / "bad.indices.i32")
+    with pytest.raises(ValueError, match=r"endpoint is outside \[0, num_nodes\)"):
+        load_with(indices_path="bad.indices.i32")
+    # EASYGRAPH_GPU_BULK_VALIDATE: only 1/TRUE/ON/YES (default TRUE) validate the contents
+    monkeypatch.setenv("EASYGRAPH_GPU_BULK_VALIDATE", "FALSE")
+    assert len(load_with(indices_path="bad.indices.i32")) == 6
+    monkeypatch.setenv("EASYGRAPH_GPU_BULK_VALIDATE", "maybe")
+    assert len(load_with(indices_path="bad.indices.i32")) == 6
+    monkeypatch.delenv("EASYGRAPH_GPU_BULK_VALIDATE")
+    with pytest.raises(ValueError, match="endpoint is outside"):
+        load_with(indices_path="bad.indices.i32")
+    w = np.fromfile(tmp_path / "tiny.weights.f64", dtype=np.float64)
+    w[0] = np.inf
+    w.tofile(tmp_path / "bad.weights.f64")
+    with pytest.raises(ValueError, match="bulk CSR weights must be finite"):
+        load_with(weights_path="bad.weights.f64")
+    off = np.fromfile(tmp_path / "tiny.offsets.i32", dtype=np.int32)
+    off[-1] = 13
+    off.tofile(tmp_path / "bad.offsets.i32")
+    with pytest.raises(ValueError, match="final offset must equal num_entries"):
+        load_with(offsets_path="bad.offsets.i32")
+    # absolute paths are taken as they are
+    assert len(load_with(offsets_path=str(tmp_path / "tiny.offsets.i32"))) == 6
 
 
 def test_install_hook_with_fake_easygraph(monkeypatch):
