@@ -192,6 +192,41 @@ def is_bulk_graph(G):
     return bool(getattr(G, "_eggpu_bulk_csr", False))
 
 
+def bulk_weight_available(G, weight):
+    """Whether a bulk graph carries edge attribute ``weight``: its own answer
+    (eggpu_b200.bulk graphs), else the reference's rule for its
+    EGGPUBulkGraph, a weights file under that key
+    (easygraph/utils/gpu_eggpu_backend.py:120-126)."""
+    if weight is None or not is_bulk_graph(G):
+        return False
+    if hasattr(G, "has_weight"):
+        return bool(G.has_weight(weight))
+    return getattr(G, "weights_path", None) is not None and getattr(G, "weight_key", None) == str(weight)
+
+
+def _bulk_csr(G, weight):
+    """(V, E, W) of a bulk graph: the arrays of an eggpu_b200.bulk graph, or
+    the artifact files of the reference's EGGPUBulkGraph, which keeps them
+    in its C++ graph and exposes only their paths."""
+    if hasattr(G, "csr_arrays"):
+        return G.csr_arrays(weight)
+    if weight is not None and not bulk_weight_available(G, weight):
+        raise NotImplementedError(
+            f"weighted PageRank requires an EGGPU CSR artifact containing the {weight!r} edge attribute")
+    n, m = int(G.num_nodes), int(G.num_entries)
+
+    def read(path, dtype, count):
+        arr = np.fromfile(path, dtype=dtype)
+        if arr.shape[0] != count:
+            raise ValueError(f"{path}: expected {count} values of {np.dtype(dtype).name}, found {arr.shape[0]}")
+        return arr
+
+    V = read(G.offsets_path, np.int32, n + 1)
+    E = read(G.indices_path, np.int32, m)
+    W = read(G.weights_path, np.float64, m) if weight is not None else None
+    return V, E, W
+
+
 def _adj_dict(G):
     adj = getattr(G, "_adj", None)
     if adj is None:
@@ -305,7 +340,7 @@ def graph_csr(G, prepared, weight=None):
     adjacency dicts runs in native code when the extension is built.
     """
     if is_bulk_graph(G):
-        return G.csr_arrays(weight)
+        return _bulk_csr(G, weight)
     if _graph_walk is not None:
         adj = _adj_dict(G)
         index = prepared["node_to_idx"]
@@ -431,7 +466,7 @@ def _personalization_vector(personalization, prepared):
 
 def pagerank(G, alpha=0.85, max_iter=200, eps=1e-6, weight=None, personalization=None):
     prepared = prepare_graph_context(G)
-    if prepared.get("bulk_csr") and weight is not None and not G.has_weight(weight):
+    if prepared.get("bulk_csr") and weight is not None and not bulk_weight_available(G, weight):
         raise NotImplementedError(
             f"weighted PageRank requires an EGGPU CSR artifact containing the {weight!r} edge attribute")
     nodes = prepared["nodes"]

@@ -310,6 +310,56 @@ def test_bulk_manifest_checks_match_the_reference_messages(tmp_path, monkeypatch
     assert len(load_with(offsets_path=str(tmp_path / "tiny.offsets.i32"))) == 6
 
 
+class _ReferenceStyleBulk:
+    """The attributes the reference's EGGPUBulkGraph exposes after loading
+    (easygraph/classes/eggpu_bulk_graph.py:296-333): artifact paths and
+    sizes, no arrays (those live in its C++ graph)."""
+
+    _eggpu_bulk_csr = True
+
+    def __init__(self, path, meta):
+        base = path.parent
+        self.num_nodes, self.num_entries = meta["num_nodes"], meta["num_entries"]
+        self.offsets_path = base / meta["offsets_path"]
+        self.indices_path = base / meta["indices_path"]
+        self.weights_path = base / meta["weights_path"] if "weights_path" in meta else None
+        self.weight_key = meta.get("weight_key", "weight") if self.weights_path else None
+        self._directed = meta["directed"]
+        self._eggpu_bulk_signature = (str(path), meta["generation"], self.num_nodes, self.num_entries,
+                                      self._directed, None, 0)
+        self.nodes = range(self.num_nodes)
+        self.cache = {}
+
+    def is_directed(self):
+        return self._directed
+
+    def is_multigraph(self):
+        return False
+
+    def __len__(self):
+        return self.num_nodes
+
+
+def test_backend_reads_the_reference_bulk_graph_from_its_artifact(tmp_path):
+    path, meta = _write_reference_style_bulk(tmp_path, directed=True, weighted=True)
+    ours = bulk.read_eggpu_csr(path)
+    theirs = _ReferenceStyleBulk(path, meta)
+    p = backend.prepare_graph_context(theirs)
+    assert p["bulk_csr"] and p["nodes"] == range(6) and backend.prepare_graph_context(theirs) is p
+    for weight in (None, "weight"):
+        a, b = backend.graph_csr(theirs, p, weight), ours.csr_arrays(weight)
+        assert all((x is None and y is None) or np.array_equal(x, y) for x, y in zip(a, b))
+    assert backend.bulk_weight_available(theirs, "weight") and not backend.bulk_weight_available(theirs, "cost")
+    assert backend.bulk_weight_available(ours, "weight") and not backend.bulk_weight_available(ours, "cost")
+    with pytest.raises(NotImplementedError, match="weighted PageRank requires an EGGPU CSR artifact"):
+        backend.graph_csr(theirs, p, "cost")
+    udir = tmp_path / "u"
+    udir.mkdir()
+    upath, umeta = _write_reference_style_bulk(udir)
+    with pytest.raises(NotImplementedError, match="weighted PageRank requires an EGGPU CSR artifact"):
+        backend.pagerank(_ReferenceStyleBulk(upath, umeta), weight="weight")
+
+
 def test_install_hook_with_fake_easygraph(monkeypatch):
     import sys
 
