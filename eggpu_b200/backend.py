@@ -57,6 +57,20 @@ def _env_int(name, default, lo):
 _GRAPH_CTX_VALIDATE_EVERY = _env_int("EASYGRAPH_GPU_CTX_VALIDATE_EVERY", 32, 1)
 
 
+def _env_flag(name, default):
+    return os.environ.get(name, default).strip().upper() in {"1", "TRUE", "ON", "YES"}
+
+
+# Opt-in result cache, per prepared graph context (easygraph/utils/
+# gpu_eggpu_backend.py:13-30,1723-1779): off unless EASYGRAPH_GPU_RESULT_CACHE
+# is set; at most MAX_ITEMS results per graph, none for graphs above MAX_NODES
+# nodes (0 = no limit); a hit hands out a copy unless RETURN_COPY is off.
+_RESULT_CACHE_ENABLED = _env_flag("EASYGRAPH_GPU_RESULT_CACHE", "FALSE")
+_RESULT_CACHE_RETURN_COPY = _env_flag("EASYGRAPH_GPU_RESULT_CACHE_RETURN_COPY", "TRUE")
+_RESULT_CACHE_MAX_ITEMS = _env_int("EASYGRAPH_GPU_RESULT_CACHE_MAX_ITEMS", 8, 1)
+_RESULT_CACHE_MAX_NODES = _env_int("EASYGRAPH_GPU_RESULT_CACHE_MAX_NODES", 2_000_000, 0)
+
+
 def set_last_kernel_time(key, seconds):
     if seconds is None:
         _LAST_KERNEL_SECONDS.pop(key, None)
@@ -171,6 +185,55 @@ class DenseValueDict(Mapping):
         if len(self._nodes) > 1000:
             return f"{type(self).__name__}(nodes={len(self._nodes)}, dtype=float64)"
         return repr(self.copy())
+
+
+# ---------------------------------------------------------- result cache --
+def _cache_key(name, *parts):
+    """Cache key of a solve; floats rounded to 12 digits (gpu_eggpu_backend.py:1723-1730)."""
+    return (name,) + tuple(round(float(p), 12) if isinstance(p, float) else p for p in parts)
+
+
+def _allow_result_cache(prepared):
+    if not _RESULT_CACHE_ENABLED:
+        return False
+    nodes = prepared.get("nodes")
+    if nodes is None:
+        return False
+    return not (_RESULT_CACHE_MAX_NODES > 0 and len(nodes) > _RESULT_CACHE_MAX_NODES)
+
+
+def _copy_for_return(result):
+    if not _RESULT_CACHE_RETURN_COPY:
+        return result
+    if isinstance(result, DenseValueDict):
+        return DenseValueDict(result._nodes, result.to_numpy(copy=True), node_to_idx=result._node_to_idx)
+    import copy
+
+    return copy.deepcopy(result)
+
+
+def _result_cache_get(prepared, key):
+    cache = prepared.get("result_cache")
+    if not isinstance(cache, dict):
+        return None
+    entry = cache.get(key)
+    if entry is None:
+        return None
+    return _copy_for_return(entry["result"]), entry["kernel"]
+
+
+def _result_cache_put(prepared, key, result, kernel):
+    """Stores a private snapshot of result under key, least recently stored out first."""
+    if not _allow_result_cache(prepared):
+        return
+    cache = prepared.setdefault("result_cache", {})
+    order = prepared.setdefault("result_cache_order", [])
+    cache[key] = {"result": _copy_for_return(result), "kernel": kernel}
+    if key in order:
+        order.remove(key)
+    order.append(key)
+    while len(order) > _RESULT_CACHE_MAX_ITEMS:
+        cache.pop(order.pop(0), None)
 
 
 # ------------------------------------------------------- prepared context --
@@ -469,6 +532,15 @@ def pagerank(G, alpha=0.85, max_iter=200, eps=1e-6, weight=None, personalization
     if prepared.get("bulk_csr") and weight is not None and not bulk_weight_available(G, weight):
         raise NotImplementedError(
             f"weighted PageRank requires an EGGPU CSR artifact containing the {weight!r} edge attribute")
+    # personalised solves are not cached: their key would be the whole vector
+    key = None
+    if personalization is None:
+        key = _cache_key("pagerank", bool(prepared["directed"]), float(alpha), int(max_iter), float(eps), str(weight))
+        cached = _result_cache_get(prepared, key)
+        if cached is not None:
+            result, kernel_s = cached
+            set_last_kernel_time("pagerank", kernel_s)
+            return result
     nodes = prepared["nodes"]
     if len(nodes) == 0:
         set_last_kernel_time("pagerank", 0.0)
@@ -479,7 +551,10 @@ def pagerank(G, alpha=0.85, max_iter=200, eps=1e-6, weight=None, personalization
     vals = normalize_dense_array(out["values_dense"], len(nodes), allow_leading_sentinel=True,
                                  result_name="PageRank values_dense")
     set_last_kernel_time("pagerank", out["kernel_seconds"])
-    return DenseValueDict(nodes, vals, node_to_idx=prepared.get("node_to_idx"))
+    result = DenseValueDict(nodes, vals, node_to_idx=prepared.get("node_to_idx"))
+    if key is not None:
+        _result_cache_put(prepared, key, result, out["kernel_seconds"])
+    return result
 
 
 def pagerank_batch(G, personalizations, alpha=0.85, max_iter=200, eps=1e-6, weight=None):

@@ -360,6 +360,70 @@ def test_backend_reads_the_reference_bulk_graph_from_its_artifact(tmp_path):
         backend.pagerank(_ReferenceStyleBulk(upath, umeta), weight="weight")
 
 
+def test_opt_in_result_cache_owns_independent_snapshots(monkeypatch):
+    # test_eggpu_cache_contracts.py:284-307, on this backend's cache
+    monkeypatch.setattr(backend, "_RESULT_CACHE_ENABLED", True)
+    monkeypatch.setattr(backend, "_RESULT_CACHE_RETURN_COPY", True)
+    prepared = {"nodes": [0], "result_cache": {}, "result_cache_order": []}
+    original = {0: [1]}
+    key = ("test",)
+    backend._result_cache_put(prepared, key, original, 0.25)
+    original[0].append(2)
+    first, kernel = backend._result_cache_get(prepared, key)
+    first[0].append(3)
+    second, _ = backend._result_cache_get(prepared, key)
+    assert kernel == 0.25 and first == {0: [1, 3]} and second == {0: [1]}
+    # a dense result comes back over an array of its own
+    dense = backend.DenseValueDict(range(3), np.array([0.2, 0.3, 0.5]))
+    backend._result_cache_put(prepared, ("dense",), dense, 0.5)
+    a, _ = backend._result_cache_get(prepared, ("dense",))
+    b, _ = backend._result_cache_get(prepared, ("dense",))
+    assert a == dense and b == dense and a is not b and a.to_numpy() is not b.to_numpy()
+
+
+def test_result_cache_is_opt_in_bounded_and_keyed_like_the_reference(monkeypatch):
+    prepared = {"nodes": list(range(4))}
+    backend._result_cache_put(prepared, ("k",), {0: 1}, 0.1)
+    assert backend._result_cache_get(prepared, ("k",)) is None  # off by default
+    monkeypatch.setattr(backend, "_RESULT_CACHE_ENABLED", True)
+    monkeypatch.setattr(backend, "_RESULT_CACHE_MAX_ITEMS", 2)
+    for i in range(3):
+        backend._result_cache_put(prepared, ("k", i), {0: i}, float(i))
+    assert backend._result_cache_get(prepared, ("k", 0)) is None
+    assert backend._result_cache_get(prepared, ("k", 2)) == ({0: 2}, 2.0)
+    monkeypatch.setattr(backend, "_RESULT_CACHE_MAX_NODES", 3)
+    backend._result_cache_put(prepared, ("big",), {0: 1}, 0.1)
+    assert backend._result_cache_get(prepared, ("big",)) is None
+    # floats rounded to 12 digits, other parts kept (gpu_eggpu_backend.py:1723-1730)
+    assert backend._cache_key("pagerank", True, 0.85 + 1e-15, 100, 1e-6, "None") == \
+        ("pagerank", True, 0.85, 100, 1e-6, "None")
+
+
+def test_pagerank_result_cache_hits_skip_the_solve(monkeypatch):
+    calls = []
+
+    def fake_dense(pg, alpha, max_iter, eps, weight=None, personalization=None):
+        calls.append((alpha, personalization is not None))
+        return {"values_dense": np.full(3, 1.0 / 3.0), "kernel_seconds": 0.125}
+
+    monkeypatch.setattr(backend, "prepared_native", lambda G, prepared, weight=None: object())
+    monkeypatch.setattr(backend, "cpp_gpu_pagerank_dense", fake_dense)
+    monkeypatch.setattr(backend, "_RESULT_CACHE_ENABLED", True)
+    G = DiGraph()
+    G.add_edges_from([(0, 1), (1, 2), (2, 0)])
+    r1 = backend.pagerank(G, alpha=0.85, max_iter=100, eps=1e-6)
+    r2 = backend.pagerank(G, alpha=0.85, max_iter=100, eps=1e-6)
+    assert len(calls) == 1 and r1 == r2 and r1 is not r2
+    assert backend.get_last_kernel_time("pagerank") == 0.125
+    backend.pagerank(G, alpha=0.9, max_iter=100, eps=1e-6)  # another alpha: another key
+    backend.pagerank(G, alpha=0.85, max_iter=100, eps=1e-6, personalization={0: 1.0})  # never cached
+    backend.pagerank(G, alpha=0.85, max_iter=100, eps=1e-6, personalization={0: 1.0})
+    assert [c[0] for c in calls] == [0.85, 0.9, 0.85, 0.85]
+    G.add_edge(2, 1)  # a mutation drops the graph context and its results
+    backend.pagerank(G, alpha=0.85, max_iter=100, eps=1e-6)
+    assert len(calls) == 5
+
+
 def test_install_hook_with_fake_easygraph(monkeypatch):
     import sys
 
