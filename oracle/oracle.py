@@ -6,7 +6,7 @@ was built, to the reference's own compiled PageRank translation unit
 (oracle/_ref/libref_pagerank.so, recipe oracle/Makefile.ref).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
-legs use this module, always as the checker or as the timed CPU baseline.  The
+legs use this module, always to check results or as the timed CPU baseline.  The
 engine in eggpu_b200/ never imports it.
 
 Reference functions restated (paths relative to the reference project root):

@@ -2,8 +2,8 @@
  * ORACLE — test infrastructure only.
  *
  * A plain-C restatement of the reference's PageRank arithmetic, used by the
- * tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the
- * CHECKER (and as the timed CPU port of the reference's OpenMP path).  The
+ * tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg to CHECK
+ * RESULTS (and as the timed CPU port of the reference's OpenMP path).  The
  * product path (eggpu_b200/) never links, loads or calls anything here.
  *
  * Functions and the reference code each one restates (paths are relative to

@@ -268,7 +268,7 @@ def test_undirected_and_bulk_paths_agree(tmp_path):
 
 
 def test_scale22_full_size_properties_and_parity():
-    # R-MAT scale 22, seed 1, reference stop rule -> one sweep at this size
+    # the scale-22 workload: R-MAT scale 22, seed 1, reference stop rule -> one sweep at this size
     g = synth.rmat(scale=22, edgefactor=16, seed=1)
     pg = _native.PreparedGraph(g.V, g.E)
     ranks, stats = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
@@ -375,7 +375,7 @@ def test_ppr_through_the_api_batch():
 
 
 def test_ppr_config_full_size_k256_rmat20():
-    # configs[4a]: R-MAT scale 20, seed 3, k = 256 seed sets of 1-64 vertices, at full size
+    # the batched PPR workload: R-MAT scale 20, seed 3, k = 256 seed sets of 1-64 vertices, at full size
     g = synth.rmat(scale=20, edgefactor=16, seed=3)
     sets = synth.seed_sets(g.n, 256, 1, 64, seed=3)
     pg = _native.PreparedGraph(g.V, g.E)
@@ -391,7 +391,8 @@ def test_ppr_config_full_size_k256_rmat20():
 
 
 def test_many_graphs_config_full_size_512_er():
-    # configs[4b]: 512 directed Erdos-Renyi graphs (n log-uniform in [1e3, 2e5], mean out-degree U[8, 32])
+    # the many-graphs workload: 512 directed Erdos-Renyi graphs (n log-uniform in [1e3, 2e5], mean
+    # out-degree U[8, 32])
     rng = np.random.Generator(np.random.PCG64(1000))
     ns = np.exp(rng.uniform(np.log(1e3), np.log(2e5), size=512)).astype(np.int64)
     ds = rng.uniform(8.0, 32.0, size=512)
