@@ -100,7 +100,8 @@ def install():
       * easygraph.utils.gpu_eggpu_backend.pagerank(G, alpha, max_iter, eps, weight)
       * easygraph.functions.centrality.pagerank.pagerank and easygraph.pagerank,
         wrapped to accept ``personalization`` and to use this engine when
-        EASYGRAPH_ENABLE_GPU is on (easygraph's own CPU code otherwise).
+        EASYGRAPH_ENABLE_GPU is on (easygraph's own CPU code otherwise; C++
+        graphs keep easygraph's routing to its C++ CPU PageRank).
     """
     try:
         import easygraph as eg  # type: ignore
@@ -116,6 +117,12 @@ def install():
         return backend.pagerank(G, alpha=alpha, max_iter=max_iter, eps=eps, weight=weight)
 
     def eg_pagerank(G, alpha=0.85, weight=None, max_iter=None, tol=None, personalization=None):
+        # C++ graphs (cflag) keep the reference's routing to cpp_pagerank
+        # through its hybrid decorator (easygraph/utils/decorators.py:140-163),
+        # with the GPU switch on or off; only a personalised solve, which that
+        # path does not offer, comes to this engine.
+        if getattr(G, "cflag", 0) and personalization is None:
+            return original(G, alpha=alpha, weight=weight, max_iter=max_iter, tol=tol)
         if gpu_runtime_enabled():
             return pagerank(G, alpha=alpha, weight=weight, max_iter=max_iter, tol=tol,
                             personalization=personalization)

@@ -458,3 +458,12 @@ def test_install_hook_with_fake_easygraph(monkeypatch):
     assert seen["alpha"] == 0.6 and seen["personalization"] == {0: 1.0}
     assert fake_backend.pagerank(G, alpha=0.7, max_iter=3, eps=1e-3) == {"ok": 1}
     assert seen["max_iter"] == 3 and seen["eps"] == 1e-3
+    # a C++ graph (cflag) keeps easygraph's own routing (hybrid -> cpp_pagerank) unless personalised
+    GC = DiGraph()
+    GC.add_edge(0, 1)
+    GC.cflag = 1
+    calls.clear()
+    seen.clear()
+    fake_eg.pagerank(GC, alpha=0.4, max_iter=7)
+    assert calls["cpu"]["alpha"] == 0.4 and calls["cpu"]["max_iter"] == 7 and not seen
+    assert fake_eg.pagerank(GC, alpha=0.3, personalization={0: 1.0}) == {"ok": 1} and seen["alpha"] == 0.3
