@@ -70,6 +70,14 @@ _RESULT_CACHE_RETURN_COPY = _env_flag("EASYGRAPH_GPU_RESULT_CACHE_RETURN_COPY", 
 _RESULT_CACHE_MAX_ITEMS = _env_int("EASYGRAPH_GPU_RESULT_CACHE_MAX_ITEMS", 8, 1)
 _RESULT_CACHE_MAX_NODES = _env_int("EASYGRAPH_GPU_RESULT_CACHE_MAX_NODES", 2_000_000, 0)
 
+# The reference's cache and result-format switches (gpu_eggpu_backend.py:40-75):
+# no graph context kept in G.cache, no prepared device graph kept in G.cache,
+# and PageRank results as plain dicts instead of the dense read-only mapping
+# (EASYGRAPH_GPU_PR_PREFER_CPP_DICT, defaulting to EASYGRAPH_GPU_PREFER_CPP_DICT).
+_GRAPH_CONTEXT_CACHE_DISABLED = _env_flag("EASYGRAPH_GPU_DISABLE_GRAPH_CONTEXT_CACHE", "")
+_NATIVE_GRAPH_CACHE_DISABLED = _env_flag("EASYGRAPH_GPU_DISABLE_CPP_GRAPH_CACHE", "")
+_PR_PREFER_DICT = _env_flag("EASYGRAPH_GPU_PR_PREFER_CPP_DICT", os.environ.get("EASYGRAPH_GPU_PREFER_CPP_DICT", ""))
+
 
 def set_last_kernel_time(key, seconds):
     if seconds is None:
@@ -341,7 +349,7 @@ def prepared_graph_usable(G, prepared):
 
 
 def prepare_graph_context(G):
-    cache = _graph_cache_dict(G)
+    cache = None if _GRAPH_CONTEXT_CACHE_DISABLED else _graph_cache_dict(G)
     prepared = cache.get(_PREPARED_CACHE_KEY) if cache is not None else None
     if prepared is not None and prepared_graph_usable(G, prepared):
         return prepared
@@ -469,7 +477,7 @@ def prepared_native(G, prepared, weight=None):
     """The device-prepared graph for (G, weight), cached in G.cache."""
     from ._native import PreparedGraph
 
-    cache = _graph_cache_dict(G)
+    cache = None if _NATIVE_GRAPH_CACHE_DISABLED else _graph_cache_dict(G)
     key = f"{_NATIVE_CACHE_KEY}:{'directed' if prepared['directed'] else 'undirected'}:{weight!r}"
     if cache is not None:
         hit = cache.get(key)
@@ -552,6 +560,8 @@ def pagerank(G, alpha=0.85, max_iter=200, eps=1e-6, weight=None, personalization
                                  result_name="PageRank values_dense")
     set_last_kernel_time("pagerank", out["kernel_seconds"])
     result = DenseValueDict(nodes, vals, node_to_idx=prepared.get("node_to_idx"))
+    if _PR_PREFER_DICT:
+        result = dict(result.items())
     if key is not None:
         _result_cache_put(prepared, key, result, out["kernel_seconds"])
     return result

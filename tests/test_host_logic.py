@@ -424,6 +424,48 @@ def test_pagerank_result_cache_hits_skip_the_solve(monkeypatch):
     assert len(calls) == 5
 
 
+def test_reference_cache_and_result_format_switches(monkeypatch):
+    # gpu_eggpu_backend.py:40-75: EASYGRAPH_GPU_DISABLE_GRAPH_CONTEXT_CACHE,
+    # EASYGRAPH_GPU_DISABLE_CPP_GRAPH_CACHE and EASYGRAPH_GPU_PR_PREFER_CPP_DICT
+    from eggpu_b200 import _native
+
+    made = []
+
+    class FakePrepared:
+        def __init__(self, V, E, W=None):
+            made.append(len(V) - 1)
+
+    monkeypatch.setattr(_native, "PreparedGraph", FakePrepared)
+    monkeypatch.setattr(backend, "cpp_gpu_pagerank_dense",
+                        lambda pg, a, m, e, w=None, personalization=None: {"values_dense": np.array([0.25, 0.75]),
+                                                                           "kernel_seconds": 0.5})
+    G = DiGraph()
+    G.add_edge("a", "b")
+    r = backend.pagerank(G)
+    assert isinstance(r, backend.DenseValueDict) and r == {"a": 0.25, "b": 0.75}
+    backend.pagerank(G)
+    assert made == [2]  # the prepared graph and the context are kept in G.cache
+    assert backend.prepare_graph_context(G) is backend.prepare_graph_context(G)
+
+    monkeypatch.setattr(backend, "_PR_PREFER_DICT", True)
+    d = backend.pagerank(G)
+    assert type(d) is dict and d == {"a": 0.25, "b": 0.75}
+    d["a"] = 1.0  # a plain dict belongs to the caller
+    assert backend.pagerank(G)["a"] == 0.25
+
+    monkeypatch.setattr(backend, "_NATIVE_GRAPH_CACHE_DISABLED", True)
+    backend.pagerank(G)
+    backend.pagerank(G)
+    assert made == [2, 2, 2]  # prepared again on every call
+
+    H = DiGraph()
+    H.add_edge(0, 1)
+    monkeypatch.setattr(backend, "_GRAPH_CONTEXT_CACHE_DISABLED", True)
+    c1, c2 = backend.prepare_graph_context(H), backend.prepare_graph_context(H)
+    assert c1 is not c2 and c1["nodes"] == c2["nodes"] == [0, 1]
+    assert backend._PREPARED_CACHE_KEY not in H.cache
+
+
 def test_install_hook_with_fake_easygraph(monkeypatch):
     import sys
 
