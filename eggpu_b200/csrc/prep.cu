@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -414,10 +415,16 @@ int radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_
     constexpr int kD = 1 << kBits;
     // warp histograms, tile offsets, digit starts, and the tile's keys and values
     const size_t smem = ((size_t)(kWarps + 2) * kD + 2 * (size_t)kSortTile) * sizeof(uint32_t);
-    static bool attr_set = false;  // per process; the attribute is per function and harmless to repeat
-    if (!attr_set) {
+    // The shared-memory opt-in is a per-device attribute of the function: made
+    // once per device (bit d of the mask; devices past 63 repeat it, which is
+    // harmless).  Atomic: several host threads prepare graphs at once.
+    static std::atomic<uint64_t> attr_devices{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+    const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (!bit || !(attr_devices.load(std::memory_order_relaxed) & bit)) {
         cudaFuncSetAttribute(k_radix_scatter<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
+        attr_devices.fetch_or(bit, std::memory_order_relaxed);
     }
     k_radix_hist<kBits><<<(unsigned)ntiles, kThreads, 0, s>>>(kin, len, shift, ntiles, hist);
     int rc = exclusive_scan_u32(hist, hist, ntiles * kD, s);

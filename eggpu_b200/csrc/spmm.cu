@@ -38,6 +38,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -860,12 +861,13 @@ int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SU
 size_t smem_bytes(bool f64) { return f64 ? sizeof(SpSmem<true>) : sizeof(SpSmem<false>); }
 
 int spmm_grid(bool f64) {
-    static int cached[2][64] = {};
+    static std::atomic<int> cached[2][64];  // per device; host threads may race to fill it with the same value
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    int& c = cached[f64 ? 1 : 0][dev];
-    if (c > 0) return c;
+    std::atomic<int>& c = cached[f64 ? 1 : 0][dev];
+    const int have = c.load(std::memory_order_relaxed);
+    if (have > 0) return have;
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (f64) {
@@ -875,8 +877,9 @@ int spmm_grid(bool f64) {
         cudaFuncSetAttribute(k_spmm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(false));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_spmm<false>, sp_threads<false>(), smem_bytes(false));
     }
-    c = sms * std::max(per, 1);
-    return c;
+    const int grid = sms * std::max(per, 1);
+    c.store(grid, std::memory_order_relaxed);
+    return grid;
 }
 
 }  // namespace

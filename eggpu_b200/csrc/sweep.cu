@@ -42,6 +42,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <type_traits>
 
@@ -742,12 +743,13 @@ int env_int(const char* name, int dflt, int lo, int hi) {
 // one graph) and one tile of row values per warp.  The kernel opts in to the
 // device's limit once per device.
 int smem_optin(int mode) {
-    static int cache[2][64] = {};
+    static std::atomic<int> cache[2][64];  // per device; host threads may race to fill it with the same value
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    int& c = cache[mode ? 1 : 0][dev];
-    if (c > 0) return c;
+    std::atomic<int>& c = cache[mode ? 1 : 0][dev];
+    const int have = c.load(std::memory_order_relaxed);
+    if (have > 0) return have;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa = {};
@@ -759,8 +761,8 @@ int smem_optin(int mode) {
     if (mode == 0) cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     else cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     cudaGetLastError();
-    c = b;
-    return c;
+    c.store(b, std::memory_order_relaxed);
+    return b;
 }
 
 size_t scratch_bytes(int mode) { return (size_t)kCtaWarps * kTileItems * (mode ? sizeof(double) : sizeof(float)); }
@@ -838,16 +840,18 @@ int work_grid(int64_t entries, int full) {
 
 // One persistent CTA per SM.
 int sweep_grid() {
-    static int cache[64] = {};
+    static std::atomic<int> cache[64];  // per device; host threads may race to fill it with the same value
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    if (cache[dev] > 0) return cache[dev];
+    const int have = cache[dev].load(std::memory_order_relaxed);
+    if (have > 0) return have;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaGetLastError();
-    cache[dev] = std::max(1, sms);
-    return cache[dev];
+    const int grid = std::max(1, sms);
+    cache[dev].store(grid, std::memory_order_relaxed);
+    return grid;
 }
 
 // The FP32 carried values z (both buffers, contiguous) are gathered once per
