@@ -422,9 +422,9 @@ int radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
     const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
-    if (!bit || !(attr_devices.load(std::memory_order_relaxed) & bit)) {
+    if (!bit || !(attr_devices.load(std::memory_order_acquire) & bit)) {
         cudaFuncSetAttribute(k_radix_scatter<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_devices.fetch_or(bit, std::memory_order_relaxed);
+        attr_devices.fetch_or(bit, std::memory_order_release);
     }
     k_radix_hist<kBits><<<(unsigned)ntiles, kThreads, 0, s>>>(kin, len, shift, ntiles, hist);
     int rc = exclusive_scan_u32(hist, hist, ntiles * kD, s);

@@ -866,7 +866,7 @@ int spmm_grid(bool f64) {
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
     std::atomic<int>& c = cached[f64 ? 1 : 0][dev];
-    const int have = c.load(std::memory_order_relaxed);
+    const int have = c.load(std::memory_order_acquire);
     if (have > 0) return have;
     int sms = 148, per = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -878,7 +878,7 @@ int spmm_grid(bool f64) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_spmm<false>, sp_threads<false>(), smem_bytes(false));
     }
     const int grid = sms * std::max(per, 1);
-    c.store(grid, std::memory_order_relaxed);
+    c.store(grid, std::memory_order_release);
     return grid;
 }
 

@@ -748,7 +748,7 @@ int smem_optin(int mode) {
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
     std::atomic<int>& c = cache[mode ? 1 : 0][dev];
-    const int have = c.load(std::memory_order_relaxed);
+    const int have = c.load(std::memory_order_acquire);
     if (have > 0) return have;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -761,7 +761,7 @@ int smem_optin(int mode) {
     if (mode == 0) cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     else cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     cudaGetLastError();
-    c.store(b, std::memory_order_relaxed);
+    c.store(b, std::memory_order_release);
     return b;
 }
 
@@ -844,13 +844,13 @@ int sweep_grid() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) dev = 0;
-    const int have = cache[dev].load(std::memory_order_relaxed);
+    const int have = cache[dev].load(std::memory_order_acquire);
     if (have > 0) return have;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaGetLastError();
     const int grid = std::max(1, sms);
-    cache[dev].store(grid, std::memory_order_relaxed);
+    cache[dev].store(grid, std::memory_order_release);
     return grid;
 }
 
