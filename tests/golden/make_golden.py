@@ -2,7 +2,7 @@
 
 Run in a container that has the reference tree (read-only) at REF_ROOT:
 
-    python tests/golden/make_golden.py [REF_ROOT]
+    python tests/golden/make_golden.py [REF_ROOT] [--only small|rmat|config|inbound|ppr]
 
 What it records:
   pagerank_small.json  eg.pagerank results (GPU runtime off, i.e. the
@@ -16,6 +16,11 @@ What it records:
                        cases.
   pagerank_rmat.npz    _pagerank_power_iteration on seeded R-MAT graphs built by
                        eggpu_b200.synth (CSR stored alongside).
+  pagerank_config.npz  _pagerank_power_iteration on the scale-14 workload (R-MAT
+                       scale 14, seed 0, alpha 0.85): its own stop rule (tol
+                       1e-6, max_iter 100) and 20 fixed sweeps.  The graph is
+                       not stored: the test regenerates it with eggpu_b200.synth
+                       and checks it against the SHA-256 recorded here.
   inbound_ref.npz      the reference's compiled build_inbound_from_csr
                        (gpu_easygraph/functions/centrality/pagerank.cu:286-347,
                        via oracle/_ref/libref_pagerank.so) on edge-case CSRs.
@@ -41,7 +46,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 
-REF_ROOT = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+REF_ROOT = Path(sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--") else "/root/reference")
 
 
 def _import_reference():
@@ -211,6 +216,38 @@ def rmat_cases(eg, pr_iter):
     return out
 
 
+def graph_digest(V, E, W=None):
+    """SHA-256 over the CSR arrays (int32 V, int32 E, float64 W if any)."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for a in (np.ascontiguousarray(V, np.int32), np.ascontiguousarray(E, np.int32)) + (
+            () if W is None else (np.ascontiguousarray(W, np.float64),)):
+        h.update(a.tobytes())
+    return h.hexdigest()
+
+
+def config_cases(eg, pr_iter):
+    from eggpu_b200 import synth
+
+    params = dict(scale=14, edgefactor=16, seed=0)
+    csr = synth.rmat(**params)
+    G = eg.DiGraph()
+    G.add_nodes(range(csr.n))
+    G.add_edges([(u, int(csr.E[p])) for u in range(csr.n) for p in range(csr.V[u], csr.V[u + 1])])
+    out, names = {}, []
+    for name, kw in (("rmat14_s0", {"alpha": 0.85, "max_iter": 100, "tol": 1e-6}),
+                     ("rmat14_s0_fixed20", {"alpha": 0.85, "max_iter": 20, "tol": 0.0})):
+        res = pr_iter(G, **kw)
+        names.append(name)
+        out[f"{name}/params"] = np.frombuffer(json.dumps(params).encode(), np.uint8)
+        out[f"{name}/kwargs"] = np.frombuffer(json.dumps(kw).encode(), np.uint8)
+        out[f"{name}/sha256"] = np.frombuffer(graph_digest(csr.V, csr.E).encode(), np.uint8)
+        out[f"{name}/expected"] = np.array([res[i] for i in range(csr.n)], np.float64)
+    out["names"] = np.frombuffer(json.dumps(names).encode(), np.uint8)
+    return out
+
+
 def inbound_cases():
     sys.path.insert(0, str(ROOT))
     from oracle import oracle
@@ -292,12 +329,19 @@ def ppr_cases():
 
 
 def main():
+    # --only NAME writes one fixture: small, rmat, config, inbound or ppr
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
     eg, pr_iter = _import_reference()
-    cases = small_cases(eg)
-    (HERE / "pagerank_small.json").write_text(json.dumps(cases, indent=1))
-    np.savez_compressed(HERE / "pagerank_rmat.npz", **rmat_cases(eg, pr_iter))
-    np.savez_compressed(HERE / "inbound_ref.npz", **inbound_cases())
-    np.savez_compressed(HERE / "ppr_networkx.npz", **ppr_cases())
+    if only in (None, "small"):
+        (HERE / "pagerank_small.json").write_text(json.dumps(small_cases(eg), indent=1))
+    if only in (None, "rmat"):
+        np.savez_compressed(HERE / "pagerank_rmat.npz", **rmat_cases(eg, pr_iter))
+    if only in (None, "config"):
+        np.savez_compressed(HERE / "pagerank_config.npz", **config_cases(eg, pr_iter))
+    if only in (None, "inbound"):
+        np.savez_compressed(HERE / "inbound_ref.npz", **inbound_cases())
+    if only in (None, "ppr"):
+        np.savez_compressed(HERE / "ppr_networkx.npz", **ppr_cases())
     print("golden fixtures written to", HERE)
 
 

@@ -138,6 +138,33 @@ def golden_rmat_cases():
     return out
 
 
+def golden_config_cases():
+    """The scale-14 workload's reference vectors; the graph is regenerated
+    here and checked against the digest the fixture recorded."""
+    import hashlib
+
+    from eggpu_b200 import synth
+
+    d = np.load(GOLDEN / "pagerank_config.npz")
+    names = json.loads(bytes(d["names"]).decode())
+    out = []
+    graphs = {}
+    for nm in names:
+        params = json.loads(bytes(d[nm + "/params"]).decode())
+        key = json.dumps(params, sort_keys=True)
+        if key not in graphs:
+            csr = synth.rmat(**params)
+            h = hashlib.sha256()
+            h.update(np.ascontiguousarray(csr.V, np.int32).tobytes())
+            h.update(np.ascontiguousarray(csr.E, np.int32).tobytes())
+            graphs[key] = (csr, h.hexdigest())
+        csr, digest = graphs[key]
+        assert digest == bytes(d[nm + "/sha256"]).decode(), f"{nm}: the generator no longer makes the recorded graph"
+        kw = json.loads(bytes(d[nm + "/kwargs"]).decode())
+        out.append((nm, csr.V, csr.E, None, kw, d[nm + "/expected"]))
+    return out
+
+
 def golden_inbound_cases():
     d = np.load(GOLDEN / "inbound_ref.npz")
     names = json.loads(bytes(d["names"]).decode())

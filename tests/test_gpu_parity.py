@@ -14,7 +14,8 @@ import pytest
 from eggpu_b200 import _native, backend, synth
 from eggpu_b200 import api as prmod
 from oracle import oracle
-from tests.graphs import DiGraph, Graph, golden_inbound_cases, golden_ppr, golden_rmat_cases, golden_small_cases
+from tests.graphs import (DiGraph, Graph, golden_config_cases, golden_inbound_cases, golden_ppr,
+                          golden_rmat_cases, golden_small_cases)
 
 pytestmark = pytest.mark.gpu
 
@@ -81,6 +82,19 @@ def test_reference_rmat_vectors(case):
     pg = _native.PreparedGraph(V, E, W)
     ranks, stats = pg.pagerank(**kw)
     _check_against_oracle(V, E, W, ranks, stats, kw["alpha"], kw["max_iter"], kw["tol"])
+
+
+@pytest.mark.parametrize("case", golden_config_cases(), ids=lambda c: c[0])
+def test_reference_vectors_of_the_scale14_workload(case):
+    # the reference's own ranks on the scale-14 workload (its stop rule, and 20 fixed sweeps)
+    name, V, E, W, kw, expected = case
+    pg = _native.PreparedGraph(V, E, W)
+    ranks, stats = pg.pagerank(**kw)
+    _check_against_oracle(V, E, W, ranks, stats, kw["alpha"], kw["max_iter"], kw["tol"])
+    _, it_ref, _ = oracle.pagerank_pull(V, E, W, **kw)
+    if stats["iterations"] == it_ref:  # the same sweep count as the reference: compare with it directly
+        assert np.abs(ranks - expected).sum() <= L1_TOL
+        assert np.allclose(ranks, expected, rtol=2e-5, atol=1e-7)
 
 
 def test_config_scale14_parity():

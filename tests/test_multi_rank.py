@@ -34,7 +34,7 @@ def _rank_main(rank, world, port, out):
 
 def test_two_gloo_ranks_take_the_slowest_time():
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:  # no fork of a process that already runs threads
         out = mgr.dict()
         mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
         got = dict(out)

@@ -7,10 +7,13 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from tests.graphs import golden_inbound_cases, golden_ppr, golden_rmat_cases, golden_small_cases
+from tests.graphs import golden_config_cases, golden_inbound_cases, golden_ppr, golden_rmat_cases, golden_small_cases
+
+# R-MAT scales 10-12 with the CSR stored, and the scale-14 workload regenerated
+_RMAT_CASES = golden_rmat_cases() + golden_config_cases()
 
 
-@pytest.mark.parametrize("case", golden_rmat_cases(), ids=lambda c: c[0])
+@pytest.mark.parametrize("case", _RMAT_CASES, ids=lambda c: c[0])
 def test_push_oracle_bit_exact_vs_reference_python(case):
     name, V, E, W, kw, expected = case
     ranks, iters, _ = oracle.pagerank_push(V, E, W, **kw)
@@ -18,7 +21,7 @@ def test_push_oracle_bit_exact_vs_reference_python(case):
     assert iters >= 1
 
 
-@pytest.mark.parametrize("case", golden_rmat_cases(), ids=lambda c: c[0])
+@pytest.mark.parametrize("case", _RMAT_CASES, ids=lambda c: c[0])
 def test_pull_oracle_bit_exact_vs_reference_python(case):
     name, V, E, W, kw, expected = case
     ranks, iters, _ = oracle.pagerank_pull(V, E, W, **kw)
