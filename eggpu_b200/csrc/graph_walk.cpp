@@ -23,11 +23,47 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
-#include <unordered_set>
 #include <utility>
 #include <vector>
 
 namespace {
+
+// The unordered pairs {u, v} an undirected walk has met, keyed lo << 32 | hi
+// (both below 2^31, so the all-ones word never is a key).  Open addressing
+// with linear probing, sized up front to at least twice the adjacency's
+// entries: one probe sequence per visit, no rehashing.
+class PairSet {
+public:
+    explicit PairSet(size_t entries) {
+        size_t cap = 16;
+        while (cap < 2 * entries) cap <<= 1;
+        slots_.assign(cap, kEmpty);
+        mask_ = cap - 1;
+    }
+    // true when the pair was not in the set yet
+    bool insert(uint64_t key) {
+        for (uint64_t h = mix(key) & mask_;; h = (h + 1) & mask_) {
+            const uint64_t s = slots_[h];
+            if (s == key) return false;
+            if (s == kEmpty) {
+                slots_[h] = key;
+                return true;
+            }
+        }
+    }
+
+private:
+    static constexpr uint64_t kEmpty = ~0ull;
+    static uint64_t mix(uint64_t x) {  // SplitMix64 finaliser
+        x ^= x >> 30;
+        x *= 0xbf58476d1ce4e5b9ull;
+        x ^= x >> 27;
+        x *= 0x94d049bb133111ebull;
+        return x ^ (x >> 31);
+    }
+    std::vector<uint64_t> slots_;
+    uint64_t mask_ = 0;
+};
 
 // float(attr.get(weight, 1.0)) with the fallbacks of backend._weight_of.
 bool weight_of(PyObject* attr, PyObject* weight, double* out) {
@@ -90,9 +126,22 @@ PyObject* out_csr(PyObject*, PyObject* args) {
         return nullptr;
     }
     const bool want_w = weight != Py_None;
+    // first pass: every row a plain dict, and the adjacency's total size
+    size_t entries = 0;
+    {
+        PyObject *u, *nbrs;
+        Py_ssize_t pos = 0;
+        while (PyDict_Next(adj, &pos, &u, &nbrs)) {
+            if (!PyDict_Check(nbrs)) Py_RETURN_NONE;
+            entries += (size_t)PyDict_Size(nbrs);
+        }
+    }
     std::vector<int32_t> src, dst;
     std::vector<double> wts;
-    std::unordered_set<uint64_t> seen;
+    src.reserve(entries);
+    dst.reserve(entries);
+    if (want_w) wts.reserve(entries);
+    PairSet seen(directed ? 0 : entries);
     {
         PyObject *u, *nbrs;
         Py_ssize_t pos = 0;
@@ -115,7 +164,7 @@ PyObject* out_csr(PyObject*, PyObject* args) {
                     if (iu == iv) continue;
                     const uint64_t key = iu < iv ? ((uint64_t)(uint32_t)iu << 32) | (uint32_t)iv
                                                  : ((uint64_t)(uint32_t)iv << 32) | (uint32_t)iu;
-                    if (!seen.insert(key).second) continue;
+                    if (!seen.insert(key)) continue;
                     double w = 1.0;
                     if (want_w && !weight_of(attr, weight, &w)) return nullptr;
                     src.push_back(iu);
