@@ -107,6 +107,26 @@ def test_native_graph_walk_equals_the_python_walk(directed, weighted):
         backend.graph_csr(G, prepared, w)
 
 
+@pytest.mark.skipif(backend._graph_walk is None, reason="native graph walk not built")
+def test_native_undirected_walk_on_an_asymmetric_adjacency():
+    # each unordered pair once per direction, its weight from where it is first met,
+    # also when the two directions disagree or only one of them is present
+    rng = np.random.default_rng(11)
+    n = 800
+    adj = {i: {} for i in range(n)}
+    for _ in range(6000):
+        a, b = (int(x) for x in rng.integers(0, n, 2))
+        adj[a][b] = {"w": float(rng.random())}
+        r = rng.random()
+        if r < 0.6:
+            adj[b][a] = {"w": float(rng.random())}  # the other direction, another weight
+    G = types.SimpleNamespace(_adj=adj)
+    prepared = {"node_to_idx": {i: i for i in range(n)}, "nodes": list(range(n)), "directed": False}
+    for w in (None, "w"):
+        a, b = backend.graph_csr(G, prepared, w), backend._graph_csr_py(G, prepared, w)
+        assert all((x is None and y is None) or np.array_equal(x, y) for x, y in zip(a, b))
+
+
 def test_prepared_context_reuse_and_mutation_invalidation():
     G = DiGraph()
     G.add_edge(0, 1, weight=8.0)
