@@ -312,8 +312,18 @@ def _mix64(h, x):
 
 def graph_stamp(G):
     """O(|V|) fingerprint: node count, adjacency slots, node hashes and degrees,
-    and the first neighbours of the first 32 nodes."""
+    and the first neighbours of the first 32 nodes (native when the graph
+    walk extension is built; _graph_stamp_py is its specification)."""
     adj = _adj_dict(G)
+    if _graph_walk is not None and isinstance(adj, dict):
+        res = _graph_walk.stamp(adj)
+        if res is not None:
+            nodes, slots, h = res
+            return (bool(G.is_directed()), nodes, slots, h)
+    return _graph_stamp_py(G, adj)
+
+
+def _graph_stamp_py(G, adj):
     edge_slots = 0
     h = 1469598103934665603
     for i, (u, nbrs) in enumerate(adj.items()):

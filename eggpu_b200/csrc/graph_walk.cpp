@@ -17,6 +17,11 @@
 // out_csr(adj, index, n, directed, weight) -> (V, E, W) as bytearrays
 // (int32 n+1, int32 m, float64 m or None), or None when adj / its rows are not
 // plain dicts (the caller then walks in Python).
+//
+// stamp(adj) -> (nodes, adjacency slots, h): the prepared-graph fingerprint of
+// backend._graph_stamp_py (node count, adjacency slots, a 64-bit mix of node
+// hashes and degrees and of the first 4 neighbours of the first 32 nodes),
+// value for value, or None when adj / its rows are not plain dicts.
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
 
@@ -244,9 +249,46 @@ PyObject* out_csr(PyObject*, PyObject* args) {
     return out;
 }
 
+// h ^= x + 0x9E3779B97F4A7C15 + (h << 6) + (h >> 2), all modulo 2^64
+// (backend._mix64; x is a Python hash, taken in two's complement).
+uint64_t mix64(uint64_t h, int64_t x) {
+    return h ^ ((uint64_t)x + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2));
+}
+
+PyObject* stamp(PyObject*, PyObject* args) {
+    PyObject* adj;
+    if (!PyArg_ParseTuple(args, "O", &adj)) return nullptr;
+    if (!PyDict_Check(adj)) Py_RETURN_NONE;
+    uint64_t h = 1469598103934665603ull;
+    unsigned long long slots = 0;
+    PyObject *u, *nbrs;
+    Py_ssize_t pos = 0, i = 0;
+    while (PyDict_Next(adj, &pos, &u, &nbrs)) {
+        if (!PyDict_Check(nbrs)) Py_RETURN_NONE;
+        const Py_ssize_t deg = PyDict_Size(nbrs);
+        slots += (unsigned long long)deg;
+        const Py_hash_t hu = PyObject_Hash(u);
+        if (hu == -1 && PyErr_Occurred()) return nullptr;
+        h = mix64(h, (int64_t)hu);
+        h = mix64(h, (int64_t)deg);
+        if (i < 32) {
+            PyObject *v, *attr;
+            Py_ssize_t p2 = 0;
+            for (int j = 0; j < 4 && PyDict_Next(nbrs, &p2, &v, &attr); ++j) {
+                const Py_hash_t hv = PyObject_Hash(v);
+                if (hv == -1 && PyErr_Occurred()) return nullptr;
+                h = mix64(h, (int64_t)hv);
+            }
+        }
+        ++i;
+    }
+    return Py_BuildValue("(nKK)", PyDict_Size(adj), slots, (unsigned long long)h);
+}
+
 PyMethodDef kMethods[] = {
     {"out_csr", out_csr, METH_VARARGS,
      "out_csr(adj, index, n, directed, weight) -> (V, E, W) bytearrays, or None for non-dict adjacency"},
+    {"stamp", stamp, METH_VARARGS, "stamp(adj) -> (nodes, adjacency slots, fingerprint), or None for non-dict adjacency"},
     {nullptr, nullptr, 0, nullptr},
 };
 

@@ -127,6 +127,25 @@ def test_native_undirected_walk_on_an_asymmetric_adjacency():
         assert all((x is None and y is None) or np.array_equal(x, y) for x, y in zip(a, b))
 
 
+@pytest.mark.skipif(backend._graph_walk is None, reason="native graph walk not built")
+def test_native_graph_stamp_equals_the_python_stamp():
+    rng = np.random.default_rng(5)
+    labels = [("v", i) for i in range(500)] + list(range(-3, 60)) + [f"s{i}" for i in range(40)] + [2.5, None]
+    adj = {u: {} for u in labels}
+    for _ in range(4000):
+        a, b = rng.integers(0, len(labels), 2)
+        adj[labels[a]][labels[b]] = {}
+    for directed in (True, False):
+        G = types.SimpleNamespace(_adj=adj, is_directed=lambda d=directed: d)
+        assert backend.graph_stamp(G) == backend._graph_stamp_py(G, adj)
+    # a row that is not a plain dict: the Python stamp answers
+    odd = dict(adj)
+    odd[labels[0]] = types.MappingProxyType(dict(adj[labels[0]]))
+    G = types.SimpleNamespace(_adj=odd, is_directed=lambda: True)
+    assert backend._graph_walk.stamp(odd) is None
+    assert backend.graph_stamp(G) == backend._graph_stamp_py(G, odd)
+
+
 def test_prepared_context_reuse_and_mutation_invalidation():
     G = DiGraph()
     G.add_edge(0, 1, weight=8.0)
