@@ -532,7 +532,11 @@ def _personalization_vector(personalization, prepared):
         vec = np.zeros(n, np.float64)
         idx_of = prepared["node_to_idx"]
         for node, val in personalization.items():
-            i = idx_of.get(node) if idx_of is not None else (int(node) if 0 <= int(node) < n else None)
+            if idx_of is not None:
+                i = idx_of.get(node)
+            else:  # bulk graphs: the nodes are 0..n-1
+                ok = isinstance(node, (int, np.integer)) and not isinstance(node, bool) and 0 <= node < n
+                i = int(node) if ok else None
             if i is None:
                 raise KeyError(f"personalization node {node!r} is not in the graph")
             vec[i] = float(val)

@@ -146,6 +146,15 @@ def test_native_graph_stamp_equals_the_python_stamp():
     assert backend.graph_stamp(G) == backend._graph_stamp_py(G, odd)
 
 
+def test_personalization_keys_of_a_bulk_graph():
+    p = {"nodes": range(4), "node_to_idx": None}
+    vec = backend._personalization_vector({0: 1.0, np.int64(3): 3.0}, p)
+    assert vec.tolist() == [1.0, 0.0, 0.0, 3.0]  # the engine normalises it
+    for bad in ("a", 4, -1, True, 1.5):
+        with pytest.raises(KeyError, match="is not in the graph"):
+            backend._personalization_vector({bad: 1.0}, p)
+
+
 def test_prepared_context_reuse_and_mutation_invalidation():
     G = DiGraph()
     G.add_edge(0, 1, weight=8.0)
