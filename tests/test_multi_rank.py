@@ -47,3 +47,13 @@ def test_whole_job_rate_and_single_process_path():
     assert bench.max_over_ranks(None, [3, 4.5], "cpu") == [3.0, 4.5]
     # 4 ranks, 1e9 units each, slowest rank 2 s -> 2e9 units/s for the job
     assert bench.whole_job_rate(4, 1e9, 2.0) == pytest.approx(2e9)
+
+
+def test_roofline_inputs_of_the_bench_line():
+    # traffic: the DRAM bytes per launch that the committed ncu summary records
+    import bench
+
+    assert bench.profile_traffic("k_sweep_rmat22.md") == 416051200.0
+    assert bench.profile_traffic("no_such_profile.md") is None
+    peak, kind = bench.measured_peaks()
+    assert peak > 0 and kind in ("measured", "fallback")
