@@ -296,6 +296,18 @@ def test_bulk_graph_contract_as_the_reference_pins_it(tmp_path):
     assert Gw._eggpu_bulk_signature[:2] == (str(Gw.metadata_path), 1)
 
 
+def test_bulk_graph_records_an_undirected_projection_without_loading_it(tmp_path):
+    path, meta = _write_reference_style_bulk(tmp_path, directed=True)
+    meta["undirected_projection_manifest"] = "tiny.projection.json"  # serves other algorithms; need not exist
+    path.write_text(json.dumps(meta), encoding="utf-8")
+    G = bulk.read_eggpu_csr(path)
+    assert G.undirected_projection_path == (tmp_path / "tiny.projection.json").resolve()
+    assert G._eggpu_bulk_signature[-1] == str(G.undirected_projection_path)
+    other = bulk.read_eggpu_csr(path, undirected_projection_path=str(tmp_path / "elsewhere.json"))
+    assert other._eggpu_bulk_signature != G._eggpu_bulk_signature
+    assert G.memory_estimate()["host_undirected_projection_bytes"] == 0
+
+
 def test_bulk_manifest_checks_match_the_reference_messages(tmp_path, monkeypatch):
     # easygraph/classes/eggpu_bulk_graph.py:200-247 and graph_convert.cpp:447-516
     path, meta = _write_reference_style_bulk(tmp_path, weighted=True)
