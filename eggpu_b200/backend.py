@@ -591,6 +591,8 @@ def pagerank_batch(G, personalizations, alpha=0.85, max_iter=200, eps=1e-6, weig
     nodes = prepared["nodes"]
     if len(nodes) == 0:
         return [{} for _ in range(len(personalizations))]
+    if len(personalizations) == 0:
+        return []
     pg = prepared_native(G, prepared, weight)
     if isinstance(personalizations, np.ndarray):
         T = np.asarray(personalizations, np.float64)

@@ -155,6 +155,14 @@ def test_personalization_keys_of_a_bulk_graph():
             backend._personalization_vector({bad: 1.0}, p)
 
 
+def test_batch_of_no_teleport_vectors_is_an_empty_list(monkeypatch):
+    monkeypatch.setattr(backend, "prepared_native", lambda *a, **k: pytest.fail("no solve for an empty batch"))
+    G = DiGraph()
+    G.add_edge(0, 1)
+    assert backend.pagerank_batch(G, []) == []
+    assert backend.pagerank_batch(G, np.zeros((0, 2))) == []
+
+
 def test_prepared_context_reuse_and_mutation_invalidation():
     G = DiGraph()
     G.add_edge(0, 1, weight=8.0)
