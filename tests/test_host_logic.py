@@ -163,6 +163,19 @@ def test_batch_of_no_teleport_vectors_is_an_empty_list(monkeypatch):
     assert backend.pagerank_batch(G, np.zeros((0, 2))) == []
 
 
+def test_runtime_switches_as_the_reference_reads_them(monkeypatch):
+    # easygraph/tests/test_eggpu_runtime.py:43-56
+    for name in ("EASYGRAPH_ENABLE_GPU", "EASYGRAPH_GPU_STRICT_ERRORS"):
+        monkeypatch.delenv(name, raising=False)
+    assert not prmod.gpu_runtime_enabled() and not prmod.gpu_strict_errors()
+    for val, on in (("TRUE", True), ("1", True), (" yes ", True), ("on", True), ("FALSE", False), ("2", False)):
+        monkeypatch.setenv("EASYGRAPH_ENABLE_GPU", val)
+        assert prmod.gpu_runtime_enabled() is on
+    monkeypatch.delenv("EASYGRAPH_ENABLE_GPU")
+    monkeypatch.setenv("EASYGRAPH_GPU_STRICT_ERRORS", "TRUE")
+    assert prmod.gpu_strict_errors() and not prmod.gpu_runtime_enabled()  # independent switches
+
+
 def test_prepared_context_reuse_and_mutation_invalidation():
     G = DiGraph()
     G.add_edge(0, 1, weight=8.0)
