@@ -33,6 +33,16 @@ def test_dense_value_dict_is_a_read_only_mapping():
     assert rng[2] == 3.0 and 3 not in rng and True not in rng
 
 
+def test_dense_result_wraps_the_result_vector_without_a_copy():
+    # the ranks land in one host vector and the Mapping is a read-only view of it
+    vec = np.linspace(0.0, 1.0, 5)
+    r = backend.DenseValueDict(range(5), vec)
+    assert np.shares_memory(r.to_numpy(), vec) and not r.to_numpy().flags.writeable
+    with_sentinel = np.concatenate([[-1.0], vec])
+    r2 = backend.DenseValueDict(range(5), backend.normalize_dense_array(with_sentinel, 5, allow_leading_sentinel=True))
+    assert np.shares_memory(r2.to_numpy(), with_sentinel) and r2[4] == 1.0
+
+
 def test_dense_shape_contract():
     # gpu_eggpu_backend.py:1092-1126 / test_eggpu_cache_contracts.py:199-221
     with pytest.raises(backend.DenseResultShapeError, match=r"expected \(3,\) or \(4,\)"):
