@@ -1,16 +1,25 @@
 """Benchmark of the PageRank hot path (one JSON line on rank 0).
 
-Default workload (the headline): plain PageRank on a directed R-MAT scale-22
-graph (4,194,304 vertices, edgefactor 16, a/b/c/d 0.57/0.19/0.19/0.05,
-seed 1, self-loops and duplicates removed, unweighted), alpha 0.85.  A step
-is one full solve of SWEEPS sweeps with tol = 0 (the reference's stop rule
-ends a scale-22 solve after one sweep, so throughput is measured at a fixed
-sweep count): set-up, SWEEPS fused sweeps, the FP64 correction sweep and the
+Default workload (the headline): plain PageRank on a directed R-MAT scale-25
+graph (33,554,432 vertices, edgefactor 16, a/b/c/d 0.57/0.19/0.19/0.05,
+seed 2, self-loops and duplicates removed), edge weights i.i.d. U(0,1] FP32
+with weighted out-degree normalisation, alpha 0.85.  A step is one full solve
+of SWEEPS sweeps with tol = 0 (the reference's stop rule, tol 1e-7 here, ends
+a scale-25 solve after one sweep, so throughput is measured at a fixed sweep
+count): set-up, SWEEPS fused sweeps, the FP64 correction sweep and the
 normalisation.  value = GTEPS per sweep = nnz * SWEEPS / step time, summed
 over ranks (replicas: every rank solves its own copy; scaling "weak").
 
+The line also carries: the roofline of the sweep kernel, the end-to-end rate
+through the drop-in C ABI entry (host CSR in page-locked and in pageable
+memory), parity against the FP64 oracle (stop rule at the config's tolerance
+and fixed 10-sweep solves), the reference's own cuSPARSE GPU solve timed on
+the same graph, the oracle's OpenMP restatement of the reference's CPU path
+timed on the host, and the scale-22 config (R-MAT scale 22, seed 1,
+unweighted) measured the same way as a secondary object.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rmat22|rmat25w|ppr|batch|serving]
+                    [--workload rmat25w|rmat22|rmat<scale>[w]|ppr|batch|serving|precision25]
 
 --impl reference times the reference's own CPU algorithm for the path (the
 oracle's port of cpp_easygraph's OpenMP _pagerank, all host threads) on the
@@ -144,23 +153,30 @@ def cpu_baseline_port(csr, alpha, budget_s=10.0):
         t_total += time.perf_counter() - t0
         sweeps_done += sw
     return {"value": csr.m * sweeps_done / t_total / 1e9, "unit": "GTEPS/iter", "cores": threads, "kind": "port",
+            "label": "restatement",
             "sample": f"{sweeps_done} sweeps of the same graph in solves of 2 sweeps (tol 0), "
-                      f"{t_total:.1f} s, OpenMP push with atomics (cpp_easygraph pagerank.cpp:21-122 port)"}
+                      f"{t_total:.1f} s: the oracle's FP64 OpenMP restatement of the reference's CPU PageRank "
+                      "(push with atomic adds, cpp_easygraph/functions/pagerank/pagerank.cpp:21-122) over the "
+                      "same CSR"}
 
 
 def make_workload(name):
+    """rmat<scale>[w]: the R-MAT graphs of the configs (scale 22: seed 1, unweighted;
+    scale 25: seed 2, weighted); other scales (smaller profiling cases) use seed 2."""
     from eggpu_b200 import synth
 
-    if name == "rmat22":
-        csr = synth.rmat(scale=22, edgefactor=16, seed=1)
-        desc = ("R-MAT scale 22 (4,194,304 vertices, edgefactor 16, a/b/c/d 0.57/0.19/0.19/0.05, seed 1, "
-                "self-loops and duplicates removed, unweighted), alpha 0.85")
-    elif name == "rmat25w":
-        csr = synth.rmat(scale=25, edgefactor=16, seed=2, weighted=True)
-        desc = ("R-MAT scale 25 (33,554,432 vertices, edgefactor 16, seed 2), weights i.i.d. U(0,1] FP32, "
-                "weighted out-degree normalisation, alpha 0.85")
-    else:
+    m = re.fullmatch(r"rmat(\d+)(w?)", name)
+    if not m:
         raise SystemExit(f"unknown workload {name}")
+    scale, weighted = int(m.group(1)), m.group(2) == "w"
+    if not 10 <= scale <= 26:
+        raise SystemExit(f"R-MAT scale {scale} out of range [10, 26]")
+    seed = 1 if scale == 22 else 2
+    csr = synth.rmat(scale=scale, edgefactor=16, seed=seed, weighted=weighted)
+    desc = (f"R-MAT scale {scale} ({1 << scale:,} vertices, edgefactor 16, a/b/c/d 0.57/0.19/0.19/0.05, "
+            f"seed {seed}, self-loops and duplicates removed, "
+            + ("weights i.i.d. U(0,1] FP32, weighted out-degree normalisation" if weighted else "unweighted")
+            + "), alpha 0.85")
     return csr, desc
 
 
@@ -198,28 +214,17 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
+def workload_tol(name):
+    """The stop-rule tolerance of the workload's config: 1e-7 for the scale-25
+    precision config, 1e-6 otherwise."""
+    return 1e-7 if name.startswith("rmat25") else 1e-6
+
+
+def time_solves(pg, stream, steps, warmup, sweeps, dist):
+    """Device time of `steps` whole solves of `sweeps` sweeps (tol 0) and of
+    steps//2 solves of 2*sweeps, CUDA events on the solve's stream, max over
+    ranks.  Returns (t_step, t_sweep, stats, stats2)."""
     import torch
-
-    from eggpu_b200 import _native
-
-    rank, world, local = _rank_env()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-
-        dist_mod.init_process_group("nccl", device_id=torch.device("cuda", local))
-        dist = dist_mod
-    csr, desc = make_workload(args.workload)
-    pg = _native.PreparedGraph(csr.V, csr.E, csr.W)
-    nnz = pg.nnz
-    # the sweep layout chosen by the per-graph tuner, before any timing (a
-    # long-lived prepared graph is tuned once)
-    tuning = pg.tuning() if args.no_autotune else pg.autotune(sweep=True, spmm=False)
-    stream = torch.cuda.Stream()
-    pg.set_stream(stream.cuda_stream)
-    sweeps = args.sweeps
 
     def timed(k, n_sweeps):
         e0 = torch.cuda.Event(enable_timing=True)
@@ -233,93 +238,199 @@ def run_ours(args):
         _, st = pg.collect(copy=False)
         return e0.elapsed_time(e1) / k / 1e3, st
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         pg.enqueue(alpha=0.85, max_iter=sweeps, tol=0.0)
     pg.collect(copy=False)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        t_step, st = timed(args.steps, sweeps)
-        t_step2, st2 = timed(max(1, args.steps // 2), 2 * sweeps)
+    t_step, st = timed(steps, sweeps)
+    t_step2, st2 = timed(max(1, steps // 2), 2 * sweeps)
     torch.cuda.synchronize()
     t_step, t_step2 = max_over_ranks(dist, [t_step, t_step2], "cuda")
     if dist:
         dist.barrier()
-    t_sweep = max((t_step2 - t_step) / sweeps, 1e-9)
-    bytes_per_iter = st["bytes_per_iter"]
-    value = whole_job_rate(world, nnz * sweeps, t_step) / 1e9
-    peak, peak_kind = measured_peaks()
-    achieved = bytes_per_iter / t_sweep / 1e9
-    traffic = profile_traffic(f"k_sweep_{args.workload}.md")
-    launches_per_step = st["launches"]
+    return t_step, max((t_step2 - t_step) / sweeps, 1e-9), st, st2
 
-    # end-to-end through the drop-in C ABI entry, host CSR in pinned memory
-    Vp = torch.from_numpy(csr.V).pin_memory().numpy()
-    Ep = torch.from_numpy(csr.E).pin_memory().numpy()
-    Wp = None if csr.W is None else torch.from_numpy(csr.W).pin_memory().numpy()
-    PRp = _native.pinned_empty(csr.n)  # the caller's result vector, reused across calls
-    e2e_steps = 0 if args.no_e2e else max(2, min(args.steps, 5))
+
+def measure_e2e(csr, sweeps, steps, rank, world, dist, pinned=True):
+    """Whole solves through the drop-in C ABI entry egpr_pagerank_csr, every
+    step: H2D of the host CSR, GPU preparation, `sweeps` sweeps, D2H of the
+    FP64 ranks.  pinned: the CSR sits in page-locked memory; otherwise in
+    ordinary (pageable) numpy arrays, which the library stages itself."""
+    import torch
+
+    from eggpu_b200 import _native
+
+    if pinned:
+        V = torch.from_numpy(csr.V).pin_memory().numpy()
+        E = torch.from_numpy(csr.E).pin_memory().numpy()
+        W = None if csr.W is None else torch.from_numpy(csr.W).pin_memory().numpy()
+    else:
+        V, E, W = csr.V, csr.E, csr.W
+    PR = _native.pinned_empty(csr.n)  # the caller's result vector, reused across calls
     _native.cache_reset()
-    if e2e_steps:
-        _native.pagerank_csr(Vp, Ep, Wp, 10**9 + rank, 0.85, sweeps, 0.0, out=PRp)  # warm the code path
+    _native.pagerank_csr(V, E, W, 10**9 + rank, 0.85, sweeps, 0.0, out=PR)  # warm the code path
     _native.cache_reset()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for i in range(e2e_steps):
-        _native.pagerank_csr(Vp, Ep, Wp, 2 * 10**9 + i, 0.85, sweeps, 0.0, out=PRp)
-        _native.cache_reset()
-    t_e2e = (time.perf_counter() - t0) / max(e2e_steps, 1)
-    (t_e2e,) = max_over_ranks(dist, [t_e2e], "cuda")
+    for i in range(steps):
+        _native.pagerank_csr(V, E, W, 2 * 10**9 + i, 0.85, sweeps, 0.0, out=PR)
+        _native.cache_reset()  # the next step prepares the graph again
+    t = (time.perf_counter() - t0) / steps
+    (t,) = max_over_ranks(dist, [t], "cuda")
+    nnz = int(np.count_nonzero((csr.E >= 0) & (csr.E < csr.n)))
     h2d = csr.V.nbytes + csr.E.nbytes + (0 if csr.W is None else csr.W.nbytes)
-    e2e = None if not e2e_steps else {"value": whole_job_rate(world, nnz * sweeps, t_e2e) / 1e9, "unit": "GTEPS/iter", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(8 * csr.n), "ms_per_step": t_e2e * 1e3,
-           "path": "egpr_pagerank_csr (drop-in for gpu_easygraph::pagerank): H2D of the out-edge CSR, GPU "
-                   "preparation, solve, D2H of FP64 ranks into the caller's page-locked result vector, every "
-                   "step"}
+    return {"value": whole_job_rate(world, nnz * sweeps, t) / 1e9, "unit": "GTEPS/iter",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(8 * csr.n), "ms_per_step": t * 1e3,
+            "steps": steps,
+            "path": "egpr_pagerank_csr (drop-in for gpu_easygraph::pagerank): H2D of the out-edge CSR from "
+                    + ("page-locked" if pinned else "pageable") + " host memory, GPU preparation, "
+                    f"{sweeps} sweeps, FP64 correction, D2H of FP64 ranks into the caller's page-locked result "
+                    "vector, every step"}
 
-    # reference stop rule on the same graph (one sweep at this size) and its accuracy vs the FP64 oracle
-    parity = None
+
+def parity_vs_oracle(pg, csr, tol):
+    """The reference's stop rule at the config's tolerance, and fixed 10-sweep
+    solves with and without the FP64 correction sweep, against the FP64
+    oracle (iterations, L1 and max-abs error)."""
+    from oracle import oracle
+
+    inbound = oracle.build_inbound(csr.V, csr.E, csr.W)
+    out = {}
+    for label, max_iter, t, corr in ((f"rule_tol{tol:g}", 100, tol, True), ("fixed10", 10, 0.0, True),
+                                     ("fixed10_no_correction", 10, 0.0, False)):
+        ranks, st = pg.pagerank(alpha=0.85, max_iter=max_iter, tol=t, correction=corr)
+        ref, it, _ = oracle.pagerank_pull(csr.V, csr.E, csr.W, alpha=0.85, max_iter=max_iter, tol=t,
+                                          inbound=inbound)
+        out[label] = {"iterations": st["iterations"], "oracle_iterations": it,
+                      "l1_vs_fp64_oracle": float(np.abs(ranks - ref).sum()),
+                      "max_abs_vs_fp64_oracle": float(np.abs(ranks - ref).max()),
+                      "solve_ms": st["kernel_seconds"] * 1e3}
+    return out
+
+
+def reference_gpu_baseline(csr, sweeps, ours_sweep_ms, ours_e2e_ms):
+    """The reference's own GPU solve on the same graph and box: cuda_pagerank
+    (cuSPARSE CSR SpMV + cuBLAS dot + two kernels and two host round trips per
+    sweep, gpu_easygraph/functions/centrality/pagerank.cu:352-713), compiled
+    for sm_100a from the reference sources into oracle/_ref.  Its per-sweep
+    time is read from its own CUDA events around the sweep loop
+    (pagerank.cu:578,666-676): (T(2S) - T(S)) / S on the warm workspace."""
+    from oracle import oracle
+
+    if not oracle.ref_available():
+        return {"unavailable": "oracle/_ref/libref_pagerank.so not built (needs the reference tree at build time)"}
+    t0 = time.perf_counter()
+    oracle.ref_cuda_pagerank(csr.V, csr.E, csr.W, 0.85, sweeps, 0.0)  # cold: host transpose, H2D, set-up
+    cold = time.perf_counter() - t0
+    _, ks1 = oracle.ref_cuda_pagerank(csr.V, csr.E, csr.W, 0.85, sweeps, 0.0)  # warm: cached device graph
+    _, ks2 = oracle.ref_cuda_pagerank(csr.V, csr.E, csr.W, 0.85, 2 * sweeps, 0.0)
+    per_sweep = max((ks2 - ks1) / sweeps, 1e-9)
+    nnz = int(np.count_nonzero((csr.E >= 0) & (csr.E < csr.n)))
+    return {"impl": "reference cuda_pagerank (cuSPARSE CSR_ALG2 SpMV + cublasSdot), sm_100a build",
+            "sweep_ms": per_sweep * 1e3, "gteps_per_iter": nnz / per_sweep / 1e9,
+            "loop_ms_for_sweeps": ks1 * 1e3, "sweeps": sweeps,
+            "cold_call_ms": cold * 1e3,
+            "cold_call_note": "one call on a new graph: host-side inbound CSR build, H2D, cuSPARSE set-up, "
+                              f"{sweeps} sweeps, D2H and host normalisation (wall clock)",
+            "ours_over_reference_sweep_speedup": per_sweep * 1e3 / ours_sweep_ms,
+            "ours_e2e_over_reference_cold_call_speedup": (cold * 1e3 / ours_e2e_ms) if ours_e2e_ms else None}
+
+
+def measure_workload(name, args, rank, world, local, dist, sweeps, with_e2e=True, e2e_pageable=False):
+    """One workload on this rank: prepared graph, autotuned layout, timed solves,
+    roofline and end-to-end legs.  Returns (csr, desc, pg, result dict)."""
+    import torch
+
+    from eggpu_b200 import _native
+
+    csr, desc = make_workload(name)
+    pg = _native.PreparedGraph(csr.V, csr.E, csr.W)
+    nnz = pg.nnz
+    # the sweep layout chosen by the per-graph tuner, before any timing (a
+    # long-lived prepared graph is tuned once)
+    tuning = pg.tuning() if args.no_autotune else pg.autotune(sweep=True, spmm=False)
+    stream = torch.cuda.Stream()
+    pg.set_stream(stream.cuda_stream)
+    with ClockSampler(local) as clk:
+        t_step, t_sweep, st, st2 = time_solves(pg, stream, args.steps, args.warmup, sweeps, dist)
+    pg.set_stream(None)
+    bytes_per_iter = st["bytes_per_iter"]
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_iter / t_sweep / 1e9
+    res = {
+        "value": whole_job_rate(world, nnz * sweeps, t_step) / 1e9,
+        "ms_per_step": t_step * 1e3,
+        "config": {"workload": f"{name}: {desc}", "n": csr.n, "nnz": int(nnz), "sweeps_per_step": sweeps,
+                   "tol": 0.0, "parallelism": f"replicas{world}",
+                   "l2": f"inputs larger than L2 (inbound CSR {(4 * (csr.n + 1) + 4 * nnz) / 1e6:.0f} MB > "
+                         f"{L2_BYTES / 1e6:.0f} MB), no flush between steps",
+                   "precision": "FP32 ranks and products; FP64 residual, dangling mass and rank sums; final FP64 "
+                                "correction sweep",
+                   "layout": {"chunks_per_warp": tuning["chunks_per_warp"], "row_cost": tuning["row_cost"],
+                              "chosen_by": "defaults (--no-autotune)" if args.no_autotune
+                              else "egpr_graph_autotune before timing"}},
+        "hbm_gbs": bytes_per_iter * sweeps / t_step / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": profile_traffic(f"k_sweep_{name}.md"),
+                     "kernel": "k_sweep<float> (fused sweep)", "peak_source": peak_kind,
+                     "bytes_per_launch": bytes_per_iter, "launch_ms": t_sweep * 1e3,
+                     "timing": "CUDA events on the launch stream; per-sweep time = (T(2S) - T(S)) / S"},
+        "gpu_launches": int(st["launches"] * args.steps + st2["launches"] * max(1, args.steps // 2)),
+        "gpu_launches_per_step": st["launches"],
+        "clocks": clk.summary(),
+    }
+    if with_e2e and not args.no_e2e:
+        e2e_steps = max(2, min(args.steps, 5))
+        res["e2e"] = measure_e2e(csr, sweeps, e2e_steps, rank, world, dist, pinned=True)
+        if e2e_pageable:
+            res["e2e_pageable"] = measure_e2e(csr, sweeps, e2e_steps, rank, world, dist, pinned=False)
+    return csr, desc, pg, res
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                    timeout=datetime.timedelta(seconds=600))
+        dist = dist_mod
+    sweeps = args.sweeps
+    csr, desc, pg, res = measure_workload(args.workload, args, rank, world, local, dist, sweeps,
+                                          e2e_pageable=not args.no_pageable)
+    secondary = None
+    if args.secondary and args.secondary != args.workload:
+        _, _, pg2, sec = measure_workload(args.secondary, args, rank, world, local, dist, sweeps)
+        pg2.close()
+        secondary = {k: sec[k] for k in ("value", "ms_per_step", "config", "hbm_gbs", "roofline", "e2e",
+                                         "gpu_launches_per_step") if k in sec}
+    parity = ref_gpu = cpu = None
     if rank == 0 and not args.no_parity:
-        from oracle import oracle
-
-        ranks, pst = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
-        ref, it_ref, _ = oracle.pagerank_pull(csr.V, csr.E, csr.W, alpha=0.85, max_iter=100, tol=1e-6)
-        parity = {"iterations": pst["iterations"], "oracle_iterations": it_ref,
-                  "l1_vs_fp64_oracle": float(np.abs(ranks - ref).sum()),
-                  "max_abs_vs_fp64_oracle": float(np.abs(ranks - ref).max()),
-                  "solve_ms": pst["kernel_seconds"] * 1e3}
-    cpu = None
+        parity = parity_vs_oracle(pg, csr, workload_tol(args.workload))
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_baseline(csr, sweeps, res["roofline"]["launch_ms"],
+                                         res.get("e2e", {}).get("ms_per_step"))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(csr, 0.85, budget_s=args.cpu_seconds)
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "GTEPS/iter", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {desc}", "n": csr.n, "nnz": int(nnz),
-                       "sweeps_per_step": sweeps, "tol": 0.0, "parallelism": f"replicas{world}",
-                       "l2": f"inputs larger than L2 (inbound CSR {(4 * (csr.n + 1) + 4 * nnz) / 1e6:.0f} MB > "
-                             f"{L2_BYTES / 1e6:.0f} MB); the FP32 rank vectors are meant to stay L2-resident",
-                       "precision": "FP32 ranks and products, FP64 residual/dangling/sums, final FP64 sweep",
-                       "layout": {"chunks_per_warp": tuning["chunks_per_warp"], "row_cost": tuning["row_cost"],
-                                  "chosen_by": "defaults (--no-autotune)" if args.no_autotune
-                                  else "egpr_graph_autotune before timing"}},
-            "hbm_gbs": bytes_per_iter * sweeps / t_step / 1e9,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_sweep<float> (fused sweep)", "peak_source": peak_kind,
-                         "bytes_per_launch": bytes_per_iter, "launch_ms": t_sweep * 1e3,
-                         "timing": "CUDA events on the launch stream; per-sweep time = (T(2S) - T(S)) / S"},
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": int(launches_per_step * args.steps + st2["launches"] * max(1, args.steps // 2)),
-            "gpu_launches_per_step": launches_per_step,
-            "clocks": clk.summary(),
-            "parity": parity,
-        }
+        line = {"metric": METRIC, "value": res["value"], "unit": "GTEPS/iter", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": res["config"], "hbm_gbs": res["hbm_gbs"],
+                "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res.get("e2e"),
+                "e2e_pageable": res.get("e2e_pageable"), "gpu_launches": res["gpu_launches"],
+                "gpu_launches_per_step": res["gpu_launches_per_step"], "clocks": res["clocks"],
+                "parity": parity, "reference_gpu": ref_gpu, "secondary": secondary}
         print(json.dumps(line), flush=True)
-    pg.set_stream(None)
+    pg.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -550,12 +661,20 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="rmat22")
+    ap.add_argument("--workload", default="rmat25w",
+                    help="rmat<scale>[w] (rmat25w: the scale-25 weighted config, rmat22: the scale-22 config), "
+                         "ppr, batch, serving, precision25")
+    ap.add_argument("--secondary", default="rmat22",
+                    help="a second plain-PageRank workload measured the same way and reported inside the line "
+                         "('' for none)")
     ap.add_argument("--sweeps", type=int, default=SWEEPS)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-pageable", action="store_true", help="skip the end-to-end leg from pageable memory")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own cuSPARSE solve on the same graph")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default sweep layout (a profiler then sees only the timed launches)")
     ap.add_argument("--serving-max-n", type=float, default=1e7)

@@ -190,6 +190,8 @@ struct egpr_graph {
     int32_t n_dangling = 0;        // out-weight <= 0 (reference mask)
     int32_t n_dangling_solve = 0;  // out-weight <= 1e-15 (EasyGraph CPU rule)
     double prep_seconds = 0.0;
+    int32_t host_inputs_registered = 0;  // host input arrays page-locked for the upload
+    int32_t host_inputs_locked = 0;      // host input arrays that were page-locked already
     // prepared graph
     egpr::DevBuf in_row, in_col, in_w, outw, dangling01, hub_ids, hub_slot, hubz, hubz64;
     // the sweep's layout (see build_sweep_layout)

@@ -60,6 +60,8 @@ struct NaState {
     int32_t ndang;
     uint32_t exited;            // blocks that left the running sweep
     int32_t pad;
+    unsigned long long t_begin; // global timer (ns) when the solve's first kernel started
+    unsigned long long t_end;   // global timer (ns) when its last kernel ran
 };
 
 constexpr size_t kStateBytes = 256;
@@ -99,8 +101,16 @@ __device__ __forceinline__ double na_fx_join(unsigned long long hi, unsigned lon
     return (double)(long long)hi * (1.0 / 4294967296.0) + (double)lo * (1.0 / 18446744073709551616.0);
 }
 
+__device__ __forceinline__ unsigned long long na_global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __global__ void k_na_reset(unsigned char* base, int32_t n, double alpha, double tol, int32_t max_iter) {
     NaState* st = na_view(base).st;
+    st->t_begin = na_global_ns();
+    st->t_end = 0ull;
     for (int i = 0; i < 6; ++i) st->acc[i] = 0ull;
     st->alpha = alpha;
     st->c1 = (1.0 - alpha) / (double)n;
@@ -269,6 +279,10 @@ __global__ void k_na_normalize(unsigned char* base, int32_t n, double* __restric
     }
 }
 
+// Device time stamp after every kernel of the solve (stream order): the
+// solve's device time is t_end - t_begin, taken without creating events.
+__global__ void k_na_stamp(unsigned char* base) { na_view(base).st->t_end = na_global_ns(); }
+
 // Device address of g_scratch, looked up once per device with that device
 // current.  In host code the name g_scratch stands for a host-side shadow, not
 // for device memory, so kernels get this address instead.
@@ -298,7 +312,10 @@ extern "C" EGPR_API int egpr_pagerank_device_noalloc(int32_t n, int64_t nnz, con
                                                      egpr_stats* stats) {
     using namespace egpr;
     const auto t0 = std::chrono::steady_clock::now();
-    if (n <= 0) return EGPR_SUCC;
+    if (n <= 0) {
+        if (stats) *stats = egpr_stats{};  // nothing to solve: zero sweeps, zero time
+        return EGPR_SUCC;
+    }
     if (n > kNoAllocMaxVertices)
         return arg_error("egpr_pagerank_device_noalloc: n exceeds the 262144-vertex limit of its fixed scratch");
     if (nnz < 0 || nnz > (int64_t)INT32_MAX) return arg_error("egpr_pagerank_device_noalloc: nnz out of range");
@@ -326,6 +343,7 @@ extern "C" EGPR_API int egpr_pagerank_device_noalloc(int32_t n, int64_t nnz, con
     if (correction)
         k_na_sweep<true><<<blocks_r, kThreadsNa, 0, s>>>(base, n, nnz, in_row, in_col, in_w, out_weight, ranks);
     k_na_normalize<<<blocks_v, kThreadsNa, 0, s>>>(base, n, ranks, correction ? 0 : 1);
+    k_na_stamp<<<1, 1, 0, s>>>(base);
     if ((e = cudaGetLastError()) != cudaSuccess) return set_cuda_error(e, "no-alloc solve launch");
     if (stats) {
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return set_cuda_error(e, "no-alloc solve");
@@ -336,10 +354,10 @@ extern "C" EGPR_API int egpr_pagerank_device_noalloc(int32_t n, int64_t nnz, con
         stats->iterations = h.iter;
         stats->converged = h.converged;
         stats->residual = h.residual;
-        stats->kernel_seconds = secs;
+        stats->kernel_seconds = h.t_end > h.t_begin ? (double)(h.t_end - h.t_begin) * 1e-9 : 0.0;
         stats->total_seconds = secs;
         stats->bytes_per_iter = (int64_t)(n + 1) * 4 + nnz * (in_w ? 8 : 4) + (int64_t)n * 20;
-        stats->launches = 4 + max_iter + (correction ? 1 : 0);
+        stats->launches = 5 + max_iter + (correction ? 1 : 0);
         stats->reserved = 0;
     }
     return EGPR_SUCC;

@@ -4,8 +4,10 @@
 // (gpu_easygraph/functions/centrality/pagerank.cu:286-347) and its H2D of the
 // result (:472-518) with GPU kernels over the uploaded out-edge CSR:
 //
-//   k_out_weight     FP64 out-weight sum per source, accumulated in row order
-//                    after sanitising each weight (pagerank.cu:301-316)
+//   k_out_weight_exact  FP64 out-weight sum per source after sanitising each
+//                    weight, bit-identical to the sequential sum in row order
+//                    (pagerank.cu:301-316): one warp per source where the sum
+//                    is provably order-free, one thread per source otherwise
 //   k_in_degree      in-degree histogram over valid endpoints (:315)
 //   exclusive scan   in_row (:319-320)
 //   radix sort       stable LSD sort of entry ids by destination: entries of
@@ -26,10 +28,12 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cctype>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "egpr_internal.cuh"
@@ -215,36 +219,86 @@ __device__ __forceinline__ double sanitize_w(double w) {
     return (!isfinite(w) || w < 0.0) ? 0.0 : w;
 }
 
-// FP64 out-weight sum per source in entry order (pagerank.cu:301-316).  For
-// unit weights the sum is a count, which is exact in any order.
-__global__ void k_out_weight(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
-                             const double* __restrict__ W, int32_t n, int32_t r0, int32_t r1,
-                             double* __restrict__ outw, uint32_t* __restrict__ hub_key,
-                             uint32_t* __restrict__ hub_val) {
-    for (int64_t u = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < r1;
-         u += (int64_t)gridDim.x * blockDim.x) {
+// Exponent of the lowest set bit of a finite w > 0: w = M * 2^q with M odd.
+__device__ __forceinline__ int lsb_exponent(double w) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(w);
+    const int ef = (int)((b >> 52) & 0x7ffull);
+    unsigned long long m = b & 0xfffffffffffffull;
+    int e = -1074;  // subnormal: w = m * 2^-1074
+    if (ef != 0) {
+        m |= 1ull << 52;
+        e = ef - 1075;
+    }
+    return e + __ffsll((long long)m) - 1;
+}
+
+// FP64 out-weight sums, one warp per source, bit-identical to the sequential
+// sum in entry order (pagerank.cu:301-316) without summing sequentially.
+// Sanitised weights are >= 0; let 2^q be the lowest set bit among a row's
+// nonzero weights.  Every partial sum, in any order, is then a multiple of
+// 2^q no larger than the row's total T, so when T < 2^(q+53) every partial sum
+// is an exact double and the lanes' sums and the shuffle tree give T, which
+// is also what the sequential loop gives.  The computed sum s is within a few
+// ulps of T, so s < 2^(q+52) proves T < 2^(q+53).  A row that fails the test
+// (weights of very different scales) is listed and summed sequentially by
+// k_out_weight_serial.  Weights drawn as FP32 values, as in the synthetic
+// workloads, always pass.
+__global__ void k_out_weight_exact(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
+                                   const double* __restrict__ W, int32_t n, int32_t r0, int32_t r1,
+                                   double* __restrict__ outw, uint32_t* __restrict__ hub_key,
+                                   uint32_t* __restrict__ hub_val, int32_t* __restrict__ serial_rows,
+                                   uint32_t* __restrict__ serial_count) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = r0 + warp; u < r1; u += nwarps) {
         const int32_t b = V[u], e = V[u + 1];
         double s = 0.0;
         int32_t c = 0;
-        if (W) {
-            for (int32_t p = b; p < e; ++p) {
-                const int32_t v = E[p];
-                if (v >= 0 && v < n) {
-                    s += sanitize_w(W[p]);
-                    ++c;
-                }
+        int q = 4096;  // no nonzero weight yet
+        for (int32_t p = b + lane; p < e; p += 32) {
+            const int32_t v = E[p];
+            if (v >= 0 && v < n) {
+                const double w = sanitize_w(W[p]);
+                s += w;
+                ++c;
+                if (w > 0.0) q = min(q, lsb_exponent(w));
             }
-        } else {
-            for (int32_t p = b; p < e; ++p) {
-                const int32_t v = E[p];
-                c += (v >= 0 && v < n) ? 1 : 0;
-            }
-            s = (double)c;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+            c += __shfl_xor_sync(0xffffffffu, c, o);
+            q = min(q, __shfl_xor_sync(0xffffffffu, q, o));
+        }
+        if (lane == 0) {
+            bool exact;
+            if (q == 4096) exact = true;             // only zero weights: the sum is 0
+            else if (q + 52 >= 1024) exact = false;  // 2^(q+52) would overflow: sum sequentially
+            else exact = s < ldexp(1.0, q + 52);
+            if (exact) outw[u] = s;
+            else serial_rows[atomicAdd(serial_count, 1u)] = (int32_t)u;
+            // hub ranking: descending out-degree, ascending id (stable sort of ~count)
+            hub_key[u] = ~(uint32_t)c;
+            hub_val[u] = (uint32_t)u;
+        }
+    }
+}
+
+// The rows k_out_weight_exact could not prove order-free: summed in entry
+// order, one thread per row, exactly as pagerank.cu:301-316 does.
+__global__ void k_out_weight_serial(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
+                                    const double* __restrict__ W, int32_t n, const int32_t* __restrict__ rows,
+                                    const uint32_t* __restrict__ count, double* __restrict__ outw) {
+    const uint32_t k = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+        const int32_t u = rows[i];
+        double s = 0.0;
+        for (int32_t p = V[u]; p < V[u + 1]; ++p) {
+            const int32_t v = E[p];
+            if (v >= 0 && v < n) s += sanitize_w(W[p]);
         }
         outw[u] = s;
-        // hub ranking: descending out-degree, ascending id (stable sort of ~count)
-        hub_key[u] = ~(uint32_t)c;
-        hub_val[u] = (uint32_t)u;
     }
 }
 
@@ -836,12 +890,73 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
     return cuda_ok(cudaStreamSynchronize(s), "sweep layout");
 }
 
+// Host inputs of the upload, page-locked in place for the copy, with the
+// switches and threshold of the reference's prepare_h2d_source /
+// release_h2d_source (gpu_easygraph/common/buffer_cache.h:115-176):
+// EASYGRAPH_GPU_HOST_REGISTER (default on; when set, on only for 1/TRUE/ON/YES)
+// and EASYGRAPH_GPU_HOST_REGISTER_MIN_BYTES (default 1 MiB).  An array that is
+// already page-locked (cudaErrorHostMemoryAlreadyRegistered) is used as it is
+// and left registered; an array that cannot be registered is copied from
+// pageable memory by the driver.  Read-only mappings (memory-mapped bulk CSR
+// files) are registered read-only where the device supports it.
+bool host_register_enabled() {
+    const char* v = std::getenv("EASYGRAPH_GPU_HOST_REGISTER");
+    if (!v) return true;
+    std::string s(v);
+    for (char& c : s) c = (char)std::toupper((unsigned char)c);
+    return s == "1" || s == "TRUE" || s == "ON" || s == "YES";
+}
+
+size_t host_register_min_bytes() {
+    const char* v = std::getenv("EASYGRAPH_GPU_HOST_REGISTER_MIN_BYTES");
+    const unsigned long long parsed = v ? std::strtoull(v, nullptr, 10) : 0ull;
+    return parsed > 0ull ? (size_t)parsed : (size_t)1 << 20;
+}
+
+struct HostInputPins {
+    cudaStream_t stream;            // the upload's stream: drained before unregistering
+    std::vector<void*> registered;  // unregistered when the upload is done
+    int registered_count = 0;
+    explicit HostInputPins(cudaStream_t s) : stream(s) {}
+    int already_locked = 0;
+    void pin(const void* p, size_t bytes, int dev) {
+        if (!p || bytes == 0 || !host_register_enabled() || bytes < host_register_min_bytes()) return;
+        int ro = 0;
+        cudaDeviceGetAttribute(&ro, cudaDevAttrHostRegisterReadOnlySupported, dev);
+        unsigned flags = cudaHostRegisterPortable | (ro ? cudaHostRegisterReadOnly : 0u);
+        cudaError_t e = cudaHostRegister(const_cast<void*>(p), bytes, flags);
+        if (e == cudaSuccess) {
+            registered.push_back(const_cast<void*>(p));
+            ++registered_count;
+        } else if (e == cudaErrorHostMemoryAlreadyRegistered) {
+            cudaGetLastError();  // not ours to unregister
+            ++already_locked;
+        } else {
+            cudaGetLastError();  // the driver copies from pageable memory instead
+        }
+    }
+    ~HostInputPins() {
+        if (registered.empty()) return;
+        cudaStreamSynchronize(stream);  // no copy from these pages may still be in flight
+        for (void* p : registered) cudaHostUnregister(p);
+        cudaGetLastError();
+    }
+};
+
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W) {
     const int32_t n = g->n;
     const int64_t m = g->m_input;
     cudaStream_t s = g->own_stream;
     int rc = EGPR_SUCC;
     const double t0 = wall_seconds();
+    // declared before the scratch so that the pins outlive every copy (the
+    // stream is synchronised before this function returns)
+    HostInputPins pins(s);
+    pins.pin(V, ((size_t)n + 1) * sizeof(int32_t), g->device);
+    pins.pin(E, (size_t)m * sizeof(int32_t), g->device);
+    pins.pin(W, W ? (size_t)m * sizeof(double) : 0, g->device);
+    g->host_inputs_registered = pins.registered_count;
+    g->host_inputs_locked = pins.already_locked;
     cudaEventRecord(g->ev0, s);
     {
         TmpAlloc tmp(s);
@@ -859,7 +974,11 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         uint32_t* hval = tmp.get<uint32_t>((size_t)n, &rc);
         uint32_t* hkey2 = tmp.get<uint32_t>((size_t)n, &rc);
         uint32_t* hval2 = tmp.get<uint32_t>((size_t)n, &rc);
+        // weighted: rows whose out-weight is summed sequentially (k_out_weight_exact)
+        int32_t* serial_rows = W ? tmp.get<int32_t>((size_t)n, &rc) : nullptr;
+        uint32_t* serial_count = W ? tmp.get<uint32_t>(1, &rc) : nullptr;
         if (rc) return rc;
+        if (W) cudaMemsetAsync(serial_count, 0, sizeof(uint32_t), s);
         // in_row, hub_slot: bulk copies of a stage's rows may read up to 3 elements past the end.
         if ((rc = g->in_row.alloc(((size_t)n + 8) * sizeof(int32_t))) ||
             (rc = g->outw.alloc((size_t)n * sizeof(double))) ||
@@ -912,8 +1031,9 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                 if (i + 1 < pieces) r_end = (int32_t)(std::upper_bound(V, V + n + 1, (int32_t)b) - V) - 1;
                 if (r_end > r_done) {
                     if (dW)
-                        k_out_weight<<<grid_for(r_end - r_done), kThreads, 0, s>>>(dV, dE, dW, n, r_done, r_end,
-                                                                                   g->outw.as<double>(), hkey, hval);
+                        k_out_weight_exact<<<grid_for((int64_t)(r_end - r_done) * 32), kThreads, 0, s>>>(
+                            dV, dE, dW, n, r_done, r_end, g->outw.as<double>(), hkey, hval, serial_rows,
+                            serial_count);
                     else
                         k_out_degree<<<grid_for((int64_t)(r_end - r_done) * 32), kThreads, 0, s>>>(
                             dV, dE, n, r_done, r_end, g->outw.as<double>(), hkey, hval);
@@ -929,6 +1049,9 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             for (cudaEvent_t e : ev)
                 if (e) cudaEventDestroy(e);
             if (rc) return rc;
+            if (dW && n > 0)
+                k_out_weight_serial<<<grid_for(n), kThreads, 0, s>>>(dV, dE, dW, n, serial_rows, serial_count,
+                                                                     g->outw.as<double>());
         }
         if ((rc = exclusive_scan_u32(indeg, reinterpret_cast<uint32_t*>(g->in_row.as<int32_t>()), (int64_t)n + 1, s)))
             return rc;

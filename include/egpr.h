@@ -256,7 +256,14 @@ EGPR_API int egpr_pagerank_csr(const int32_t* V, int32_t len_V, const int32_t* E
  * call reuses the array, so calls that overlap on the GPU (other threads or
  * other streams) race and give wrong results: serialise them.  Work is
  * enqueued on `stream` (a cudaStream_t, NULL = default stream); with stats
- * non-NULL the call waits for it and fills stats.
+ * non-NULL the call waits for it and fills stats (kernel_seconds: device time
+ * from the first to the last kernel of the solve, read from the GPU's global
+ * timer; n <= 0 zeroes stats).  Every one of the max_iter sweeps is launched:
+ * sweeps after convergence return at once but each still costs a kernel
+ * launch (a few microseconds), so pick max_iter near the sweeps needed.  The
+ * array's device address is cached per device for the life of the process;
+ * after cudaDeviceReset on that device the cached address is stale, so do not
+ * reset a device between calls.
  */
 EGPR_API int egpr_pagerank_device_noalloc(int32_t n, int64_t nnz, const int32_t* in_row, const int32_t* in_col,
                                           const float* in_w, const double* out_weight, double alpha,

@@ -62,6 +62,29 @@ def test_preparation_bit_exact_rmat(scale, weighted):
     assert pg.info()["n_dangling"] == int(od.sum())
 
 
+@pytest.mark.parametrize("kind", ["fp32_values", "full_doubles", "mixed_scales"])
+def test_out_weight_sums_bit_exact_with_the_sequential_sum(kind):
+    """The out-weight sums are taken in parallel where that is provably the
+    sequential sum and sequentially elsewhere: bit-identical to the
+    reference's sequential FP64 loop (pagerank.cu:301-316) either way, on
+    long rows (R-MAT hubs) and for weights that force the sequential path."""
+    g = synth.rmat(scale=15, edgefactor=16, seed=41)
+    rng = np.random.Generator(np.random.PCG64(41))
+    if kind == "fp32_values":  # the synthetic workloads' weights: always order-free
+        W = (1.0 - rng.random(g.m, dtype=np.float32)).astype(np.float64)
+    elif kind == "full_doubles":  # 53-bit mantissas: long rows need the sequential path
+        W = rng.random(g.m)
+    else:  # several rows mix weights 2^100 apart, plus zeros, NaN and negatives
+        W = rng.random(g.m) * np.where(rng.random(g.m) < 0.5, 2.0**60, 2.0**-40)
+        W[rng.random(g.m) < 0.01] = 0.0
+        W[rng.random(g.m) < 0.001] = np.nan
+        W[rng.random(g.m) < 0.001] = -1.0
+    pg = _native.PreparedGraph(g.V, g.E, W)
+    _, _, _, _, outw = pg.export_inbound()
+    _, _, _, _, oout = oracle.build_inbound(g.V, g.E, W)
+    assert np.array_equal(outw.view(np.uint64), oout.view(np.uint64))
+
+
 @pytest.mark.parametrize("case", golden_small_cases(), ids=lambda c: c[0])
 def test_reference_small_cases_through_the_api(case, monkeypatch):
     monkeypatch.setenv("EASYGRAPH_ENABLE_GPU", "TRUE")
