@@ -103,10 +103,14 @@ def install():
         EASYGRAPH_ENABLE_GPU is on (easygraph's own CPU code otherwise; C++
         graphs keep easygraph's routing to its C++ CPU PageRank).
     """
+    import importlib
+
     try:
         import easygraph as eg  # type: ignore
-        from easygraph.functions.centrality import pagerank as pr_mod  # type: ignore
-        from easygraph.utils import gpu_eggpu_backend as eb  # type: ignore
+        # the submodule itself: in easygraph the package attribute
+        # easygraph.functions.centrality.pagerank is the re-exported function
+        pr_mod = importlib.import_module("easygraph.functions.centrality.pagerank")
+        eb = importlib.import_module("easygraph.utils.gpu_eggpu_backend")
     except Exception:  # noqa: BLE001
         return False
     if _INSTALLED:
@@ -134,9 +138,16 @@ def install():
     eb.pagerank = backend_pagerank
     pr_mod.pagerank = eg_pagerank
     eg.pagerank = eg_pagerank
-    if hasattr(eg, "functions"):
-        try:
-            eg.functions.pagerank = eg_pagerank
-        except Exception:  # noqa: BLE001
-            pass
+    # the re-exports of the function on the package path
+    for path in ("functions", "functions.centrality"):
+        obj = eg
+        for part in path.split("."):
+            obj = getattr(obj, part, None)
+            if obj is None:
+                break
+        if obj is not None and getattr(obj, "pagerank", None) is original:
+            try:
+                obj.pagerank = eg_pagerank
+            except Exception:  # noqa: BLE001
+                pass
     return True

@@ -6,17 +6,24 @@
 // the normalisation), the multi-graph plan cache and the keyed prepared-graph
 // cache behind the drop-in egpr_pagerank_csr.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <list>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -255,6 +262,14 @@ int check_device(const egpr_graph* g) {
     return EGPR_SUCC;
 }
 
+// ---- profiler ranges ------------------------------------------------------------
+// NVTX ranges around the phases of a call (prepare, solve, readback, tune), so a
+// profiler's timeline shows where host time goes; free when no tool listens.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
 static int cuda_ok(cudaError_t e, const char* what) { return e == cudaSuccess ? EGPR_SUCC : set_cuda_error(e, what); }
 
 static int64_t plain_bytes_per_iter(int64_t n, int64_t nnz, bool weighted) {
@@ -298,6 +313,12 @@ static int read_states(Plan& plan, int32_t idx, cudaStream_t s, SolveOut* o) {
     o->launches = ctl.launches;
     o->error = ctl.error;
     return EGPR_SUCC;
+}
+
+// The state of a graph's last single-vector solve (binned or tile sweep).
+static int read_single_state(egpr_graph* g, cudaStream_t s, SolveOut* o) {
+    if (!g->bins) return read_states(g->plan, 0, s, o);
+    return bins_read_state(g, s, &o->iterations, &o->converged, &o->residual, &o->launches, &o->error);
 }
 
 static void fill_stats(egpr_stats* stats, const egpr_graph* g, const SolveOut& o, double kernel_s,
@@ -377,16 +398,24 @@ static int solve_single(egpr_graph* g, double alpha, int32_t max_iter, double to
     cudaStream_t s = g->stream;
     std::vector<float> staging;
     if (pers && (rc = upload_teleport(g, pers, s, staging))) return rc;
-    if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event"))) return rc;
+    const bool personalised = pers != nullptr || tele_on_device;
+    if (personalised && g->bins && (rc = bins_upload_tele(g, s))) return rc;
     int32_t host_launches = 0;
-    if ((rc = enqueue_plan(g->plan, alpha, max_iter, tol, pers != nullptr || tele_on_device, flags, s,
-                           &host_launches)))
-        return rc;
-    if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
+    {
+        NvtxRange nv("egpr solve");
+        if ((rc = cuda_ok(cudaEventRecord(g->ev0, s), "event"))) return rc;
+        if (g->bins)
+            rc = bins_enqueue(g, alpha, max_iter, tol, personalised, flags, s, &host_launches);
+        else
+            rc = enqueue_plan(g->plan, alpha, max_iter, tol, personalised, flags, s, &host_launches);
+        if (rc) return rc;
+        if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
+    }
+    NvtxRange nv_read("egpr readback");
     if ((rc = cuda_ok(cudaMemcpyAsync(out, g->out.p, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ranks")))
         return rc;
     SolveOut o;
-    if ((rc = read_states(g->plan, 0, s, &o))) return rc;
+    if ((rc = read_single_state(g, s, &o))) return rc;
     if (o.error) {
         t_last_error = "sweep launch cap reached";
         return o.error;
@@ -489,7 +518,7 @@ int64_t egpr_graph::device_bytes() const {
                      plan.d_span_list.bytes +
                      scale.bytes + tele.bytes + x0.bytes + x1.bytes + z0.bytes + z1.bytes + out.bytes + z64.bytes +
                      plan.d_chunks.bytes + plan.d_graphs.bytes + plan.d_states.bytes + plan.d_ndang.bytes +
-                     plan.d_ctl.bytes);
+                     plan.d_ctl.bytes) + (bins ? bins->device_bytes() : 0);
 }
 
 using namespace egpr;
@@ -502,6 +531,8 @@ static void destroy_graph_object(egpr_graph* g) {
     if (g->device >= 0 && cur != g->device) cudaSetDevice(g->device);
     if (g->own_stream) cudaStreamSynchronize(g->own_stream);
     spmm_work_release(g);
+    delete g->bins;
+    g->bins = nullptr;
     g->plan.release();
     for (DevBuf* b : {&g->in_row, &g->in_col, &g->in_w, &g->outw, &g->dangling01, &g->sw_row,
                       &g->sw_col, &g->sw_w, &g->tile_bits, &g->tile_row,
@@ -514,6 +545,129 @@ static void destroy_graph_object(egpr_graph* g) {
     if (cur >= 0 && cur != g->device) cudaSetDevice(cur);
     g_live_graphs -= 1;
     delete g;
+}
+
+// ---- persisted layout choices ------------------------------------------------------
+// egpr_graph_autotune records its choice per GPU model and graph-shape bucket
+// (log2 of n, log2 of the mean degree, weighted or not) in a small text file:
+// EGPR_TUNE_CACHE names it (EGPR_TUNE_CACHE=0 turns the store off), default
+// $XDG_CACHE_HOME/eggpu_b200/tuning.txt or ~/.cache/eggpu_b200/tuning.txt.  A
+// graph prepared later (egpr_graph_create, and so egpr_pagerank_csr) whose
+// shape falls in a recorded bucket starts with that layout, unless the layout
+// is fixed through EGPR_CHUNKS_PER_WARP / EGPR_ROW_COST / EGPR_SPMM_CHUNK.
+// One line per bucket: key, chunks_per_warp, row_cost, spmm_chunk, sweep ms.
+namespace {
+std::mutex g_tune_mu;
+
+std::string tune_store_path() {
+    const char* e = std::getenv("EGPR_TUNE_CACHE");
+    if (e && e[0] == '0' && e[1] == 0) return std::string();
+    if (e && e[0]) return std::string(e);
+    const char* x = std::getenv("XDG_CACHE_HOME");
+    const char* h = std::getenv("HOME");
+    std::string dir = (x && x[0]) ? std::string(x) : (h && h[0]) ? std::string(h) + "/.cache" : std::string("/tmp");
+    return dir + "/eggpu_b200/tuning.txt";
+}
+
+int floor_log2(uint64_t x) {
+    int b = -1;
+    while (x) {
+        x >>= 1;
+        ++b;
+    }
+    return b;
+}
+
+std::string tune_key(int dev, int32_t n, int64_t m, bool weighted) {
+    static std::mutex name_mu;
+    static std::map<int, std::string> names;
+    std::string name;
+    {
+        std::lock_guard<std::mutex> lk(name_mu);
+        auto it = names.find(dev);
+        if (it == names.end()) {
+            cudaDeviceProp pr = {};
+            if (cudaGetDeviceProperties(&pr, dev) != cudaSuccess) {
+                cudaGetLastError();
+                std::snprintf(pr.name, sizeof(pr.name), "device%d", dev);
+            }
+            std::string nm(pr.name);
+            for (char& c : nm)
+                if (c == ' ' || c == '\t') c = '_';
+            it = names.emplace(dev, nm).first;
+        }
+        name = it->second;
+    }
+    const int ln = floor_log2((uint64_t)std::max<int32_t>(n, 1));
+    const int ld = floor_log2((uint64_t)std::max<int64_t>(m / std::max<int32_t>(n, 1), 1));
+    return name + "|n2^" + std::to_string(ln) + "|d2^" + std::to_string(ld) + "|w" + (weighted ? "1" : "0");
+}
+
+bool tune_lookup(const std::string& key, egpr_tuning* out) {
+    const std::string path = tune_store_path();
+    if (path.empty()) return false;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream ss(line);
+        std::string k;
+        egpr_tuning t = {};
+        if (!(ss >> k >> t.chunks_per_warp >> t.row_cost >> t.spmm_chunk >> t.sweep_ms)) continue;
+        if (k == key) {
+            *out = t;
+            return true;
+        }
+    }
+    return false;
+}
+
+void tune_record(const std::string& key, const egpr_tuning& t) {
+    const std::string path = tune_store_path();
+    if (path.empty()) return;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::vector<std::string> keep;
+    {
+        std::ifstream f(path);
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream ss(line);
+            std::string k;
+            if ((ss >> k) && k != key) keep.push_back(line);
+        }
+    }
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos) {
+        const std::string dir = path.substr(0, slash);
+        for (size_t i = 1; i <= dir.size(); ++i)  // the directory chain, part by part
+            if (i == dir.size() || dir[i] == '/') {
+                const std::string part = dir.substr(0, i);
+                if (!part.empty()) ::mkdir(part.c_str(), 0755);
+            }
+    }
+    const std::string tmp = path + ".tmp" + std::to_string((long long)::getpid());
+    {
+        std::ofstream o(tmp, std::ios::trunc);
+        if (!o) return;
+        for (const std::string& l : keep) o << l << "\n";
+        o << key << " " << t.chunks_per_warp << " " << t.row_cost << " " << t.spmm_chunk << " " << t.sweep_ms << "\n";
+    }
+    std::rename(tmp.c_str(), path.c_str());
+}
+}  // namespace
+
+// The recorded layout of a graph of this shape, if any (before preparation).
+void apply_recorded_tuning(egpr_graph* g) {
+    if (std::getenv("EGPR_CHUNKS_PER_WARP") || std::getenv("EGPR_ROW_COST") || std::getenv("EGPR_SPMM_CHUNK")) return;
+    egpr_tuning t = {};
+    if (!tune_lookup(tune_key(g->device, g->n, g->m_input, g->weighted != 0), &t)) return;
+    if (t.chunks_per_warp >= 1 && t.chunks_per_warp <= 64 && t.row_cost >= 0 && t.row_cost <= 64 &&
+        t.spmm_chunk >= 64 && t.spmm_chunk <= (1 << 16) && (t.spmm_chunk % 32) == 0) {
+        g->tune_cpw = t.chunks_per_warp;
+        g->tune_rc = t.row_cost;
+        g->tune_spmm_chunk = t.spmm_chunk;
+        g->tuning_recorded = 1;
+    }
 }
 
 // ---- layout tuning ----------------------------------------------------------
@@ -646,9 +800,13 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
     g->tune_cpw = default_chunks_per_warp();
     g->tune_rc = default_row_cost();
     g->tune_spmm_chunk = default_spmm_chunk();
-    if ((rc = prepare_graph(g, V, E, W))) {
-        destroy_graph_object(g);
-        return rc;
+    apply_recorded_tuning(g);
+    {
+        NvtxRange r("egpr prepare");
+        if ((rc = prepare_graph(g, V, E, W))) {
+            destroy_graph_object(g);
+            return rc;
+        }
     }
     // Row arrays are read by 16-byte bulk copies that may run up to 3 elements past n.
     const size_t nf = ((size_t)n + 8) * sizeof(float), nd = (size_t)n * sizeof(double);
@@ -752,6 +910,7 @@ int egpr_graph_set_tuning(egpr_graph* g, const egpr_tuning* in) {
 
 int egpr_graph_autotune(egpr_graph* g, uint32_t what, egpr_tuning* out) {
     if (!g) return fail_arg("NULL graph");
+    NvtxRange nv("egpr autotune");
     if (what == 0) what = EGPR_TUNE_SWEEP | EGPR_TUNE_SPMM;
     std::lock_guard<std::mutex> lk(g->mu);
     if (g->pending) return fail_arg("a solve is pending on this graph");
@@ -805,6 +964,7 @@ int egpr_graph_autotune(egpr_graph* g, uint32_t what, egpr_tuning* out) {
     res.chunks_per_warp = g->tune_cpw;
     res.row_cost = g->tune_rc;
     res.spmm_chunk = g->tune_spmm_chunk;
+    if (g->nnz > 0) tune_record(tune_key(g->device, g->n, g->m_input, g->weighted != 0), res);
     if (out) *out = res;
     return EGPR_SUCC;
 }
@@ -838,7 +998,11 @@ int egpr_pagerank_enqueue(egpr_graph* g, double alpha, int32_t max_iter, double 
     g->pending_launches = 0;
     if (g->nnz > 0) {
         if ((rc = cuda_ok(cudaEventRecord(g->ev0, g->stream), "event"))) return rc;
-        if ((rc = enqueue_plan(g->plan, alpha, max_iter, tol, false, flags, g->stream, &g->pending_launches))) return rc;
+        if (g->bins)
+            rc = bins_enqueue(g, alpha, max_iter, tol, false, flags, g->stream, &g->pending_launches);
+        else
+            rc = enqueue_plan(g->plan, alpha, max_iter, tol, false, flags, g->stream, &g->pending_launches);
+        if (rc) return rc;
         if ((rc = cuda_ok(cudaEventRecord(g->ev1, g->stream), "event"))) return rc;
     }
     g->pending = true;
@@ -861,7 +1025,7 @@ int egpr_pagerank_collect(egpr_graph* g, double* out_ranks, egpr_stats* stats) {
         (rc = cuda_ok(cudaMemcpyAsync(out_ranks, g->out.p, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ranks")))
         return rc;
     SolveOut o;
-    if ((rc = read_states(g->plan, 0, s, &o))) return rc;
+    if ((rc = read_single_state(g, s, &o))) return rc;
     if (o.error) return o.error;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);

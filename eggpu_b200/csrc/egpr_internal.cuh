@@ -54,7 +54,8 @@ constexpr int kTileWords = 16;
 // largest out-degree are kept in shared memory by the sweep; inbound entries
 // from a hub store -(slot + 1) instead of the source id.  Slot nhub holds 0 and
 // is read by the placeholder entry of every row without entries.
-constexpr int kHubCap = 32768;
+constexpr int kHubCap = 49152;      // largest hub cache (values) a sweep CTA stages
+constexpr int kHubDefault = 32768;  // hub cache of a prepared graph unless EGPR_HUBS says otherwise
 
 // Per-graph device view used by the sweep kernels.
 struct GraphDev {
@@ -177,6 +178,71 @@ struct Plan {
 
 struct SpmmWork;  // batched personalised PageRank workspace (spmm.cu)
 
+// ---------------------------------------------------------------------------
+// The binned single-graph sweep (bins.cu; layout built in prep.cu).
+//
+// Vertices are renumbered: first the H sources of largest out-degree (the hub
+// block, whose carried values the sweep stages in shared memory, so a source
+// id below H is a shared-memory read), then every other vertex; inside each
+// block vertices go by descending in-degree.  The inbound CSR in that order
+// keeps, per row, the entries in ascending original-source order.  Rows of
+// one length class are then contiguous, and the work queue holds:
+//   kBinPiece  a piece of a long row (>= bin_piece entries), one warp; a row cut
+//              into several pieces is finished by the last piece to arrive
+//              (pieces add exact fixed-point sums)
+//   kBinGroup  rows [r0, r1) of one length class, G lanes per row with G a
+//              power of two sized so that each lane gathers 4..8 entries
+//   kBinEmpty  rows [r0, r1) without inbound entries (teleport and dangling
+//              terms only)
+// ---------------------------------------------------------------------------
+constexpr int32_t kBinPiece = 0;
+constexpr int32_t kBinGroup = 1;
+constexpr int32_t kBinEmpty = 2;
+
+struct BinItem {
+    int32_t kind;
+    int32_t r0, r1;  // rows [r0, r1); kBinPiece: r0 is the row
+    int32_t e0, e1;  // kBinPiece: entries [e0, e1)
+    int32_t span;    // kBinPiece: span slot of a row cut into several pieces, -1 for one piece
+    int32_t parts;   // kBinPiece: pieces of the row; kBinGroup: lanes per row (G)
+    int32_t pad;
+};
+
+struct BinLayout {
+    int32_t n = 0;
+    int32_t hubs = 0;            // hub block [0, hubs)
+    int64_t nnz = 0;
+    DevBuf perm;                 // n: new id of each vertex
+    DevBuf inv;                  // n: vertex of each new id
+    DevBuf row;                  // n + 1 (+ pad): offsets of the renumbered inbound CSR
+    DevBuf col;                  // nnz (+ pad): renumbered sources
+    DevBuf w;                    // nnz (+ pad): FP32 weights (weighted graphs)
+    DevBuf outw;                 // n: FP64 out-weight sums, renumbered
+    std::vector<int32_t> h_row_bounds;  // row offsets at the class boundaries (host copy, item building)
+    // work queue
+    DevBuf items;
+    int32_t nitems = 0;
+    int32_t nspans = 0;
+    int32_t piece = 2048;        // entries per piece of a long row (tuning)
+    int32_t group_entries = 4096;  // target entries of a kBinGroup item (tuning)
+    // per-solve state (renumbered)
+    DevBuf scale, tele, x, z, z64, out64, states, ctl, acc, span_acc, span_cnt;
+    int32_t acc_slots = 0;
+    int32_t grid = 0;
+    cudaGraph_t cg = nullptr;
+    cudaGraphExec_t cg_exec = nullptr;
+    cudaGraphConditionalHandle cond = 0;
+    bool cg_failed = false;
+    int64_t device_bytes() const {
+        int64_t b = 0;
+        for (const DevBuf* d : {&perm, &inv, &row, &col, &w, &outw, &items, &scale, &tele, &x, &z, &z64, &out64, &states,
+                                &ctl, &acc, &span_acc, &span_cnt})
+            b += (int64_t)d->bytes;
+        return b;
+    }
+    ~BinLayout();
+};
+
 // ---- prepared graph handle ---------------------------------------------------
 }  // namespace egpr
 
@@ -192,6 +258,7 @@ struct egpr_graph {
     double prep_seconds = 0.0;
     int32_t host_inputs_registered = 0;  // host input arrays page-locked for the upload
     int32_t host_inputs_locked = 0;      // host input arrays that were page-locked already
+    int32_t host_inputs_staged = 0;      // host input arrays copied through the staging pool
     // prepared graph
     egpr::DevBuf in_row, in_col, in_w, outw, dangling01, hub_ids, hub_slot, hubz, hubz64;
     // the sweep's layout (see build_sweep_layout)
@@ -203,11 +270,13 @@ struct egpr_graph {
     int32_t tune_cpw = 8;           // sweep: work-queue chunks per resident warp
     int32_t tune_rc = 4;            // sweep: cost of finishing a row, in entries
     int32_t tune_spmm_chunk = 1024; // batched solve: entries per work unit
+    int32_t tuning_recorded = 0;    // the layout came from the persisted tuner choices
     // solve workspace
     egpr::DevBuf scale, tele, x0, x1, z0, z1, out, z64;
     egpr::DevBuf seed_ids;         // seed set of a single-vector PPR solve
     egpr::Plan plan;               // single-graph plan
     egpr::SpmmWork* spmm = nullptr; // batched personalised PageRank workspace
+    egpr::BinLayout* bins = nullptr; // binned single-graph sweep (null: the tile sweep serves single solves)
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr; // active stream (own or user-given)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -240,6 +309,17 @@ int default_chunks_per_warp();  // EGPR_CHUNKS_PER_WARP, else 8
 int default_row_cost();         // EGPR_ROW_COST, else 4
 int32_t default_spmm_chunk();   // EGPR_SPMM_CHUNK, else 1024
 int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
+
+// Binned single-graph sweep (bins.cu).
+bool bins_wanted(int32_t n, int64_t nnz);  // build the binned layout for this graph (EGPR_BINS, size)
+int32_t bin_hub_cap();                      // hub block size limit (shared memory of one CTA)
+int bins_build_items(egpr_graph* g, cudaStream_t s);
+int bins_alloc_solve(egpr_graph* g, cudaStream_t s);
+int bins_upload_tele(egpr_graph* g, cudaStream_t s);  // renumbers g->tele into the layout's order
+int bins_enqueue(egpr_graph* g, double alpha, int32_t max_iter, double tol, bool personalised, uint32_t flags,
+                 cudaStream_t s, int32_t* host_launches);
+int bins_read_state(egpr_graph* g, cudaStream_t s, int32_t* iterations, int32_t* converged, double* residual,
+                    int32_t* launches, int32_t* error);
 
 // Plans and sweeps (sweep.cu).
 int sweep_grid();

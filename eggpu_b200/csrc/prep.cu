@@ -10,13 +10,12 @@
 //                    is provably order-free, one thread per source otherwise
 //   k_in_degree      in-degree histogram over valid endpoints (:315)
 //   exclusive scan   in_row (:319-320)
-//   radix sort       stable LSD sort of entry ids by destination: entries of
+//   radix sort       stable LSD sort of the entries by destination: entries of
 //                    one destination keep ascending entry order, i.e. the
 //                    ascending-source order of the reference's sequential
-//                    scatter (:328-346)
-//   k_gather_inbound in_col / in_w from the sorted entry ids (weighted; with
-//                    unit weights the pairs carry the source, and the sorted
-//                    values are in_col)
+//                    scatter (:328-346); the sorted pairs carry each entry's
+//                    source and, when weighted, its FP32 weight, so the sorted
+//                    values are in_col and in_w
 //   k_dangling       dangling mask outw <= 0 (:323-326) and the counts used by
 //                    the solver
 //
@@ -127,12 +126,13 @@ k_radix_hist(const uint32_t* __restrict__ keys, int64_t len, int shift, int64_t 
 // order; inside a warp, rounds of 32 consecutive items rank equal digits by
 // lane order.  Global order = tile order (digit-major scanned histogram),
 // then warp order, then item order.  keys_out may be NULL (last pass: only
-// the values are needed).
-template <int kBits>
+// the values are needed).  kTwo: a second value array moves with the first.
+template <int kBits, bool kTwo>
 __global__ void __launch_bounds__(kThreads)
 k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t len,
-                int shift, int64_t ntiles, const uint32_t* __restrict__ offsets) {
+                int shift, int64_t ntiles, const uint32_t* __restrict__ offsets,
+                const uint32_t* __restrict__ vals2_in, uint32_t* __restrict__ vals2_out) {
     constexpr int kD = 1 << kBits;
     extern __shared__ uint32_t radix_smem[];
     uint32_t (*warp_hist)[kD] = reinterpret_cast<uint32_t (*)[kD]>(radix_smem);  // [kWarps][kD]
@@ -142,7 +142,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
     for (int d = tid; d < kD; d += kThreads) tile_off[d] = offsets[(int64_t)d * ntiles + blockIdx.x];
     __syncthreads();
     const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortPerLane;
-    uint32_t key[kSortPerLane], val[kSortPerLane], rank[kSortPerLane];
+    uint32_t key[kSortPerLane], val[kSortPerLane], val2[kTwo ? kSortPerLane : 1], rank[kSortPerLane];
     const uint32_t lt_mask = (1u << lane) - 1u;
 #pragma unroll
     for (int r = 0; r < kSortPerLane; ++r) {
@@ -150,6 +150,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         const bool valid = idx < len;
         key[r] = valid ? keys_in[idx] : 0u;
         val[r] = valid ? vals_in[idx] : 0u;
+        if (kTwo) val2[r] = valid ? vals2_in[idx] : 0u;
         const uint32_t d = (key[r] >> shift) & (kD - 1);
         const uint32_t tag = valid ? d : (uint32_t)(kD + lane);
         const uint32_t peers = __match_any_sync(0xffffffffu, tag);
@@ -192,6 +193,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
     // then warp, then item), then each digit's run written out contiguously
     uint32_t* skey = dstart + kD;          // [kSortTile]
     uint32_t* sval = skey + kSortTile;     // [kSortTile]
+    uint32_t* sval2 = sval + kSortTile;    // [kSortTile] (kTwo)
 #pragma unroll
     for (int r = 0; r < kSortPerLane; ++r) {
         const int64_t idx = wbase + (int64_t)r * 32 + lane;
@@ -200,6 +202,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
             const uint32_t lpos = dstart[d] + warp_hist[warp][d] + rank[r];
             skey[lpos] = key[r];
             sval[lpos] = val[r];
+            if (kTwo) sval2[lpos] = val2[r];
         }
     }
     __syncthreads();
@@ -211,6 +214,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         const uint32_t dst = tile_off[d] + ((uint32_t)i - dstart[d]);
         if (keys_out) keys_out[dst] = k;
         vals_out[dst] = sval[i];
+        if (kTwo) vals2_out[dst] = sval2[i];
     }
 }
 
@@ -356,15 +360,13 @@ __global__ void k_decode_hubs(const int32_t* __restrict__ in_col, int64_t nnz, c
 // In-degree histogram and the sort keys: destination, or n for an entry whose
 // destination is outside [0, n) (those sort last and are dropped).
 __global__ void k_in_degree_keys(const int32_t* __restrict__ E, int64_t p0, int64_t p1, int32_t n,
-                                 uint32_t* __restrict__ indeg, uint32_t* __restrict__ keys,
-                                 uint32_t* __restrict__ vals) {
+                                 uint32_t* __restrict__ indeg, uint32_t* __restrict__ keys) {
     for (int64_t p = p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < p1;
          p += (int64_t)gridDim.x * blockDim.x) {
         const int32_t v = E[p];
         const bool ok = v >= 0 && v < n;
         if (ok) atomicAdd(&indeg[v], 1u);
         keys[p] = ok ? (uint32_t)v : (uint32_t)n;
-        if (vals) vals[p] = (uint32_t)p;  // weighted: the entry id (its weight is gathered after the sort)
     }
 }
 
@@ -379,15 +381,11 @@ __global__ void k_expand_src(const int32_t* __restrict__ V, int32_t n, int32_t* 
     }
 }
 
-__global__ void k_gather_inbound(const uint32_t* __restrict__ sorted_ids, int64_t nnz,
-                                 const int32_t* __restrict__ src, const double* __restrict__ W,
-                                 int32_t* __restrict__ in_col, float* __restrict__ in_w) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t p = sorted_ids[i];
-        in_col[i] = src[p];
-        if (in_w) in_w[i] = (float)sanitize_w(W[p]);
-    }
+// FP32 bits of each entry's sanitised weight (the stored in_w), for entries [p0, p1).
+__global__ void k_weight_bits(const double* __restrict__ W, int64_t p0, int64_t p1, uint32_t* __restrict__ out) {
+    for (int64_t p = p0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < p1;
+         p += (int64_t)gridDim.x * blockDim.x)
+        out[p] = __float_as_uint((float)sanitize_w(W[p]));
 }
 
 __global__ void k_dangling(const double* __restrict__ outw, int32_t n, int32_t* __restrict__ mask,
@@ -463,12 +461,12 @@ struct TmpAlloc {
     }
 };
 
-template <int kBits>
+template <int kBits, bool kTwo>
 int radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int64_t len, int shift,
-               bool last, int64_t ntiles, uint32_t* hist, cudaStream_t s) {
+               bool last, int64_t ntiles, uint32_t* hist, cudaStream_t s, const uint32_t* v2in, uint32_t* v2out) {
     constexpr int kD = 1 << kBits;
     // warp histograms, tile offsets, digit starts, and the tile's keys and values
-    const size_t smem = ((size_t)(kWarps + 2) * kD + 2 * (size_t)kSortTile) * sizeof(uint32_t);
+    const size_t smem = ((size_t)(kWarps + 2) * kD + (kTwo ? 3 : 2) * (size_t)kSortTile) * sizeof(uint32_t);
     // The shared-memory opt-in is a per-device attribute of the function: made
     // once per device (bit d of the mask; devices past 63 repeat it, which is
     // harmless).  Atomic: several host threads prepare graphs at once.
@@ -477,14 +475,14 @@ int radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_
     if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
     const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
     if (!bit || !(attr_devices.load(std::memory_order_acquire) & bit)) {
-        cudaFuncSetAttribute(k_radix_scatter<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_radix_scatter<kBits, kTwo>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr_devices.fetch_or(bit, std::memory_order_release);
     }
     k_radix_hist<kBits><<<(unsigned)ntiles, kThreads, 0, s>>>(kin, len, shift, ntiles, hist);
     int rc = exclusive_scan_u32(hist, hist, ntiles * kD, s);
     if (rc) return rc;
-    k_radix_scatter<kBits><<<(unsigned)ntiles, kThreads, smem, s>>>(kin, vin, last ? nullptr : kout, vout, len, shift,
-                                                                    ntiles, hist);
+    k_radix_scatter<kBits, kTwo><<<(unsigned)ntiles, kThreads, smem, s>>>(kin, vin, last ? nullptr : kout, vout, len,
+                                                                          shift, ntiles, hist, v2in, v2out);
     return EGPR_SUCC;
 }
 
@@ -493,7 +491,7 @@ int radix_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_
 // alongside except in the last pass, which writes values only.
 int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
                      int64_t len, int bits, cudaStream_t s, TmpAlloc& tmp, bool* result_in_alt,
-                     bool keys_needed = true) {
+                     bool keys_needed = true, uint32_t* vals2 = nullptr, uint32_t* vals2_alt = nullptr) {
     *result_in_alt = false;
     if (len <= 1 || bits <= 0) return EGPR_SUCC;
     int rc = EGPR_SUCC;
@@ -504,14 +502,16 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_
     const int64_t ntiles = (len + kSortTile - 1) / kSortTile;
     uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles << 8, &rc);
     if (!hist) return rc;
-    uint32_t *kin = keys, *vin = vals, *kout = keys_alt, *vout = vals_alt;
+    uint32_t *kin = keys, *vin = vals, *kout = keys_alt, *vout = vals_alt, *v2in = vals2, *v2out = vals2_alt;
     for (int p = 0; p < passes; ++p) {
         const int shift = p * 8;
         const bool last = p == passes - 1 && !keys_needed;
-        rc = radix_pass<8>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s);
+        rc = vals2 ? radix_pass<8, true>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, v2in, v2out)
+                   : radix_pass<8, false>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, nullptr, nullptr);
         if (rc) return rc;
         std::swap(kin, kout);
         std::swap(vin, vout);
+        std::swap(v2in, v2out);
     }
     *result_in_alt = (vin == vals_alt);
     return cuda_ok(cudaGetLastError(), "radix sort");
@@ -890,18 +890,125 @@ int build_sweep_layout(egpr_graph* g, int32_t resident_warps, const uint32_t* so
     return cuda_ok(cudaStreamSynchronize(s), "sweep layout");
 }
 
-// Host inputs of the upload, page-locked in place for the copy, with the
-// switches and threshold of the reference's prepare_h2d_source /
-// release_h2d_source (gpu_easygraph/common/buffer_cache.h:115-176):
-// EASYGRAPH_GPU_HOST_REGISTER (default on; when set, on only for 1/TRUE/ON/YES)
-// and EASYGRAPH_GPU_HOST_REGISTER_MIN_BYTES (default 1 MiB).  An array that is
-// already page-locked (cudaErrorHostMemoryAlreadyRegistered) is used as it is
-// and left registered; an array that cannot be registered is copied from
-// pageable memory by the driver.  Read-only mappings (memory-mapped bulk CSR
-// files) are registered read-only where the device supports it.
-bool host_register_enabled() {
+// ---- the binned sweep's layout -------------------------------------------------
+// Renumbering key of vertex v: the hub block (the first `hubs` vertices of the
+// out-degree ranking) first, then everyone else; descending in-degree inside
+// each block; the sort is stable, so equal keys keep ascending vertex ids.
+__global__ void k_bin_keys(const int32_t* __restrict__ in_row, int32_t n, const uint8_t* __restrict__ hub_flag,
+                           uint32_t* __restrict__ key, uint32_t* __restrict__ val) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t deg = (uint32_t)(in_row[v + 1] - in_row[v]);
+        key[v] = (hub_flag[v] ? 0u : 0x80000000u) | (0x7fffffffu - deg);
+        val[v] = (uint32_t)v;
+    }
+}
+
+__global__ void k_bin_hub_flags(const uint32_t* __restrict__ ranked, int32_t hubs, uint8_t* __restrict__ flag) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hubs; i += gridDim.x * blockDim.x) flag[ranked[i]] = 1;
+}
+
+// inv: the sorted vertex list; perm[inv[i]] = i; row lengths and FP64
+// out-weights in the new order.
+__global__ void k_bin_perm(const uint32_t* __restrict__ inv, int32_t n, const int32_t* __restrict__ in_row,
+                           const double* __restrict__ outw, int32_t* __restrict__ perm, uint32_t* __restrict__ len,
+                           double* __restrict__ outw_new) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = (int32_t)inv[i];
+        perm[v] = (int32_t)i;
+        len[i] = (uint32_t)(in_row[v + 1] - in_row[v]);
+        outw_new[i] = outw[v];
+    }
+}
+
+// Inbound entry e (destination dst[e], source in_col[e]) to its place in the
+// renumbered CSR: same position inside its row, source renumbered.
+__global__ void k_bin_entries(const uint32_t* __restrict__ dst, int64_t nnz, const int32_t* __restrict__ in_row,
+                              const int32_t* __restrict__ in_col, const float* __restrict__ in_w,
+                              const int32_t* __restrict__ perm, const int32_t* __restrict__ row_new,
+                              int32_t* __restrict__ col_new, float* __restrict__ w_new) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = (int32_t)dst[e];
+        const int64_t pos = (int64_t)row_new[perm[v]] + (e - (int64_t)in_row[v]);
+        col_new[pos] = perm[in_col[e]];
+        if (w_new) w_new[pos] = in_w[e];
+    }
+}
+
+// Builds g->bins from the natural inbound CSR (in_row, plain source ids in
+// in_col, in_w, outw) and the out-degree ranking of the vertices.  The work
+// queue follows in bins_build_items.
+int build_bin_layout(egpr_graph* g, const uint32_t* sorted_dst, const uint32_t* ranked, TmpAlloc& tmp,
+                     cudaStream_t s) {
+    const int32_t n = g->n;
+    const int64_t nnz = g->nnz;
+    BinLayout* B = new (std::nothrow) BinLayout();
+    if (!B) return EGPR_FAILED_TO_ALLOCATE_HOST_MEM;
+    g->bins = B;
+    B->n = n;
+    B->nnz = nnz;
+    B->hubs = std::min<int32_t>(n, bin_hub_cap()) & ~3;  // a multiple of 4: the staging copy moves 16-byte units
+    if (const char* e = std::getenv("EGPR_BIN_HUBS")) B->hubs = std::min<int32_t>(B->hubs, std::max(0, atoi(e)) & ~3);
+    int rc = EGPR_SUCC;
+    uint8_t* flag = tmp.get<uint8_t>((size_t)n, &rc);
+    uint32_t* key = tmp.get<uint32_t>((size_t)n, &rc);
+    uint32_t* val = tmp.get<uint32_t>((size_t)n, &rc);
+    uint32_t* key2 = tmp.get<uint32_t>((size_t)n, &rc);
+    uint32_t* val2 = tmp.get<uint32_t>((size_t)n, &rc);
+    uint32_t* len = tmp.get<uint32_t>((size_t)n + 1, &rc);
+    if (rc) return rc;
+    // Every array the sweep reads row by row is padded by 16 entries (vector
+    // loads near the end); the padding is zero.
+    const size_t pad = 16;
+    if ((rc = B->perm.alloc((size_t)n * sizeof(int32_t))) || (rc = B->inv.alloc((size_t)n * sizeof(int32_t))) ||
+        (rc = B->row.alloc(((size_t)n + 1 + pad) * sizeof(int32_t))) ||
+        (rc = B->col.alloc(((size_t)std::max<int64_t>(nnz, 1) + pad) * sizeof(int32_t))) ||
+        (rc = B->outw.alloc(((size_t)n + pad) * sizeof(double))) ||
+        (g->weighted && (rc = B->w.alloc(((size_t)std::max<int64_t>(nnz, 1) + pad) * sizeof(float)))))
+        return rc;
+    cudaMemsetAsync(flag, 0, (size_t)n, s);
+    cudaMemsetAsync(len, 0, ((size_t)n + 1) * sizeof(uint32_t), s);  // len[n] = 0 closes the scan
+    cudaMemsetAsync(B->row.p, 0, B->row.bytes, s);
+    cudaMemsetAsync(B->col.p, 0, B->col.bytes, s);
+    if (g->weighted) cudaMemsetAsync(B->w.p, 0, B->w.bytes, s);
+    if (B->hubs > 0) k_bin_hub_flags<<<grid_for(B->hubs), kThreads, 0, s>>>(ranked, B->hubs, flag);
+    k_bin_keys<<<grid_for(n), kThreads, 0, s>>>(g->in_row.as<int32_t>(), n, flag, key, val);
+    bool alt = false;
+    if ((rc = radix_sort_pairs(key, val, key2, val2, n, 32, s, tmp, &alt, false))) return rc;
+    const uint32_t* inv = alt ? val2 : val;
+    cudaMemcpyAsync(B->inv.p, inv, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    k_bin_perm<<<grid_for(n), kThreads, 0, s>>>(inv, n, g->in_row.as<int32_t>(), g->outw.as<double>(),
+                                                B->perm.as<int32_t>(), len, B->outw.as<double>());
+    if ((rc = exclusive_scan_u32(len, reinterpret_cast<uint32_t*>(B->row.as<int32_t>()), (int64_t)n + 1, s)))
+        return rc;
+    if (nnz > 0)
+        k_bin_entries<<<grid_for(nnz), kThreads, 0, s>>>(sorted_dst, nnz, g->in_row.as<int32_t>(),
+                                                         g->in_col.as<int32_t>(), g->weighted ? g->in_w.as<float>() : nullptr,
+                                                         B->perm.as<int32_t>(), B->row.as<int32_t>(),
+                                                         B->col.as<int32_t>(), g->weighted ? B->w.as<float>() : nullptr);
+    if ((rc = cuda_ok(cudaGetLastError(), "binned layout"))) return rc;
+    if ((rc = bins_build_items(g, s))) return rc;
+    return bins_alloc_solve(g, s);
+}
+
+// ---- host inputs ------------------------------------------------------------
+// A host input array reaches the device in one of three ways:
+//  * already page-locked (torch pinned memory, cudaHostAlloc, a registered
+//    range): copied by DMA directly;
+//  * pageable, with EASYGRAPH_GPU_HOST_REGISTER set to 1/TRUE/ON/YES:
+//    page-locked in place for the upload and released after it, as the
+//    reference's prepare_h2d_source / release_h2d_source do
+//    (gpu_easygraph/common/buffer_cache.h:115-176), for arrays of at least
+//    EASYGRAPH_GPU_HOST_REGISTER_MIN_BYTES (default 1 MiB); read-only
+//    mappings (memory-mapped bulk CSR files) are registered read-only where
+//    the device supports it;
+//  * pageable otherwise (the default here; the reference registers by
+//    default): copied through a process-wide pool of page-locked staging
+//    buffers, host threads filling one buffer while DMA drains the others.
+//    Registering pages in place cost about 0.2 s per GB on B200 hosts, several
+//    times the copy itself, and it is paid again on every call.
+bool host_register_requested() {
     const char* v = std::getenv("EASYGRAPH_GPU_HOST_REGISTER");
-    if (!v) return true;
+    if (!v) return false;
     std::string s(v);
     for (char& c : s) c = (char)std::toupper((unsigned char)c);
     return s == "1" || s == "TRUE" || s == "ON" || s == "YES";
@@ -913,29 +1020,120 @@ size_t host_register_min_bytes() {
     return parsed > 0ull ? (size_t)parsed : (size_t)1 << 20;
 }
 
-struct HostInputPins {
-    cudaStream_t stream;            // the upload's stream: drained before unregistering
-    std::vector<void*> registered;  // unregistered when the upload is done
-    int registered_count = 0;
-    explicit HostInputPins(cudaStream_t s) : stream(s) {}
-    int already_locked = 0;
-    void pin(const void* p, size_t bytes, int dev) {
-        if (!p || bytes == 0 || !host_register_enabled() || bytes < host_register_min_bytes()) return;
-        int ro = 0;
-        cudaDeviceGetAttribute(&ro, cudaDevAttrHostRegisterReadOnlySupported, dev);
-        unsigned flags = cudaHostRegisterPortable | (ro ? cudaHostRegisterReadOnly : 0u);
-        cudaError_t e = cudaHostRegister(const_cast<void*>(p), bytes, flags);
-        if (e == cudaSuccess) {
-            registered.push_back(const_cast<void*>(p));
-            ++registered_count;
-        } else if (e == cudaErrorHostMemoryAlreadyRegistered) {
-            cudaGetLastError();  // not ours to unregister
-            ++already_locked;
-        } else {
-            cudaGetLastError();  // the driver copies from pageable memory instead
-        }
+bool host_page_locked(const void* p) {
+    cudaPointerAttributes a = {};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
     }
-    ~HostInputPins() {
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Page-locked staging buffers shared by every upload of the process (one
+// upload at a time uses them).
+constexpr int kStageSlots = 4;
+constexpr size_t kStageBytes = (size_t)32 << 20;
+struct StagePool {
+    std::mutex mu;
+    void* slot[kStageSlots] = {};
+};
+StagePool& stage_pool() {
+    static StagePool* p = new StagePool();  // never destroyed: pinned memory outlives static teardown order
+    return *p;
+}
+
+void parallel_memcpy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kBlock = (size_t)1 << 20;
+    const int64_t blocks = (int64_t)((bytes + kBlock - 1) / kBlock);
+    if (blocks <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+#pragma omp parallel for schedule(static) num_threads(std::min<int64_t>(blocks, 16))
+    for (int64_t i = 0; i < blocks; ++i) {
+        const size_t off = (size_t)i * kBlock;
+        std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off,
+                    std::min(kBlock, bytes - off));
+    }
+}
+
+// H2D copy of a pageable host array through the staging pool, enqueued on s.
+// Returns once every byte has left the source array (later work on s sees
+// the data in stream order).
+int staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    StagePool& P = stage_pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    for (int k = 0; k < kStageSlots; ++k)
+        if (!P.slot[k]) {
+            const cudaError_t e = cudaHostAlloc(&P.slot[k], kStageBytes, cudaHostAllocPortable);
+            if (e != cudaSuccess) {
+                P.slot[k] = nullptr;
+                cudaGetLastError();
+                // no staging memory: the driver copies from pageable memory
+                return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "H2D (pageable)");
+            }
+        }
+    cudaEvent_t ev[kStageSlots] = {};
+    bool used[kStageSlots] = {};
+    int rc = EGPR_SUCC;
+    for (int k = 0; k < kStageSlots && !rc; ++k)
+        rc = cuda_ok(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming), "event");
+    size_t off = 0;
+    for (int i = 0; off < bytes && !rc; ++i) {
+        const int k = i % kStageSlots;
+        const size_t len = std::min(kStageBytes, bytes - off);
+        if (used[k] && (rc = cuda_ok(cudaEventSynchronize(ev[k]), "staging"))) break;
+        parallel_memcpy(P.slot[k], static_cast<const char*>(src) + off, len);
+        if ((rc = cuda_ok(cudaMemcpyAsync(static_cast<char*>(dst) + off, P.slot[k], len, cudaMemcpyHostToDevice, s),
+                          "H2D (staged)")))
+            break;
+        if ((rc = cuda_ok(cudaEventRecord(ev[k], s), "event"))) break;
+        used[k] = true;
+        off += len;
+    }
+    // the slots are free again once their last copies are done
+    for (int k = 0; k < kStageSlots; ++k) {
+        if (used[k]) cudaEventSynchronize(ev[k]);
+        if (ev[k]) cudaEventDestroy(ev[k]);
+    }
+    return rc;
+}
+
+struct HostInputs {
+    cudaStream_t stream;            // the upload's stream: drained before unregistering
+    std::vector<void*> registered;  // registered here, unregistered when the upload is done
+    int registered_count = 0;
+    int already_locked = 0;
+    int staged = 0;
+    explicit HostInputs(cudaStream_t s) : stream(s) {}
+    // Decides how `p` is uploaded; true when it is (now) page-locked.
+    bool prepare(const void* p, size_t bytes, int dev) {
+        if (!p || bytes == 0) return true;
+        if (host_page_locked(p)) {
+            ++already_locked;
+            return true;
+        }
+        if (host_register_requested() && bytes >= host_register_min_bytes()) {
+            int ro = 0;
+            cudaDeviceGetAttribute(&ro, cudaDevAttrHostRegisterReadOnlySupported, dev);
+            const unsigned flags = cudaHostRegisterPortable | (ro ? cudaHostRegisterReadOnly : 0u);
+            const cudaError_t e = cudaHostRegister(const_cast<void*>(p), bytes, flags);
+            if (e == cudaSuccess) {
+                registered.push_back(const_cast<void*>(p));
+                ++registered_count;
+                return true;
+            }
+            cudaGetLastError();
+            if (e == cudaErrorHostMemoryAlreadyRegistered) {  // not ours to unregister
+                ++already_locked;
+                return true;
+            }
+        }
+        if (bytes >= ((size_t)1 << 20)) ++staged;
+        return bytes < ((size_t)1 << 20);  // small arrays: the driver's pageable copy
+    }
+    ~HostInputs() {
         if (registered.empty()) return;
         cudaStreamSynchronize(stream);  // no copy from these pages may still be in flight
         for (void* p : registered) cudaHostUnregister(p);
@@ -943,20 +1141,28 @@ struct HostInputPins {
     }
 };
 
+// H2D of [src, src + bytes): direct when `locked`, else through the staging pool.
+int upload_h2d(void* dst, const void* src, size_t bytes, bool locked, cudaStream_t s, const char* what) {
+    if (bytes == 0) return EGPR_SUCC;
+    if (locked) return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), what);
+    return staged_h2d(dst, src, bytes, s);
+}
+
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W) {
     const int32_t n = g->n;
     const int64_t m = g->m_input;
     cudaStream_t s = g->own_stream;
     int rc = EGPR_SUCC;
     const double t0 = wall_seconds();
-    // declared before the scratch so that the pins outlive every copy (the
-    // stream is synchronised before this function returns)
-    HostInputPins pins(s);
-    pins.pin(V, ((size_t)n + 1) * sizeof(int32_t), g->device);
-    pins.pin(E, (size_t)m * sizeof(int32_t), g->device);
-    pins.pin(W, W ? (size_t)m * sizeof(double) : 0, g->device);
-    g->host_inputs_registered = pins.registered_count;
-    g->host_inputs_locked = pins.already_locked;
+    // declared before the scratch so that registrations outlive every copy
+    // (the stream is synchronised before this function returns)
+    HostInputs host(s);
+    const bool v_locked = host.prepare(V, ((size_t)n + 1) * sizeof(int32_t), g->device);
+    const bool e_locked = host.prepare(E, (size_t)m * sizeof(int32_t), g->device);
+    const bool w_locked = host.prepare(W, W ? (size_t)m * sizeof(double) : 0, g->device);
+    g->host_inputs_registered = host.registered_count;
+    g->host_inputs_locked = host.already_locked;
+    g->host_inputs_staged = host.staged;
     cudaEventRecord(g->ev0, s);
     {
         TmpAlloc tmp(s);
@@ -968,7 +1174,9 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         uint32_t* vals = tmp.get<uint32_t>((size_t)m, &rc);
         uint32_t* keys2 = tmp.get<uint32_t>((size_t)m, &rc);
         uint32_t* vals2 = tmp.get<uint32_t>((size_t)m, &rc);
-        int32_t* src = W ? tmp.get<int32_t>((size_t)m, &rc) : nullptr;  // weighted: source of every entry
+        // weighted: the FP32 weight of every entry moves through the sort with its source
+        uint32_t* wbits = W ? tmp.get<uint32_t>((size_t)m, &rc) : nullptr;
+        uint32_t* wbits2 = W ? tmp.get<uint32_t>((size_t)m, &rc) : nullptr;
         unsigned long long* counts = tmp.get<unsigned long long>(2, &rc);
         uint32_t* hkey = tmp.get<uint32_t>((size_t)n, &rc);
         uint32_t* hval = tmp.get<uint32_t>((size_t)n, &rc);
@@ -984,13 +1192,13 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             (rc = g->outw.alloc((size_t)n * sizeof(double))) ||
             (rc = g->dangling01.alloc((size_t)n * sizeof(int32_t))))
             return rc;
-        if ((rc = cuda_ok(cudaMemcpyAsync(dV, V, ((size_t)n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D offsets")))
-            return rc;
+        if ((rc = upload_h2d(dV, V, ((size_t)n + 1) * sizeof(int32_t), v_locked, s, "H2D offsets"))) return rc;
         cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * sizeof(uint32_t), s);
         cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s);
-        // unit weights: the sort carries each entry's source (written from the
-        // offsets alone, while E is still arriving), so no gather follows it
-        if (!W && m > 0)
+        // the sort carries each entry's source (written from the offsets alone,
+        // while E is still arriving) and, when weighted, its FP32 weight
+        // (converted as each piece of W arrives), so no gather follows it
+        if (m > 0)
             k_expand_src<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, n, reinterpret_cast<int32_t*>(vals));
         {
             // E (and W) arrive in pieces on a copy stream; the degree passes of
@@ -1015,11 +1223,9 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                 const int64_t a = m * i / pieces, b = m * (i + 1) / pieces;
                 cudaStream_t cs = pieces > 1 ? sc : s;
                 if (b > a) {
-                    rc = cuda_ok(cudaMemcpyAsync(dE + a, E + a, (size_t)(b - a) * sizeof(int32_t), cudaMemcpyHostToDevice, cs),
-                                 "H2D indices");
+                    rc = upload_h2d(dE + a, E + a, (size_t)(b - a) * sizeof(int32_t), e_locked, cs, "H2D indices");
                     if (!rc && W)
-                        rc = cuda_ok(cudaMemcpyAsync(dW + a, W + a, (size_t)(b - a) * sizeof(double),
-                                                     cudaMemcpyHostToDevice, cs), "H2D weights");
+                        rc = upload_h2d(dW + a, W + a, (size_t)(b - a) * sizeof(double), w_locked, cs, "H2D weights");
                 }
                 if (!rc && pieces > 1) {
                     rc = cuda_ok(cudaEventRecord(ev[(size_t)i], sc), "event");
@@ -1040,7 +1246,8 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                     r_done = r_end;
                 }
                 if (b > a)
-                    k_in_degree_keys<<<grid_for(b - a), kThreads, 0, s>>>(dE, a, b, n, indeg, keys, W ? vals : nullptr);
+                    k_in_degree_keys<<<grid_for(b - a), kThreads, 0, s>>>(dE, a, b, n, indeg, keys);
+                if (b > a && W) k_weight_bits<<<grid_for(b - a), kThreads, 0, s>>>(dW, a, b, wbits);
             }
             if (sc) {
                 if (rc) cudaStreamSynchronize(sc);
@@ -1075,33 +1282,41 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
             int bits = 0;
             while (bits < 32 && (kmax >> bits) != 0) ++bits;
             bool alt = false;
-            if ((rc = radix_sort_pairs(keys, vals, keys2, vals2, m, bits, s, tmp, &alt))) return rc;
+            if ((rc = radix_sort_pairs(keys, vals, keys2, vals2, m, bits, s, tmp, &alt, true, wbits, wbits2)))
+                return rc;
             const uint32_t* sorted_vals = alt ? vals2 : vals;
             sorted_dst = alt ? keys2 : keys;
-            if (!W) {
-                if (nnz > 0 && (rc = cuda_ok(cudaMemcpyAsync(g->in_col.p, sorted_vals, (size_t)nnz * sizeof(int32_t),
-                                                             cudaMemcpyDeviceToDevice, s), "inbound sources")))
-                    return rc;
-            } else {
-                k_expand_src<<<grid_for((int64_t)n * 32), kThreads, 0, s>>>(dV, n, src);
-                if (nnz > 0)
-                    k_gather_inbound<<<grid_for(nnz), kThreads, 0, s>>>(sorted_vals, nnz, src, dW,
-                                                                       g->in_col.as<int32_t>(), g->in_w.as<float>());
-            }
+            if (nnz > 0 && (rc = cuda_ok(cudaMemcpyAsync(g->in_col.p, sorted_vals, (size_t)nnz * sizeof(int32_t),
+                                                         cudaMemcpyDeviceToDevice, s), "inbound sources")))
+                return rc;
+            if (W && nnz > 0 &&
+                (rc = cuda_ok(cudaMemcpyAsync(g->in_w.p, alt ? wbits2 : wbits, (size_t)nnz * sizeof(float),
+                                              cudaMemcpyDeviceToDevice, s), "inbound weights")))
+                return rc;
         }
         // Hubs: the min(n, kHubCap) sources of largest out-degree (a multiple of 4,
         // the granule of the shared-memory staging copy).
-        const char* hub_env = std::getenv("EGPR_HUBS");  // EGPR_HUBS=0: no hub cache
-        // (kHubCap - 32 leaves room for the zero slot nhub in a kHubCap-value copy)
-        g->nhub = (hub_env && hub_env[0] == '0') ? 0 : (std::min<int32_t>(n, kHubCap - 32) & ~3);
+        // EGPR_HUBS=N: hub cache size (0: none); at most kHubCap - 32, which leaves
+        // room for the zero slot nhub in a kHubCap-value copy
+        const char* hub_env = std::getenv("EGPR_HUBS");
+        const int32_t hub_want = hub_env ? std::max(0, std::atoi(hub_env)) : kHubDefault - 32;
+        g->nhub = std::min<int32_t>(std::min<int32_t>(n, hub_want), kHubCap - 32) & ~3;
         if ((rc = g->hub_slot.alloc(((size_t)n + 8) * sizeof(int32_t))) ||
             (rc = g->hub_ids.alloc((size_t)std::max(g->nhub + 1, 4) * sizeof(int32_t))) ||
             (rc = cuda_ok(cudaMemsetAsync(g->hub_slot.p, 0xff, ((size_t)n + 8) * sizeof(int32_t), s), "memset")))
             return rc;
-        if (g->nhub > 0) {
+        // the out-degree ranking (descending, ties by id): the hubs of both sweeps
+        const bool want_bins = bins_wanted(n, nnz);
+        const uint32_t* ranked = nullptr;
+        if (g->nhub > 0 || want_bins) {
             bool alt = false;
             if ((rc = radix_sort_pairs(hkey, hval, hkey2, hval2, n, 32, s, tmp, &alt, false))) return rc;
-            k_hub_slots<<<grid_for(g->nhub), kThreads, 0, s>>>(alt ? hval2 : hval, g->nhub, g->hub_ids.as<int32_t>(),
+            ranked = alt ? hval2 : hval;
+        }
+        // the binned layout reads in_col before the hub codes go in
+        if (want_bins && (rc = build_bin_layout(g, sorted_dst, ranked, tmp, s))) return rc;
+        if (g->nhub > 0) {
+            k_hub_slots<<<grid_for(g->nhub), kThreads, 0, s>>>(ranked, g->nhub, g->hub_ids.as<int32_t>(),
                                                                g->hub_slot.as<int32_t>());
             if (nnz > 0)
                 k_encode_hubs<<<grid_for(nnz), kThreads, 0, s>>>(g->in_col.as<int32_t>(), nnz, g->hub_slot.as<int32_t>());

@@ -330,16 +330,16 @@ template <typename Real>
 __device__ void process_chunk(const SweepParams& P, int32_t c, const Chunk& ck, const WarpCtx& X,
                               const float* hub_s, int32_t hub_count, Real* scr) {
     constexpr bool kFinal = std::is_same<Real, double>::value;
-    using Acc = Real;
+    // per-lane sums of the chunk (residual, dangling mass, rank sum) are FP64
+    // in both sweeps: they decide the stop rule and the mass carried into the
+    // next sweep
+    using Acc = double;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int32_t kb = ck.nnz_begin, ke = ck.nnz_end, T0 = kb & ~7;
     const int32_t fl = ck.flags;
     bool head_pending = (fl & kHasHead) && !(fl & kInterior);
     double head_val = 0.0;
-    // per-lane sums of the chunk: residual and dangling mass in FP32 for the
-    // FP32 sweep (they steer the stop rule and the next dangling term, at far
-    // below FP32 iterate resolution), the rank sum always in FP64
     Acc err = Acc(0), dsum = Acc(0);
     double xsum = 0.0;
     Real carry = Real(0);  // the row still open at the end of the previous tile

@@ -160,6 +160,13 @@ typedef struct egpr_tuning {
  * x row_cost in {2, 4, 8} for the sweep, spmm_chunk in {512, 1024, 2048} for
  * the batched solve.  Results do not depend on the layout beyond FP32
  * rounding.  out (nullable) receives the chosen parameters and timings.
+ * The choice is recorded per GPU model and graph-shape bucket (log2 of n,
+ * log2 of the mean degree, weighted or not) in the file EGPR_TUNE_CACHE
+ * names (default $XDG_CACHE_HOME/eggpu_b200/tuning.txt or
+ * ~/.cache/eggpu_b200/tuning.txt; EGPR_TUNE_CACHE=0 turns recording off), and
+ * every graph prepared later whose shape falls in a recorded bucket, through
+ * egpr_graph_create or egpr_pagerank_csr, starts with that layout (unless
+ * EGPR_CHUNKS_PER_WARP, EGPR_ROW_COST or EGPR_SPMM_CHUNK fix it).
  */
 EGPR_API int egpr_graph_autotune(egpr_graph* g, uint32_t what, egpr_tuning* out);
 /* Reads / applies layout parameters (values outside their ranges are refused). */

@@ -31,9 +31,11 @@ def pytest_collection_modifyitems(config, items):
 
 
 @pytest.fixture(autouse=True)
-def _env_guard(monkeypatch):
-    """Each test starts from the reference's default switches (test_eggpu_runtime.py:18-33)."""
+def _env_guard(monkeypatch, tmp_path_factory):
+    """Each test starts from the reference's default switches (test_eggpu_runtime.py:18-33),
+    and the tuner's persisted choices go to a store of the test session, not the user's."""
     for name in ("EASYGRAPH_ENABLE_GPU", "EASYGRAPH_GPU_STRICT_ERRORS", "EASYGRAPH_CPU_PR_MAX_ITER",
                  "EASYGRAPH_CPU_PR_TOL"):
         monkeypatch.delenv(name, raising=False)
+    monkeypatch.setenv("EGPR_TUNE_CACHE", str(tmp_path_factory.getbasetemp() / "tuning.txt"))
     yield

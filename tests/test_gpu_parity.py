@@ -321,6 +321,58 @@ def test_scale22_full_size_properties_and_parity():
     assert np.abs(fixed - ref5).sum() <= L1_TOL
 
 
+def test_config_scale25_weighted_precision_full_size():
+    """The precision config: R-MAT scale 25 (seed 2, edgefactor 16), weights
+    i.i.d. U(0,1] FP32, weighted out-degree normalisation, alpha 0.85, tol
+    1e-7.  The stop rule (one sweep at this size, N*tol = 3.36 > 2) and ten
+    fixed sweeps with and without the FP64 correction sweep, each against the
+    FP64 oracle: iterations within +-1, L1 <= 1e-6 and the reference's
+    per-entry tolerance; max-abs and L1 are printed."""
+    g = synth.rmat(scale=25, edgefactor=16, seed=2, weighted=True)
+    pg = _native.PreparedGraph(g.V, g.E, g.W)
+    inbound = oracle.build_inbound(g.V, g.E, g.W)
+    for label, max_iter, tol, corr in (("rule_tol1e-7", 100, 1e-7, True), ("fixed10", 10, 0.0, True),
+                                       ("fixed10_no_correction", 10, 0.0, False)):
+        ranks, st = pg.pagerank(alpha=0.85, max_iter=max_iter, tol=tol, correction=corr)
+        ref, it, _ = oracle.pagerank_pull(g.V, g.E, g.W, alpha=0.85, max_iter=max_iter, tol=tol, inbound=inbound)
+        assert abs(st["iterations"] - it) <= 1, (label, st["iterations"], it)
+        if st["iterations"] != it:
+            ref, _, _ = oracle.pagerank_pull(g.V, g.E, g.W, alpha=0.85, max_iter=st["iterations"], tol=0.0,
+                                             inbound=inbound)
+        l1 = float(np.abs(ranks - ref).sum())
+        mx = float(np.abs(ranks - ref).max())
+        print(f"scale-25 weighted {label}: iterations {st['iterations']} (oracle {it}), L1 {l1:.3e}, max-abs {mx:.3e}")
+        assert l1 <= L1_TOL, (label, l1)
+        assert np.allclose(ranks, ref, rtol=2e-5, atol=1e-7), label
+        if label == "rule_tol1e-7":
+            assert st["converged"] == 1
+
+
+@pytest.mark.parametrize("case", ["scale14", "scale16w_fixed", "scale15_personalised"])
+def test_binned_layout_opt_in_matches_oracle(case, monkeypatch):
+    """The degree-binned layout (EGPR_BINS=1: vertices renumbered by hub block
+    and in-degree, rows served by length class) gives the oracle's ranks."""
+    monkeypatch.setenv("EGPR_BINS", "1")
+    if case == "scale14":
+        g = synth.rmat(scale=14, edgefactor=16, seed=0)
+        pg = _native.PreparedGraph(g.V, g.E)
+        ranks, st = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+        _check_against_oracle(g.V, g.E, None, ranks, st, 0.85, 100, 1e-6)
+    elif case == "scale16w_fixed":
+        g = synth.rmat(scale=16, edgefactor=16, seed=5, weighted=True)
+        pg = _native.PreparedGraph(g.V, g.E, g.W)
+        for corr in (True, False):
+            ranks, st = pg.pagerank(alpha=0.85, max_iter=12, tol=0.0, correction=corr)
+            assert st["iterations"] == 12
+            _check_against_oracle(g.V, g.E, g.W, ranks, st, 0.85, 12, 0.0)
+    else:
+        g = synth.rmat(scale=15, edgefactor=16, seed=6)
+        pg = _native.PreparedGraph(g.V, g.E)
+        tele = _seed_teleport(g.n, np.array([3, 17, 400, 9000]))
+        ranks, st = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6, personalization=tele)
+        _check_against_oracle(g.V, g.E, None, ranks, st, 0.85, 100, 1e-6, teleport=tele)
+
+
 def _seed_teleport(n, s):
     p = np.zeros(n)
     p[np.unique(s)] = 1.0

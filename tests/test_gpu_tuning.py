@@ -66,3 +66,32 @@ def test_out_of_range_tuning_is_refused():
         with pytest.raises(_native.EgprError):
             pg.set_tuning(**kw)
     assert pg.tuning()["spmm_chunk"] in (512, 1024, 2048) or pg.tuning()["spmm_chunk"] % 32 == 0
+
+
+def test_autotune_choice_is_recorded_and_applied_to_new_graphs(tmp_path, monkeypatch):
+    """egpr_graph_autotune records its choice per GPU model and graph-shape
+    bucket; a graph of the same bucket prepared later starts with it."""
+    store = tmp_path / "tuning.txt"
+    monkeypatch.setenv("EGPR_TUNE_CACHE", str(store))
+    for name in ("EGPR_CHUNKS_PER_WARP", "EGPR_ROW_COST", "EGPR_SPMM_CHUNK"):
+        monkeypatch.delenv(name, raising=False)
+    g = synth.rmat(scale=14, edgefactor=16, seed=44)
+    pg = _native.PreparedGraph(g.V, g.E)
+    pg.autotune(sweep=True, spmm=False)
+    lines = store.read_text().splitlines()
+    assert len(lines) == 1 and "|n2^14|" in lines[0] and lines[0].split()[0].endswith("|w0")
+    # a recorded choice unlike the defaults, to see it applied
+    key = lines[0].split()[0]
+    store.write_text(f"{key} 16 2 512 0.01\n")
+    h = synth.rmat(scale=14, edgefactor=16, seed=45)  # another graph of the same shape bucket
+    ph = _native.PreparedGraph(h.V, h.E)
+    assert ph.tuning() == {"chunks_per_warp": 16, "row_cost": 2, "spmm_chunk": 512}
+    ranks, st = ph.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+    ref, it, _ = oracle.pagerank_pull(h.V, h.E, None, alpha=0.85, max_iter=100, tol=1e-6)
+    assert abs(st["iterations"] - it) <= 1 and np.abs(ranks - ref).sum() <= L1_TOL
+    # a weighted graph is another bucket; the store switched off gives the defaults
+    w = synth.rmat(scale=14, edgefactor=16, seed=45, weighted=True)
+    assert _native.PreparedGraph(w.V, w.E, w.W).tuning() != {"chunks_per_warp": 16, "row_cost": 2,
+                                                            "spmm_chunk": 512}
+    monkeypatch.setenv("EGPR_TUNE_CACHE", "0")
+    assert _native.PreparedGraph(h.V, h.E).tuning() != {"chunks_per_warp": 16, "row_cost": 2, "spmm_chunk": 512}
