@@ -15,8 +15,11 @@ through the drop-in C ABI entry (host CSR in page-locked and in pageable
 memory), parity against the FP64 oracle (stop rule at the config's tolerance
 and fixed 10-sweep solves), the reference's own cuSPARSE GPU solve timed on
 the same graph, the oracle's OpenMP restatement of the reference's CPU path
-timed on the host, and the scale-22 config (R-MAT scale 22, seed 1,
-unweighted) measured the same way as a secondary object.
+timed on the host, the scale-22 config (R-MAT scale 22, seed 1, unweighted)
+measured the same way as a secondary object, and (one GPU) the batched-PPR
+config (R-MAT scale 20, k=256 seed sets) and the serving config (Poisson
+arrivals over 64 graphs, with and without continuous batching), each
+measured after the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload rmat25w|rmat22|rmat<scale>[w]|ppr|batch|serving|precision25]
@@ -420,6 +423,15 @@ def run_ours(args):
                                          res.get("e2e", {}).get("ms_per_step"))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(csr, 0.85, budget_s=args.cpu_seconds)
+    # the batched-PPR and serving configs, measured after the timed region
+    ppr = served = None
+    if rank == 0 and world == 1 and args.with_ppr:
+        res = measure_ppr(args)
+        if res is not None:
+            ppr = {"config": res[1], **res[0]}
+    if rank == 0 and world == 1 and args.with_serving:
+        out, cfg = measure_serving(args)
+        served = {"config": cfg, **out}
     if rank == 0:
         line = {"metric": METRIC, "value": res["value"], "unit": "GTEPS/iter", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
@@ -428,7 +440,8 @@ def run_ours(args):
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res.get("e2e"),
                 "e2e_pageable": res.get("e2e_pageable"), "gpu_launches": res["gpu_launches"],
                 "gpu_launches_per_step": res["gpu_launches_per_step"], "clocks": res["clocks"],
-                "parity": parity, "reference_gpu": ref_gpu, "secondary": secondary}
+                "parity": parity, "reference_gpu": ref_gpu, "secondary": secondary, "ppr": ppr,
+                "serving": served}
         print(json.dumps(line), flush=True)
     pg.close()
     if dist:
@@ -447,10 +460,20 @@ def run_ppr(args):
     k plain single-vector solves on the same GPU; accuracy against the FP64 oracle."""
     import torch
 
+    torch.cuda.set_device(0)
+    res = measure_ppr(args)
+    if res is None:
+        return
+    out, cfg = res
+    line = {"metric": METRIC, "value": out["rule"]["batched_solves_per_s_e2e"], "unit": "PPR solves/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic", "dtype": "f32", "config": cfg, "ppr": out}
+    print(json.dumps(line), flush=True)
+
+
+def measure_ppr(args):
     from eggpu_b200 import _native, synth
     from oracle import oracle
 
-    torch.cuda.set_device(0)
     g = synth.rmat(scale=20, edgefactor=16, seed=3)
     sets = synth.seed_sets(g.n, 256, 1, 64, seed=3)
     pg = _native.PreparedGraph(g.V, g.E)
@@ -459,7 +482,7 @@ def run_ppr(args):
         for _ in range(2):
             _, sts = pg.pagerank_seeds(sets[:k], alpha=0.85, max_iter=4, tol=0.0)
         print(json.dumps({"ppr_profile": {"k": k, "sweeps": 4, "device_ms": sts[0]["kernel_seconds"] * 1e3}}))
-        return
+        return None
     out = {}
     res = _native.pinned_empty((len(sets), g.n))  # the result array a serving caller keeps and reuses
     for label, max_iter, tol in (("rule", 100, 1e-6), ("fixed20", 20, 0.0)):
@@ -493,13 +516,13 @@ def run_ppr(args):
             "iterations_vs_oracle": [(e[2], e[3]) for e in errs],
             "bytes_per_sweep_ppr": sts[0]["bytes_per_iter"],
         }
-    line = {"metric": METRIC, "value": out["rule"]["batched_solves_per_s_e2e"], "unit": "PPR solves/s",
-            "higher_is_better": True, "n_gpus": 1, "data": "synthetic", "dtype": "f32",
-            "config": {"workload": "ppr: R-MAT scale 20 (seed 3, edgefactor 16), k=256 teleport vectors uniform over "
-                                   "seed sets of 1-64 vertices (numpy PCG64 seed 3), alpha 0.85; 'rule' = tol 1e-6 "
-                                   "max_iter 100, 'fixed20' = 20 sweeps", "n": g.n, "nnz": pg.nnz},
-            "ppr": out}
-    print(json.dumps(line), flush=True)
+    cfg = {"workload": "ppr: R-MAT scale 20 (seed 3, edgefactor 16), k=256 teleport vectors uniform over seed sets "
+                       "of 1-64 vertices (numpy PCG64 seed 3), alpha 0.85; 'rule' = tol 1e-6 max_iter 100, 'fixed20' = "
+                       "20 sweeps", "n": g.n, "nnz": pg.nnz}
+    for label in out:  # per-sweep device time of the batched solve (k = 256: eight 32-column panels)
+        out[label]["batch_sweep_ms"] = out[label]["batch_device_ms"] / max(1, out[label]["iterations"])
+    pg.close()
+    return out, cfg
 
 
 def run_batch(args):
@@ -552,9 +575,16 @@ def run_serving(args):
     (n log-uniform in [1e3, 1e7], edgefactor uniform in [8, 32], seeds 2000-2063)."""
     import torch
 
+    torch.cuda.set_device(0)
+    out, cfg = measure_serving(args)
+    line = {"metric": METRIC, "value": out["solves_per_s"], "unit": "solves/s", "higher_is_better": True,
+            "n_gpus": 1, "data": "synthetic", "dtype": "f32", "config": cfg, "serving": out}
+    print(json.dumps(line), flush=True)
+
+
+def measure_serving(args):
     from eggpu_b200 import _native, serving, synth
 
-    torch.cuda.set_device(0)
     rng = np.random.Generator(np.random.PCG64(2000))
     count = 64
     max_n = int(args.serving_max_n)
@@ -586,6 +616,13 @@ def run_serving(args):
     wall = serving.replay(srv, reqs, times)
     srv.close()
     lat = serving.latency_summary(reqs)
+    # the same arrivals without continuous batching: PPR requests that arrive
+    # while a graph is being served wait for its running solve to end
+    again = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
+    srv1 = serving.Server(reg, workers=int(os.environ.get("EGPR_SERVING_WORKERS", "4")), sessions=False)
+    wall1 = serving.replay(srv1, again, times)
+    srv1.close()
+    lat_one_shot = serving.latency_summary(again)
     # capacity: the same requests all at once (queued requests fold into batched solves)
     burst = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
     srv2 = serving.Server(reg, workers=int(os.environ.get("EGPR_SERVING_WORKERS", "4")))
@@ -606,24 +643,24 @@ def run_serving(args):
         finally:
             reg.release(r.graph)
     plain = np.array(plain_lat)
-    line = {"metric": METRIC, "value": n_req / wall, "unit": "solves/s", "higher_is_better": True, "n_gpus": 1,
-            "data": "synthetic", "dtype": "f32",
-            "config": {"workload": "serving: Poisson arrivals at 1000 req/s, 50/50 PageRank/PPR (1-16 seeds), 64 "
-                                   f"R-MAT graphs n log-uniform in [1e3, {max_n:.0e}] (ids >= n dropped), edgefactor "
-                                   "uniform in [8, 32], seeds 2000-2063, alpha 0.85, tol 1e-6",
-                       "requests": n_req, "hbm_budget_gb": args.serving_hbm_gb,
-                       "graphs_loaded_before_traffic_s": warm_s,
-                       "total_nnz": int(sum(len(v[1]) for v in src.values()))},
-            "serving": {"latency": lat, "solves_per_s": n_req / wall, "offered_req_per_s": 1000.0,
-                        "server_stats": dict(srv.stats), "admissions": reg.admissions, "evictions": reg.evictions,
-                        "capacity_burst": {"solves_per_s": n_req / burst_wall, "wall_s": burst_wall,
-                                           "server_stats": dict(srv2.stats)},
-                        "plain_unbatched_service_ms": {"p50": float(np.percentile(plain, 50) * 1e3),
-                                                       "p99": float(np.percentile(plain, 99) * 1e3),
-                                                       "mean": float(plain.mean() * 1e3)},
-                        "plain_unbatched_capacity_solves_per_s": float(1.0 / plain.mean())}}
+    cfg = {"workload": "serving: Poisson arrivals at 1000 req/s, 50/50 PageRank/PPR (1-16 seeds), 64 "
+                       f"R-MAT graphs n log-uniform in [1e3, {max_n:.0e}] (ids >= n dropped), edgefactor "
+                       "uniform in [8, 32], seeds 2000-2063, alpha 0.85, tol 1e-6",
+           "requests": n_req, "hbm_budget_gb": args.serving_hbm_gb,
+           "graphs_loaded_before_traffic_s": warm_s,
+           "total_nnz": int(sum(len(v[1]) for v in src.values()))}
+    out = {"latency": lat, "solves_per_s": n_req / wall, "offered_req_per_s": 1000.0,
+           "server_stats": dict(srv.stats), "admissions": reg.admissions, "evictions": reg.evictions,
+           "without_continuous_batching": {"latency": lat_one_shot, "solves_per_s": n_req / wall1,
+                                           "server_stats": dict(srv1.stats)},
+           "capacity_burst": {"solves_per_s": n_req / burst_wall, "wall_s": burst_wall,
+                              "server_stats": dict(srv2.stats)},
+           "plain_unbatched_service_ms": {"p50": float(np.percentile(plain, 50) * 1e3),
+                                          "p99": float(np.percentile(plain, 99) * 1e3),
+                                          "mean": float(plain.mean() * 1e3)},
+           "plain_unbatched_capacity_solves_per_s": float(1.0 / plain.mean())}
     reg.close()
-    print(json.dumps(line), flush=True)
+    return out, cfg
 
 
 def run_precision25(args):
@@ -675,6 +712,11 @@ def main():
     ap.add_argument("--no-pageable", action="store_true", help="skip the end-to-end leg from pageable memory")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own cuSPARSE solve on the same graph")
+    ap.add_argument("--with-ppr", action=argparse.BooleanOptionalAction, default=True,
+                    help="plain-PageRank workloads: also measure the batched-PPR config (R-MAT 20, k=256) and "
+                         "report it inside the line")
+    ap.add_argument("--with-serving", action=argparse.BooleanOptionalAction, default=True,
+                    help="plain-PageRank workloads: also run the serving config and report it inside the line")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default sweep layout (a profiler then sees only the timed launches)")
     ap.add_argument("--serving-max-n", type=float, default=1e7)

@@ -122,6 +122,12 @@ _SIGNATURES = [
     ("egpr_pagerank_device_noalloc", c_int,
      [c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int32, c_double, c_uint32, c_void_p,
       c_void_p, POINTER(EgprStats)]),
+    ("egpr_session_create", c_int, [c_void_p, c_double, c_double, c_int32, POINTER(c_void_p)]),
+    ("egpr_session_admit", c_int, [c_void_p, c_int32, c_void_p, c_void_p, c_int32, c_void_p]),
+    ("egpr_session_step", c_int, [c_void_p, c_int32, c_void_p, POINTER(c_int32)]),
+    ("egpr_session_collect", c_int, [c_void_p, c_int32, c_void_p, c_uint32, c_void_p, c_void_p]),
+    ("egpr_session_info", c_int, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_int32)]),
+    ("egpr_session_destroy", c_int, [c_void_p]),
     ("egpr_cache_stats_get", c_int, [POINTER(EgprCacheStats)]),
     ("egpr_cache_reset", c_int, []),
     ("egpr_cache_set_budget", c_int, [c_int64]),
@@ -323,8 +329,88 @@ class PreparedGraph:
         return res, [s.as_dict() for s in sts]
 
     def close(self) -> None:
+        """Frees the device graph; refused (EgprError, the handle kept) while a
+        Session on it is alive."""
         if getattr(self, "_h", None) is not None:
-            lib.egpr_graph_destroy(self._h)
+            check(lib.egpr_graph_destroy(self._h), "egpr_graph_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Session:
+    """A running batched personalised-PageRank solve that requests join and
+    leave column by column (owns an ``egpr_session``; see include/egpr.h).
+
+    ``admit`` places seed-set requests in free slots, ``step`` runs a few
+    sweeps of every running column and returns the finished slots, ``collect``
+    hands back their ranks (FP64 correction sweep, normalisation) and frees
+    the slots.  The session keeps its PreparedGraph alive.
+    """
+
+    def __init__(self, graph: "PreparedGraph", alpha=0.85, tol=1e-6, slots=32):
+        h = c_void_p()
+        check(lib.egpr_session_create(graph.handle, float(alpha), float(tol), int(slots), ctypes.byref(h)),
+              "egpr_session_create")
+        self._h = h
+        self.graph = graph
+        self.alpha = float(alpha)
+        self.tol = float(tol)
+        self.n = graph.n
+        self.slots = self.info()["slots"]
+        self._done = np.zeros(self.slots, np.int32)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("Session is closed")
+        return self._h
+
+    def info(self) -> dict:
+        a, b, c = c_int32(), c_int32(), c_int32()
+        check(lib.egpr_session_info(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+              "egpr_session_info")
+        return {"slots": a.value, "running": b.value, "done": c.value, "free": a.value - b.value - c.value}
+
+    def admit(self, seed_sets, max_iter=100) -> list:
+        k = len(seed_sets)
+        if k == 0:
+            return []
+        ptr = np.zeros(k + 1, np.int32)
+        for j, s in enumerate(seed_sets):
+            ptr[j + 1] = ptr[j] + len(s)
+        seeds = _i32(np.concatenate([np.asarray(s, np.int32) for s in seed_sets]))
+        out = np.zeros(k, np.int32)
+        check(lib.egpr_session_admit(self.handle, k, _ptr(ptr), _ptr(seeds), int(max_iter), _ptr(out)),
+              "egpr_session_admit")
+        return [int(x) for x in out]
+
+    def step(self, sweeps=4) -> list:
+        nd = c_int32()
+        check(lib.egpr_session_step(self.handle, int(sweeps), _ptr(self._done), ctypes.byref(nd)),
+              "egpr_session_step")
+        return [int(x) for x in self._done[: nd.value]]
+
+    def collect(self, slots, correction=True, out=None):
+        k = len(slots)
+        if out is None:
+            out = np.empty((k, self.n), np.float64)
+        elif out.shape != (k, self.n) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape {(k, self.n)}")
+        sl = np.asarray(slots, np.int32)
+        sts = (EgprStats * max(k, 1))()
+        flags = 0 if correction else EGPR_FLAG_NO_CORRECTION
+        check(lib.egpr_session_collect(self.handle, k, _ptr(sl), flags, _ptr(out), ctypes.cast(sts, c_void_p)),
+              "egpr_session_collect")
+        return out, [sts[i].as_dict() for i in range(k)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            lib.egpr_session_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -772,11 +772,16 @@ int egpr_graph_create(const int32_t* V, const int32_t* E, const double* W, int32
     if (m > 0 && !E) return fail_arg("E is NULL");
     if (V[0] != 0 || (int64_t)V[n] != m) return fail_arg("CSR offsets must start at 0 and end at m");
     {
-        // branch-free over blocks of 4096 (the compiler vectorises it), checked per block
+        // branch-free over blocks of 4096 (the compiler vectorises them), the
+        // blocks spread over host threads for large graphs
         int bad = 0;
-        for (int32_t b = 0; b < n && !bad; b += 4096) {
-            const int32_t e = std::min(n, b + 4096);
-            for (int32_t i = b; i < e; ++i) bad |= V[i + 1] < V[i];
+        const int64_t blocks = ((int64_t)n + 4095) / 4096;
+#pragma omp parallel for schedule(static) reduction(| : bad) if (blocks >= 64)
+        for (int64_t k = 0; k < blocks; ++k) {
+            const int32_t b = (int32_t)(k * 4096), e = std::min(n, b + 4096);
+            int bb = 0;
+            for (int32_t i = b; i < e; ++i) bb |= V[i + 1] < V[i];
+            bad |= bb;
         }
         if (bad) return fail_arg("CSR offsets must be non-decreasing");
     }
@@ -836,6 +841,7 @@ int egpr_graph_destroy(egpr_graph* g) {
     if (!g) return EGPR_SUCC;
     {
         std::lock_guard<std::mutex> lk(g->mu);
+        if (g->sessions > 0) return fail_arg("the graph has live sessions (egpr_session_destroy them first)");
     }
     destroy_graph_object(g);
     return EGPR_SUCC;
@@ -897,6 +903,7 @@ int egpr_graph_set_tuning(egpr_graph* g, const egpr_tuning* in) {
     if ((rc = check_device(g))) return rc;
     const bool sweep = in->chunks_per_warp != g->tune_cpw || in->row_cost != g->tune_rc;
     const bool spmm = in->spmm_chunk != g->tune_spmm_chunk;
+    if (spmm && g->sessions > 0) return fail_arg("the batched solve's layout is in use by a session");
     g->tune_cpw = in->chunks_per_warp;
     g->tune_rc = in->row_cost;
     g->tune_spmm_chunk = in->spmm_chunk;
@@ -939,6 +946,8 @@ int egpr_graph_autotune(egpr_graph* g, uint32_t what, egpr_tuning* out) {
         if ((rc = rebuild_sweep(g))) return rc;
         res.sweep_ms = best;
     }
+    if (g->nnz > 0 && (what & EGPR_TUNE_SPMM) && g->sessions > 0)
+        return fail_arg("the batched solve's layout is in use by a session");
     if (g->nnz > 0 && (what & EGPR_TUNE_SPMM)) {
         double best = 1e30;
         int32_t bc = g->tune_spmm_chunk;

@@ -55,7 +55,6 @@ constexpr int kTileWords = 16;
 // from a hub store -(slot + 1) instead of the source id.  Slot nhub holds 0 and
 // is read by the placeholder entry of every row without entries.
 constexpr int kHubCap = 49152;      // largest hub cache (values) a sweep CTA stages
-constexpr int kHubDefault = 32768;  // hub cache of a prepared graph unless EGPR_HUBS says otherwise
 
 // Per-graph device view used by the sweep kernels.
 struct GraphDev {
@@ -277,6 +276,7 @@ struct egpr_graph {
     egpr::Plan plan;               // single-graph plan
     egpr::SpmmWork* spmm = nullptr; // batched personalised PageRank workspace
     egpr::BinLayout* bins = nullptr; // binned single-graph sweep (null: the tile sweep serves single solves)
+    int32_t sessions = 0;            // live batched-solve sessions (egpr_session_*) on this graph
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr; // active stream (own or user-given)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -6,8 +6,9 @@
 //
 //   k_out_weight_exact  FP64 out-weight sum per source after sanitising each
 //                    weight, bit-identical to the sequential sum in row order
-//                    (pagerank.cu:301-316): one warp per source where the sum
-//                    is provably order-free, one thread per source otherwise
+//                    (pagerank.cu:301-316): four lanes per source (a warp for
+//                    sources of more than 64 entries) where the sum is provably
+//                    order-free, one thread per source otherwise
 //   k_in_degree      in-degree histogram over valid endpoints (:315)
 //   exclusive scan   in_row (:319-320)
 //   radix sort       stable LSD sort of the entries by destination: entries of
@@ -247,45 +248,100 @@ __device__ __forceinline__ int lsb_exponent(double w) {
 // (weights of very different scales) is listed and summed sequentially by
 // k_out_weight_serial.  Weights drawn as FP32 values, as in the synthetic
 // workloads, always pass.
+// One source's sums over G lanes (lanes sub = 0..G-1 of a G-lane group).
+template <int G>
+__device__ __forceinline__ void out_weight_row(const int32_t* __restrict__ E, const double* __restrict__ W,
+                                               int32_t n, int32_t b, int32_t e, int sub, double& s, int32_t& c,
+                                               int& q) {
+    s = 0.0;
+    c = 0;
+    q = 4096;  // no nonzero weight yet
+    for (int32_t p = b + sub; p < e; p += G) {
+        const int32_t v = E[p];
+        if (v >= 0 && v < n) {
+            const double w = sanitize_w(W[p]);
+            s += w;
+            ++c;
+            if (w > 0.0) q = min(q, lsb_exponent(w));
+        }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+        q = min(q, __shfl_xor_sync(0xffffffffu, q, o));
+    }
+}
+
+// The sum s of a source's weights is its sequential sum when every partial sum
+// is provably exact (see above); otherwise the source is listed for the
+// sequential kernel.
+__device__ __forceinline__ void out_weight_store(int64_t u, double s, int32_t c, int q, double* __restrict__ outw,
+                                                 uint32_t* __restrict__ hub_key, uint32_t* __restrict__ hub_val,
+                                                 int32_t* __restrict__ serial_rows,
+                                                 uint32_t* __restrict__ serial_count) {
+    bool exact;
+    if (q == 4096) exact = true;             // only zero weights: the sum is 0
+    else if (q + 52 >= 1024) exact = false;  // 2^(q+52) would overflow: sum sequentially
+    else exact = s < ldexp(1.0, q + 52);
+    if (exact) outw[u] = s;
+    else serial_rows[atomicAdd(serial_count, 1u)] = (int32_t)u;
+    // hub ranking: descending out-degree, ascending id (stable sort of ~count)
+    hub_key[u] = ~(uint32_t)c;
+    hub_val[u] = (uint32_t)u;
+}
+
+constexpr int32_t kOutWeightShort = 64;  // sources with more entries are summed by a whole warp
+
+// Sources [r0, r1), four lanes each; a source with more than kOutWeightShort
+// entries is listed for k_out_weight_long instead.
 __global__ void k_out_weight_exact(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
                                    const double* __restrict__ W, int32_t n, int32_t r0, int32_t r1,
                                    double* __restrict__ outw, uint32_t* __restrict__ hub_key,
                                    uint32_t* __restrict__ hub_val, int32_t* __restrict__ serial_rows,
-                                   uint32_t* __restrict__ serial_count) {
+                                   uint32_t* __restrict__ serial_count, int32_t* __restrict__ long_rows,
+                                   uint32_t* __restrict__ long_count) {
+    constexpr int G = 4;
+    const int lane = threadIdx.x & 31, sub = lane & (G - 1), grp = lane / G;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t ub = r0 + warp * (32 / G); ub < r1; ub += nwarps * (32 / G)) {
+        const int64_t u = ub + grp;
+        int32_t b = 0, e = 0;
+        if (u < r1) {
+            b = V[u];
+            e = V[u + 1];
+            if (e - b > kOutWeightShort) {
+                if (sub == 0) long_rows[atomicAdd(long_count, 1u)] = (int32_t)u;
+                e = b;  // the group still takes part in the shuffles
+            }
+        }
+        double s;
+        int32_t c;
+        int q;
+        out_weight_row<G>(E, W, n, b, e, sub, s, c, q);
+        if (u < r1 && sub == 0 && V[u + 1] - V[u] <= kOutWeightShort)
+            out_weight_store(u, s, c, q, outw, hub_key, hub_val, serial_rows, serial_count);
+    }
+}
+
+// The long sources listed by k_out_weight_exact, one warp each.
+__global__ void k_out_weight_long(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
+                                  const double* __restrict__ W, int32_t n, const int32_t* __restrict__ long_rows,
+                                  const uint32_t* __restrict__ long_count, double* __restrict__ outw,
+                                  uint32_t* __restrict__ hub_key, uint32_t* __restrict__ hub_val,
+                                  int32_t* __restrict__ serial_rows, uint32_t* __restrict__ serial_count) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t u = r0 + warp; u < r1; u += nwarps) {
-        const int32_t b = V[u], e = V[u + 1];
-        double s = 0.0;
-        int32_t c = 0;
-        int q = 4096;  // no nonzero weight yet
-        for (int32_t p = b + lane; p < e; p += 32) {
-            const int32_t v = E[p];
-            if (v >= 0 && v < n) {
-                const double w = sanitize_w(W[p]);
-                s += w;
-                ++c;
-                if (w > 0.0) q = min(q, lsb_exponent(w));
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            s += __shfl_xor_sync(0xffffffffu, s, o);
-            c += __shfl_xor_sync(0xffffffffu, c, o);
-            q = min(q, __shfl_xor_sync(0xffffffffu, q, o));
-        }
-        if (lane == 0) {
-            bool exact;
-            if (q == 4096) exact = true;             // only zero weights: the sum is 0
-            else if (q + 52 >= 1024) exact = false;  // 2^(q+52) would overflow: sum sequentially
-            else exact = s < ldexp(1.0, q + 52);
-            if (exact) outw[u] = s;
-            else serial_rows[atomicAdd(serial_count, 1u)] = (int32_t)u;
-            // hub ranking: descending out-degree, ascending id (stable sort of ~count)
-            hub_key[u] = ~(uint32_t)c;
-            hub_val[u] = (uint32_t)u;
-        }
+    const uint32_t k = *long_count;
+    for (int64_t i = warp; i < (int64_t)k; i += nwarps) {
+        const int32_t u = long_rows[i];
+        double s;
+        int32_t c;
+        int q;
+        out_weight_row<32>(E, W, n, V[u], V[u + 1], lane, s, c, q);
+        if (lane == 0) out_weight_store(u, s, c, q, outw, hub_key, hub_val, serial_rows, serial_count);
     }
 }
 
@@ -1185,6 +1241,8 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         // weighted: rows whose out-weight is summed sequentially (k_out_weight_exact)
         int32_t* serial_rows = W ? tmp.get<int32_t>((size_t)n, &rc) : nullptr;
         uint32_t* serial_count = W ? tmp.get<uint32_t>(1, &rc) : nullptr;
+        int32_t* long_rows = W ? tmp.get<int32_t>((size_t)n, &rc) : nullptr;  // per piece: sources of many entries
+        uint32_t* long_count = W ? tmp.get<uint32_t>(1, &rc) : nullptr;
         if (rc) return rc;
         if (W) cudaMemsetAsync(serial_count, 0, sizeof(uint32_t), s);
         // in_row, hub_slot: bulk copies of a stage's rows may read up to 3 elements past the end.
@@ -1236,11 +1294,15 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                 int32_t r_end = n;
                 if (i + 1 < pieces) r_end = (int32_t)(std::upper_bound(V, V + n + 1, (int32_t)b) - V) - 1;
                 if (r_end > r_done) {
-                    if (dW)
-                        k_out_weight_exact<<<grid_for((int64_t)(r_end - r_done) * 32), kThreads, 0, s>>>(
+                    if (dW) {
+                        cudaMemsetAsync(long_count, 0, sizeof(uint32_t), s);
+                        k_out_weight_exact<<<grid_for((int64_t)(r_end - r_done) * 8), kThreads, 0, s>>>(
                             dV, dE, dW, n, r_done, r_end, g->outw.as<double>(), hkey, hval, serial_rows,
-                            serial_count);
-                    else
+                            serial_count, long_rows, long_count);
+                        k_out_weight_long<<<148 * 8, kThreads, 0, s>>>(dV, dE, dW, n, long_rows, long_count,
+                                                                       g->outw.as<double>(), hkey, hval,
+                                                                       serial_rows, serial_count);
+                    } else
                         k_out_degree<<<grid_for((int64_t)(r_end - r_done) * 32), kThreads, 0, s>>>(
                             dV, dE, n, r_done, r_end, g->outw.as<double>(), hkey, hval);
                     r_done = r_end;
@@ -1297,9 +1359,15 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         // Hubs: the min(n, kHubCap) sources of largest out-degree (a multiple of 4,
         // the granule of the shared-memory staging copy).
         // EGPR_HUBS=N: hub cache size (0: none); at most kHubCap - 32, which leaves
-        // room for the zero slot nhub in a kHubCap-value copy
+        // room for the zero slot nhub in a kHubCap-value copy.  By default 24,544
+        // hubs, and 16,352 from 2^24 vertices: the shared memory the hubs take is
+        // L1 the sweep's other loads lose, and measured on B200 the smaller cache
+        // wins once the rank vector no longer fits L2 (R-MAT scale 25 weighted:
+        // 2.32 ms per sweep with 16K hubs, 2.37 with 24K, 2.56 with 32K; scale 22:
+        // 0.232, 0.228, 0.227 ms)
         const char* hub_env = std::getenv("EGPR_HUBS");
-        const int32_t hub_want = hub_env ? std::max(0, std::atoi(hub_env)) : kHubDefault - 32;
+        const int32_t hub_default = n >= (1 << 24) ? 16384 - 32 : 24576 - 32;
+        const int32_t hub_want = hub_env ? std::max(0, std::atoi(hub_env)) : hub_default;
         g->nhub = std::min<int32_t>(std::min<int32_t>(n, hub_want), kHubCap - 32) & ~3;
         if ((rc = g->hub_slot.alloc(((size_t)n + 8) * sizeof(int32_t))) ||
             (rc = g->hub_ids.alloc((size_t)std::max(g->nhub + 1, 4) * sizeof(int32_t))) ||

@@ -43,6 +43,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "egpr_internal.cuh"
@@ -78,10 +79,12 @@ struct ColState {
     double residual64;
     double xsum;
     double dsum;
-    int32_t iter;
+    int32_t iter;      // sweeps of the column's panel when the column last advanced (parity of its iterate)
     int32_t done;
     int32_t converged;
-    int32_t active;  // column < k
+    int32_t active;    // column < k (a session: the slot holds a request)
+    int32_t base;      // panel sweeps before the column joined (its own sweeps are iter - base)
+    int32_t max_iter;  // the column's sweep limit
 };
 
 struct SpmmParams {
@@ -107,6 +110,7 @@ struct SpmmParams {
     uint32_t* span_cnt;       // [panel][chunk] arrivals per span (reset by the last)
     unsigned long long* gacc; // [panel][kAccQ][32] fixed-point column sums
     Ctl* ctl;
+    int32_t step_cap;         // session steps: stop after this many sweeps without an error (0: none)
 };
 
 template <bool kF64>
@@ -647,7 +651,7 @@ k_spmm(const SpmmParams* __restrict__ Pd, cudaGraphConditionalHandle cond, int32
                 const int32_t it = cs->iter + 1;
                 cs->iter = it;
                 const bool conv = e < P.tol_n;
-                if (conv || it >= P.max_iter) {
+                if (conv || it - cs->base >= cs->max_iter) {
                     cs->done = 1;
                     cs->converged = conv ? 1 : 0;
                     atomicSub(&P.ctl->active, 1);
@@ -667,7 +671,7 @@ k_spmm(const SpmmParams* __restrict__ Pd, cudaGraphConditionalHandle cond, int32
             const int32_t launches = P.ctl->launches + 1;
             P.ctl->launches = launches;
             const int32_t active = __ldcg(&P.ctl->active);
-            const bool more = active > 0 && launches < P.ctl->cap;
+            const bool more = active > 0 && launches < P.ctl->cap && (P.step_cap == 0 || launches < P.step_cap);
             if (active > 0 && launches >= P.ctl->cap) P.ctl->error = EGPR_TIMEOUT;
             if (use_cond) cudaGraphSetConditional(cond, more ? 1u : 0u);
         }
@@ -760,10 +764,17 @@ __global__ void k_sp_tele_rows(const int32_t* __restrict__ tv, int32_t nt, uint3
     if (t < nt) meta[tv[t]] |= (uint32_t)(t + 1);
 }
 
+// Teleport rows row0 .. row0 + nt - 1 of a session, for vertices tv[0 .. nt).
+__global__ void k_sp_tele_rows_at(const int32_t* __restrict__ tv, int32_t nt, int32_t row0,
+                                  uint32_t* __restrict__ meta) {
+    const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nt) meta[tv[t]] |= (uint32_t)(row0 + t + 1);
+}
+
 // X0 = 1/n on live columns, 0 on padding columns and on row n of both
 // iterates (grid.y = panel, 16-byte stores); column states.
 __global__ void k_sp_init(float* X0, float* X1, ColState* cols, int32_t n, int32_t npanels, int32_t k, double alpha,
-                          int32_t ndang) {
+                          int32_t ndang, int32_t max_iter) {
     const float x0 = (float)(1.0 / (double)n);
     const int32_t p = blockIdx.y;
     const int64_t quads = ((int64_t)n + 1) * (kLanes / 4);
@@ -791,8 +802,24 @@ __global__ void k_sp_init(float* X0, float* X1, ColState* cols, int32_t n, int32
         cs.active = j < k ? 1 : 0;
         cs.done = j < k ? 0 : 1;
         cs.converged = 0;
+        cs.base = 0;
+        cs.max_iter = max_iter;
         cols[j] = cs;
     }
+}
+
+// A session's newly admitted columns start at x0 = 1/n in the iterate their
+// panel reads next (X[panel sweeps & 1]); row n stays zero.  cols_new[i] is
+// a column index p * 32 + lane, par_new[i] its buffer.
+__global__ void k_sp_init_cols(float* X0, float* X1, int32_t n, const int32_t* __restrict__ cols_new,
+                               const int32_t* __restrict__ par_new, int32_t count) {
+    const float x0 = (float)(1.0 / (double)n);
+    const int32_t i = blockIdx.y;
+    if (i >= count) return;
+    const int32_t j = cols_new[i], p = j / kLanes, c = j - p * kLanes;
+    float* x = (par_new[i] ? X1 : X0) + (size_t)p * ((size_t)n + 1) * kLanes + c;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        x[(size_t)v * kLanes] = x0;
 }
 
 // Rank sum of each column's final FP32 iterate (runs when the FP64 correction
@@ -827,7 +854,8 @@ __global__ void k_sp_colsum_set(ColState* __restrict__ cols, const unsigned long
 constexpr int kNormRows = 128;
 __global__ void __launch_bounds__(256) k_sp_normalize(const double* __restrict__ out64, const float* X0, const float* X1,
                                                       const ColState* __restrict__ cols, int32_t n, int32_t k,
-                                                      int32_t from_fp32, double* __restrict__ out) {
+                                                      int32_t from_fp32, double* __restrict__ out,
+                                                      const int32_t* __restrict__ out_row) {
     __shared__ double tile[kNormRows][kLanes + 1];
     const int32_t p = blockIdx.y;
     const int32_t v0 = blockIdx.x * kNormRows;
@@ -852,7 +880,9 @@ __global__ void __launch_bounds__(256) k_sp_normalize(const double* __restrict__
     for (int idx = threadIdx.x; idx < kLanes * kNormRows; idx += blockDim.x) {
         const int jj = idx / kNormRows, i = idx - jj * kNormRows;
         const int32_t j = p * kLanes + jj, v = v0 + i;
-        if (j < k && v < n) out[(size_t)j * n + v] = tile[i][jj];
+        if (j >= k || v >= n) continue;
+        const int32_t r = out_row ? out_row[j] : j;  // a session writes only the columns it collects
+        if (r >= 0) out[(size_t)r * n + v] = tile[i][jj];
     }
 }
 
@@ -1109,7 +1139,7 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     if (nt > 0) k_sp_tele_rows<<<(nt + 255) / 256, 256, 0, s>>>(w.tele_v.as<int32_t>(), nt, w.meta.as<uint32_t>());
     k_sp_init<<<dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 1) * 8 / 256 + 1, 148 * 8)),
                      (unsigned)npanels), 256, 0, s>>>(
-        w.X0.as<float>(), w.X1.as<float>(), w.cols.as<ColState>(), n, npanels, kg, alpha, g->n_dangling_solve);
+        w.X0.as<float>(), w.X1.as<float>(), w.cols.as<ColState>(), n, npanels, kg, alpha, g->n_dangling_solve, max_iter);
     int32_t launches = nt > 0 ? 3 : 2;
     if (graph_loop_enabled()) build_loop_graph(w, grid);
     if (w.cg_exec && graph_loop_enabled()) {
@@ -1137,7 +1167,8 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     {
         dim3 gr((unsigned)((n + kNormRows - 1) / kNormRows), (unsigned)npanels);
         k_sp_normalize<<<gr, 256, 0, s>>>(w.out64.as<double>(), w.X0.as<float>(), w.X1.as<float>(),
-                                          w.cols.as<ColState>(), n, kg, correction ? 0 : 1, w.out.as<double>());
+                                          w.cols.as<ColState>(), n, kg, correction ? 0 : 1, w.out.as<double>(),
+                                          nullptr);
         launches += 1;
     }
     if ((rc = cuda_ok(cudaGetLastError(), "spmm finish"))) return rc;
@@ -1243,4 +1274,455 @@ int ppr_batch_solve(egpr_graph* g, double alpha, int32_t max_iter, double tol, i
     return EGPR_SUCC;
 }
 
+
+// ---- continuous batching: a session of column slots ------------------------
+// No counterpart in the reference.  A session keeps one batched solve of a
+// graph running: requests join it in free column slots between steps of a
+// few sweeps, each column keeps its own stop rule and sweep count, and a
+// finished column is collected (FP64 correction sweep, normalisation, D2H)
+// and its slot freed while the others keep sweeping.  Live columns of a
+// 32-column panel share the parity of their iterate buffers, so a column that
+// joins a panel starts at the panel's sweep count and counts its own sweeps
+// from there (ColState::base).
+namespace {
+constexpr uint8_t kSlotFree = 0, kSlotRunning = 1, kSlotDone = 2;
+
+struct SessionState {
+    egpr_graph* g = nullptr;
+    SpmmWork w;                       // solve buffers; the entry stream is the graph's (g->spmm)
+    double alpha = 0.85, tol = 0.0;
+    int32_t slots = 0, npanels = 0;
+    std::vector<ColState> cols;       // host mirror of the column states
+    std::vector<int32_t> panel_sweeps;
+    std::vector<uint8_t> state;
+    std::vector<std::vector<int32_t>> rows_of;  // per slot: its teleport rows
+    std::vector<double> started, device_s;      // per slot: admission time, device time while live
+    std::unordered_map<int32_t, int32_t> row_of_vertex;
+    std::vector<int32_t> row_vertex;  // teleport row -> vertex
+    std::vector<float> tt;            // teleport rows x (npanels * 32)
+    int32_t rows_on_device = 0;       // rows whose meta bits are set
+    bool tele_dirty = false;
+    DevBuf out_row;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~SessionState() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        out_row.release();
+    }
+};
+
+int session_params(SessionState& S, int32_t step_cap, cudaStream_t s) {
+    egpr_graph* g = S.g;
+    SpmmWork& base = *g->spmm;
+    SpmmWork& w = S.w;
+    SpmmParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.chunks = base.chunks.as<SpChunk>();
+    P.nchunks = base.nchunks;
+    P.npanels = S.npanels;
+    P.n = g->n;
+    P.tele_ld = S.npanels * kLanes;
+    P.max_iter = 1 << 30;
+    P.src = base.src.as<int32_t>();
+    P.coef32 = base.c32.as<float>();
+    P.coef64 = base.c64.as<double>();
+    P.meta = w.meta.as<uint32_t>();
+    P.tele = w.tele.as<float>();
+    P.X[0] = w.X0.as<float>();
+    P.X[1] = w.X1.as<float>();
+    P.out64 = w.out64.as<double>();
+    P.cols = w.cols.as<ColState>();
+    P.alpha = S.alpha;
+    P.alpha_hi = (float)S.alpha;
+    P.alpha_lo = (float)(S.alpha - (double)P.alpha_hi);
+    P.oma_hi = (float)(1.0 - S.alpha);
+    P.oma_lo = (float)((1.0 - S.alpha) - (double)P.oma_hi);
+    P.tol_n = S.tol * (double)g->n;
+    P.parts = w.parts.p;
+    P.span_cnt = w.span_cnt.as<uint32_t>();
+    P.gacc = w.gacc.as<unsigned long long>();
+    P.ctl = w.ctl.as<Ctl>();
+    P.step_cap = step_cap;
+    return cuda_ok(cudaMemcpyAsync(w.params.p, &P, sizeof(P), cudaMemcpyHostToDevice, s), "H2D params");
+}
+
+int session_upload(SessionState& S, int32_t active, cudaStream_t s) {
+    SpmmWork& w = S.w;
+    int rc;
+    if (S.tele_dirty) {
+        const size_t bytes = std::max<size_t>(S.tt.size(), 1) * sizeof(float);
+        if ((rc = w.tele.grow_on(bytes, s))) return rc;
+        if (!S.tt.empty() &&
+            (rc = cuda_ok(cudaMemcpyAsync(w.tele.p, S.tt.data(), S.tt.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+                          "H2D teleport")))
+            return rc;
+        const int32_t nrows = (int32_t)S.row_vertex.size();
+        if (nrows > S.rows_on_device) {
+            const int32_t nt = nrows - S.rows_on_device;
+            if ((rc = w.tele_v.grow_on((size_t)nt * sizeof(int32_t), s)) ||
+                (rc = cuda_ok(cudaMemcpyAsync(w.tele_v.p, S.row_vertex.data() + S.rows_on_device,
+                                              (size_t)nt * sizeof(int32_t), cudaMemcpyHostToDevice, s), "H2D rows")))
+                return rc;
+            k_sp_tele_rows_at<<<(nt + 255) / 256, 256, 0, s>>>(w.tele_v.as<int32_t>(), nt, S.rows_on_device,
+                                                               w.meta.as<uint32_t>());
+            S.rows_on_device = nrows;
+        }
+        S.tele_dirty = false;
+    }
+    Ctl c{};
+    c.active = active;
+    c.cap = 1 << 30;
+    if ((rc = cuda_ok(cudaMemcpyAsync(w.cols.p, S.cols.data(), S.cols.size() * sizeof(ColState), cudaMemcpyHostToDevice,
+                                      s), "H2D cols")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(w.ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D ctl")))
+        return rc;
+    return EGPR_SUCC;
+}
+
+int session_create(egpr_graph* g, double alpha, double tol, int32_t slots, SessionState** out) {
+    *out = nullptr;
+    int rc;
+    if ((rc = check_device(g))) return rc;
+    if (g->nnz <= 0) return arg_error("a session needs a graph with inbound entries");
+    if (!(alpha >= 0.0 && alpha < 1.0)) return arg_error("alpha must be in [0, 1)");
+    if (slots < 1 || slots > kMaxPanels * kLanes) return arg_error("slots must be in [1, 512]");
+    cudaStream_t s = g->stream;
+    if (!g->spmm) g->spmm = new SpmmWork();
+    if (!g->spmm->C && (rc = build_spmm_layout(g, *g->spmm, s))) return rc;
+    SessionState* S = new SessionState();
+    S->g = g;
+    S->alpha = alpha;
+    S->tol = tol > 0.0 ? tol : 0.0;
+    S->npanels = (slots + kLanes - 1) / kLanes;
+    S->slots = S->npanels * kLanes;
+    S->w.C = g->spmm->C;
+    S->w.nchunks = g->spmm->nchunks;
+    S->w.epad = g->spmm->epad;
+    if ((rc = ensure_capacity(g, S->w, S->npanels, s)) ||
+        (rc = cuda_ok(cudaMemsetAsync(S->w.X0.p, 0, S->w.X0.bytes, s), "memset")) ||
+        (rc = S->out_row.alloc((size_t)S->slots * sizeof(int32_t))) ||
+        (rc = cuda_ok(cudaEventCreate(&S->e0), "event")) || (rc = cuda_ok(cudaEventCreate(&S->e1), "event"))) {
+        delete S;
+        return rc;
+    }
+    k_sp_meta<<<grid_1d(g->n), 256, 0, s>>>(g->outw.as<double>(), g->n, S->w.meta.as<uint32_t>());
+    ColState free_col;
+    std::memset(&free_col, 0, sizeof(free_col));
+    free_col.done = 1;
+    S->cols.assign((size_t)S->slots, free_col);
+    S->panel_sweeps.assign((size_t)S->npanels, 0);
+    S->state.assign((size_t)S->slots, kSlotFree);
+    S->rows_of.assign((size_t)S->slots, {});
+    S->started.assign((size_t)S->slots, 0.0);
+    S->device_s.assign((size_t)S->slots, 0.0);
+    if ((rc = cuda_ok(cudaStreamSynchronize(s), "session"))) {
+        delete S;
+        return rc;
+    }
+    *out = S;
+    return EGPR_SUCC;
+}
+
+int session_admit(SessionState& S, int32_t count, const int32_t* seed_ptr, const int32_t* seeds, int32_t max_iter,
+                  int32_t* slots_out) {
+    egpr_graph* g = S.g;
+    const int32_t n = g->n;
+    if (max_iter < 1) max_iter = 1;
+    std::vector<int32_t> free_slots;
+    for (int32_t j = 0; j < S.slots && (int32_t)free_slots.size() < count; ++j)
+        if (S.state[(size_t)j] == kSlotFree) free_slots.push_back(j);
+    if ((int32_t)free_slots.size() < count) return arg_error("not enough free slots in the session");
+    std::vector<std::vector<int32_t>> sets((size_t)count);
+    for (int32_t i = 0; i < count; ++i) {
+        const int32_t b = seed_ptr[i], e = seed_ptr[i + 1];
+        if (e <= b || b < 0) return arg_error("every request needs at least one seed");
+        std::vector<int32_t> sv(seeds + b, seeds + e);
+        std::sort(sv.begin(), sv.end());
+        sv.erase(std::unique(sv.begin(), sv.end()), sv.end());
+        if (sv.front() < 0 || sv.back() >= n) return arg_error("seed ids must lie in [0, n)");
+        sets[(size_t)i] = std::move(sv);
+    }
+    const int32_t ld = S.npanels * kLanes;
+    std::vector<int32_t> cols_new, par_new;
+    const double x0 = (double)(float)(1.0 / (double)n);
+    const double t0 = wall_seconds();
+    for (int32_t i = 0; i < count; ++i) {
+        const int32_t j = free_slots[(size_t)i], p = j / kLanes;
+        const float val = (float)(1.0 / (double)sets[(size_t)i].size());
+        for (int32_t v : sets[(size_t)i]) {
+            auto it = S.row_of_vertex.find(v);
+            int32_t r;
+            if (it == S.row_of_vertex.end()) {
+                r = (int32_t)S.row_vertex.size();
+                S.row_of_vertex.emplace(v, r);
+                S.row_vertex.push_back(v);
+                S.tt.resize((size_t)(r + 1) * ld, 0.f);
+            } else {
+                r = it->second;
+            }
+            S.tt[(size_t)r * ld + j] = val;
+            S.rows_of[(size_t)j].push_back(r);
+        }
+        // the panel's sweep count: that of its live columns, if any
+        ColState& cs = S.cols[(size_t)j];
+        std::memset(&cs, 0, sizeof(cs));
+        const int32_t base = S.panel_sweeps[(size_t)p];
+        cs.dsum = (double)g->n_dangling_solve * x0;
+        cs.dmass = S.alpha * cs.dsum / (double)n;
+        cs.dmass_prev = cs.dmass;
+        cs.iter = base;
+        cs.base = base;
+        cs.max_iter = max_iter;
+        cs.active = 1;
+        cs.done = 0;
+        S.state[(size_t)j] = kSlotRunning;
+        S.started[(size_t)j] = t0;
+        S.device_s[(size_t)j] = 0.0;
+        cols_new.push_back(j);
+        par_new.push_back(base & 1);
+        slots_out[i] = j;
+    }
+    S.tele_dirty = true;
+    // the new columns' start vectors (stream order: before the next step)
+    cudaStream_t s = g->stream;
+    int rc;
+    const size_t cn = cols_new.size();
+    if ((rc = S.w.colsum.grow_on(2 * cn * sizeof(int32_t), s)) ||
+        (rc = cuda_ok(cudaMemcpyAsync(S.w.colsum.p, cols_new.data(), cn * sizeof(int32_t), cudaMemcpyHostToDevice, s),
+                      "H2D columns")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(S.w.colsum.as<int32_t>() + cn, par_new.data(), cn * sizeof(int32_t),
+                                      cudaMemcpyHostToDevice, s), "H2D columns")))
+        return rc;
+    k_sp_init_cols<<<dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 255) / 256, 148 * 4)),
+                          (unsigned)cn), 256, 0, s>>>(S.w.X0.as<float>(), S.w.X1.as<float>(), n,
+                                                      S.w.colsum.as<int32_t>(), S.w.colsum.as<int32_t>() + cn,
+                                                      (int32_t)cn);
+    if ((rc = cuda_ok(cudaGetLastError(), "session admit"))) return rc;
+    // the colsum buffer is reused by the next call: the copies must be done
+    return cuda_ok(cudaStreamSynchronize(s), "session admit");
+}
+
+int session_step(SessionState& S, int32_t sweeps, int32_t* done_slots, int32_t* ndone) {
+    egpr_graph* g = S.g;
+    cudaStream_t s = g->stream;
+    *ndone = 0;
+    int32_t live = 0;
+    for (int32_t j = 0; j < S.slots; ++j) live += S.state[(size_t)j] == kSlotRunning ? 1 : 0;
+    int rc;
+    if (live > 0 && sweeps > 0) {
+        if ((rc = session_upload(S, live, s)) || (rc = session_params(S, sweeps, s))) return rc;
+        const int64_t work = 4 * (int64_t)S.npanels * S.w.epad;
+        const int grid = work_grid(work, spmm_grid(false));
+        if ((rc = cuda_ok(cudaEventRecord(S.e0, s), "event"))) return rc;
+        const SpmmParams* Pd = S.w.params.as<SpmmParams>();
+        if (graph_loop_enabled()) build_loop_graph(S.w, grid);
+        if (S.w.cg_exec && graph_loop_enabled()) {
+            if ((rc = cuda_ok(cudaGraphLaunch(S.w.cg_exec, s), "graph launch"))) return rc;
+        } else {
+            for (int32_t it = 0; it < sweeps; ++it)
+                k_spmm<false><<<grid, sp_threads<false>(), smem_bytes(false), s>>>(Pd, 0, 0);
+            if ((rc = cuda_ok(cudaGetLastError(), "spmm launch"))) return rc;
+        }
+        if ((rc = cuda_ok(cudaEventRecord(S.e1, s), "event"))) return rc;
+        Ctl ctl;
+        if ((rc = cuda_ok(cudaMemcpyAsync(S.cols.data(), S.w.cols.p, S.cols.size() * sizeof(ColState),
+                                          cudaMemcpyDeviceToHost, s), "D2H cols")) ||
+            (rc = cuda_ok(cudaMemcpyAsync(&ctl, S.w.ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s), "D2H ctl")) ||
+            (rc = cuda_ok(cudaStreamSynchronize(s), "session step")))
+            return rc;
+        if (ctl.error) return ctl.error;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, S.e0, S.e1);
+        for (int32_t j = 0; j < S.slots; ++j)
+            if (S.state[(size_t)j] == kSlotRunning) {
+                S.device_s[(size_t)j] += ms * 1e-3;
+                if (S.cols[(size_t)j].done) S.state[(size_t)j] = kSlotDone;
+            }
+        // A panel's sweep count (the parity of its iterate buffers) is that of
+        // its columns still running: one that stopped inside the step holds
+        // an older count, and a column admitted next would start in the wrong
+        // buffer.  A panel with no running column keeps its count.
+        for (int32_t j = 0; j < S.slots; ++j)
+            if (S.state[(size_t)j] == kSlotRunning) S.panel_sweeps[(size_t)(j / kLanes)] = S.cols[(size_t)j].iter;
+    }
+    for (int32_t j = 0; j < S.slots; ++j)
+        if (S.state[(size_t)j] == kSlotDone) done_slots[(*ndone)++] = j;
+    return EGPR_SUCC;
+}
+
+int session_collect(SessionState& S, int32_t count, const int32_t* slots, uint32_t flags, double* out,
+                    egpr_stats* stats) {
+    egpr_graph* g = S.g;
+    const int32_t n = g->n;
+    cudaStream_t s = g->stream;
+    for (int32_t i = 0; i < count; ++i)
+        if (slots[i] < 0 || slots[i] >= S.slots || S.state[(size_t)slots[i]] != kSlotDone)
+            return arg_error("only finished slots can be collected");
+    // the FP64 correction and the normalisation see only the collected columns
+    std::vector<ColState> view = S.cols;
+    std::vector<int32_t> out_row((size_t)S.slots, -1);
+    for (ColState& c : view) c.active = 0;
+    for (int32_t i = 0; i < count; ++i) {
+        view[(size_t)slots[i]].active = 1;
+        out_row[(size_t)slots[i]] = i;
+    }
+    int rc;
+    const bool correction = (flags & EGPR_FLAG_NO_CORRECTION) == 0;
+    if ((rc = S.w.out.grow_on((size_t)count * n * sizeof(double), s)) ||
+        (rc = cuda_ok(cudaMemcpyAsync(S.w.cols.p, view.data(), view.size() * sizeof(ColState), cudaMemcpyHostToDevice, s),
+                      "H2D cols")) ||
+        (rc = cuda_ok(cudaMemcpyAsync(S.out_row.p, out_row.data(), out_row.size() * sizeof(int32_t),
+                                      cudaMemcpyHostToDevice, s), "H2D rows")) ||
+        (rc = session_params(S, 0, s)))
+        return rc;
+    if ((rc = cuda_ok(cudaEventRecord(S.e0, s), "event"))) return rc;
+    const int64_t work = 4 * (int64_t)S.npanels * S.w.epad;
+    const SpmmParams* Pd = S.w.params.as<SpmmParams>();
+    if (correction) {
+        k_spmm<true><<<work_grid(work, spmm_grid(true)), sp_threads<true>(), smem_bytes(true), s>>>(Pd, 0, 0);
+    } else {
+        if ((rc = cuda_ok(cudaMemsetAsync(S.w.colsum.p, 0, (size_t)S.npanels * 2 * kLanes * sizeof(unsigned long long),
+                                          s), "memset")))
+            return rc;
+        k_sp_colsum<<<dim3(148, (unsigned)S.npanels), 256, 0, s>>>(S.w.X0.as<float>(), S.w.X1.as<float>(),
+                                                                   S.w.cols.as<ColState>(), n,
+                                                                   S.w.colsum.as<unsigned long long>());
+        k_sp_colsum_set<<<(S.npanels * kLanes + 255) / 256, 256, 0, s>>>(S.w.cols.as<ColState>(),
+                                                                         S.w.colsum.as<unsigned long long>(),
+                                                                         S.npanels);
+    }
+    dim3 gr((unsigned)((n + kNormRows - 1) / kNormRows), (unsigned)S.npanels);
+    k_sp_normalize<<<gr, 256, 0, s>>>(S.w.out64.as<double>(), S.w.X0.as<float>(), S.w.X1.as<float>(),
+                                      S.w.cols.as<ColState>(), n, S.slots, correction ? 0 : 1, S.w.out.as<double>(),
+                                      S.out_row.as<int32_t>());
+    if ((rc = cuda_ok(cudaGetLastError(), "session collect"))) return rc;
+    if ((rc = cuda_ok(cudaEventRecord(S.e1, s), "event"))) return rc;
+    if (out && (rc = cuda_ok(cudaMemcpyAsync(out, S.w.out.p, (size_t)count * n * sizeof(double), cudaMemcpyDeviceToHost,
+                                             s), "D2H ranks")))
+        return rc;
+    if ((rc = cuda_ok(cudaStreamSynchronize(s), "session collect"))) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, S.e0, S.e1);
+    const int32_t ld = S.npanels * kLanes;
+    const double now = wall_seconds();
+    for (int32_t i = 0; i < count; ++i) {
+        const int32_t j = slots[i];
+        const ColState& c = S.cols[(size_t)j];
+        if (stats) {
+            egpr_stats& st = stats[i];
+            std::memset(&st, 0, sizeof(st));
+            st.iterations = c.iter - c.base;
+            st.converged = c.converged;
+            st.residual = c.residual;
+            st.kernel_seconds = S.device_s[(size_t)j] + ms * 1e-3;
+            st.total_seconds = now - S.started[(size_t)j];
+            st.bytes_per_iter = (int64_t)S.npanels * (S.w.epad * 8 + 2 * ((int64_t)n + 1) * kLanes * 4 + 4 * (int64_t)n);
+        }
+        // free the slot: its teleport entries go, its state is a free column again
+        for (int32_t r : S.rows_of[(size_t)j]) S.tt[(size_t)r * ld + j] = 0.f;
+        S.rows_of[(size_t)j].clear();
+        std::memset(&S.cols[(size_t)j], 0, sizeof(ColState));
+        S.cols[(size_t)j].done = 1;
+        S.state[(size_t)j] = kSlotFree;
+    }
+    S.tele_dirty = true;
+    return EGPR_SUCC;
+}
+
+}  // namespace
+
 }  // namespace egpr
+
+
+// ---- C ABI of the sessions ---------------------------------------------------
+extern "C" {
+
+struct egpr_session {
+    egpr::SessionState* st;
+};
+
+int egpr_session_create(egpr_graph* g, double alpha, double tol, int32_t slots, egpr_session** out) {
+    using namespace egpr;
+    if (!g || !out) return arg_error("NULL argument");
+    *out = nullptr;
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->pending) return arg_error("a solve is pending on this graph");
+    SessionState* S = nullptr;
+    int rc = session_create(g, alpha, tol, slots, &S);
+    if (rc) return rc;
+    egpr_session* h = new (std::nothrow) egpr_session{S};
+    if (!h) {
+        delete S;
+        return EGPR_FAILED_TO_ALLOCATE_HOST_MEM;
+    }
+    g->sessions += 1;
+    *out = h;
+    return EGPR_SUCC;
+}
+
+int egpr_session_admit(egpr_session* h, int32_t count, const int32_t* seed_ptr, const int32_t* seeds,
+                       int32_t max_iter, int32_t* slots_out) {
+    using namespace egpr;
+    if (!h || !h->st) return arg_error("NULL session");
+    if (count < 0 || (count > 0 && (!seed_ptr || !seeds || !slots_out))) return arg_error("NULL argument");
+    if (count == 0) return EGPR_SUCC;
+    SessionState& S = *h->st;
+    std::lock_guard<std::mutex> lk(S.g->mu);
+    int rc;
+    if ((rc = check_device(S.g))) return rc;
+    return session_admit(S, count, seed_ptr, seeds, max_iter, slots_out);
+}
+
+int egpr_session_step(egpr_session* h, int32_t sweeps, int32_t* done_slots, int32_t* ndone) {
+    using namespace egpr;
+    if (!h || !h->st) return arg_error("NULL session");
+    if (!done_slots || !ndone) return arg_error("NULL argument");
+    SessionState& S = *h->st;
+    std::lock_guard<std::mutex> lk(S.g->mu);
+    int rc;
+    if ((rc = check_device(S.g))) return rc;
+    return session_step(S, sweeps, done_slots, ndone);
+}
+
+int egpr_session_collect(egpr_session* h, int32_t count, const int32_t* slots, uint32_t flags, double* out,
+                         egpr_stats* stats) {
+    using namespace egpr;
+    if (!h || !h->st) return arg_error("NULL session");
+    if (count < 0 || (count > 0 && !slots)) return arg_error("NULL argument");
+    if (count == 0) return EGPR_SUCC;
+    SessionState& S = *h->st;
+    std::lock_guard<std::mutex> lk(S.g->mu);
+    int rc;
+    if ((rc = check_device(S.g))) return rc;
+    return session_collect(S, count, slots, flags, out, stats);
+}
+
+int egpr_session_info(const egpr_session* h, int32_t* slots, int32_t* running, int32_t* done) {
+    using namespace egpr;
+    if (!h || !h->st || !slots || !running || !done) return arg_error("NULL argument");
+    const SessionState& S = *h->st;
+    *slots = S.slots;
+    *running = 0;
+    *done = 0;
+    for (uint8_t st : S.state) {
+        *running += st == kSlotRunning ? 1 : 0;
+        *done += st == kSlotDone ? 1 : 0;
+    }
+    return EGPR_SUCC;
+}
+
+int egpr_session_destroy(egpr_session* h) {
+    using namespace egpr;
+    if (!h) return EGPR_SUCC;
+    if (h->st) {
+        egpr_graph* g = h->st->g;
+        std::lock_guard<std::mutex> lk(g->mu);
+        cudaStreamSynchronize(g->stream);
+        delete h->st;
+        g->sessions -= 1;
+    }
+    delete h;
+    return EGPR_SUCC;
+}
+
+}  // extern "C"

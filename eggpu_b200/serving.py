@@ -5,11 +5,14 @@ registry.  The server keeps prepared graphs (inbound CSR and rank state) on
 the device, admits graphs by HBM bytes with least-recently-used eviction of
 idle graphs, and serves requests as they arrive:
 
-* every graph has at most one solve in flight; requests that arrive while it
-  runs queue up and are folded into that graph's next solve: all queued PPR
-  requests go to one ``egpr_pagerank_seeds`` call (one batched SpMM solve
-  from six columns on, single-vector solves below), all queued plain requests
-  share one solve (their answer is identical);
+* continuous batching of PPR: a graph with PPR requests waiting keeps one
+  batched SpMM solve running (``egpr_session``); requests that arrive while it
+  runs join it in free column slots between steps of a few sweeps, each
+  leaves it (FP64 correction, normalisation, copy out) as soon as its own stop
+  rule fires, and its slot is reused; requests with other alpha / tol, and
+  a lone request when no batched solve is running, take one-shot solves;
+* queued plain requests for a graph share one solve (their answer is
+  identical);
 * solves on different graphs run concurrently from a pool of worker threads,
   each prepared graph on its own CUDA stream, so their kernels overlap on the
   device;
@@ -167,8 +170,15 @@ class Server:
     """Serves Request objects; submit() returns a Future resolving to (ranks, stats)."""
 
     def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True, pinned=True,
-                 multi_min=8, ppr_min_batch=1):
+                 multi_min=8, ppr_min_batch=1, sessions=True, session_slots=32, session_sweeps=4, session_min=2):
         self.registry = registry
+        # continuous batching: a graph with at least session_min PPR requests
+        # waiting gets a running batched solve (egpr_session) of session_slots
+        # column slots; requests join it between steps of session_sweeps sweeps
+        self.sessions = bool(sessions)
+        self.session_slots = int(session_slots)
+        self.session_sweeps = int(session_sweeps)
+        self.session_min = int(session_min)
         # PPR groups smaller than this go through the dense single-vector
         # entry one request at a time; otherwise through egpr_pagerank_seeds,
         # which itself solves fewer than six columns as single-vector solves
@@ -277,33 +287,92 @@ class Server:
             return
         gid, reqs = work[0]
         pg = self.registry.acquire(gid)
+        session = None
         try:
-            by_params = collections.defaultdict(list)
-            for r in reqs:
-                by_params[(r.kind, r.alpha, r.max_iter, r.tol)].append(r)
-            for (kind, alpha, max_iter, tol), group in by_params.items():
-                if kind == "pr":
-                    ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol, out=self._out(pg.n))
-                    self.stats["pr_solves"] += 1
-                    for r in group:
-                        self._finish(r, ranks, st)
-                elif len(group) < self.ppr_min_batch:
-                    for r in group:
-                        ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol,
-                                                personalization=_teleport(pg.n, r.seeds), out=self._out(pg.n))
-                        self.stats["ppr_single"] += 1
-                        self._finish(r, ranks, st)
+            if not self.sessions:
+                self._serve_groups(pg, reqs)
+                return
+            # Continuous batching: while this graph has PPR work, one batched
+            # solve stays running; requests that arrive meanwhile join it in free
+            # column slots between steps of a few sweeps, and each leaves it as
+            # soon as its own stop rule fires.
+            running = {}  # slot -> request
+            waiting = []  # PPR requests of the session's parameters without a free slot yet
+            pending = list(reqs)
+            while True:
+                with self.cv:  # requests that arrived while this graph was being served
+                    more = self.queues.pop(gid, None)
+                if more:
+                    pending.extend(more)
+                ppr = [r for r in pending if r.kind == "ppr"]
+                others = [r for r in pending if r.kind != "ppr"]
+                pending = []
+                if session is None and len(ppr) >= self.session_min:
+                    r0 = ppr[0]
+                    session = _native.Session(pg, alpha=r0.alpha, tol=r0.tol, slots=self.session_slots)
+                    self.stats["sessions"] += 1
+                if session is not None:
+                    fits = [r for r in ppr if r.alpha == session.alpha and r.tol == session.tol]
+                    others += [r for r in ppr if not (r.alpha == session.alpha and r.tol == session.tol)]
+                    waiting += fits
                 else:
-                    for s in range(0, len(group), self.max_columns):
-                        part = group[s:s + self.max_columns]
-                        ranks, sts = pg.pagerank_seeds([r.seeds for r in part], alpha=alpha, max_iter=max_iter,
-                                                       tol=tol, out=self._out((len(part), pg.n)))
-                        self.stats["ppr_batches"] += 1
-                        self.stats["ppr_columns"] += len(part)
-                        for j, r in enumerate(part):
-                            self._finish(r, ranks[j], sts[j])
+                    others += ppr
+                if others:
+                    self._serve_groups(pg, others)
+                if session is not None:
+                    free = session.info()["free"]
+                    take, waiting = waiting[:free], waiting[free:]
+                    by_iter = collections.defaultdict(list)
+                    for r in take:
+                        by_iter[r.max_iter].append(r)
+                    for max_iter, group in by_iter.items():
+                        for sl, r in zip(session.admit([r.seeds for r in group], max_iter=max_iter), group):
+                            running[sl] = r
+                        self.stats["session_admitted"] += len(group)
+                    if running:
+                        done = session.step(self.session_sweeps)
+                        self.stats["session_steps"] += 1
+                        if done:
+                            out, sts = session.collect(done, out=self._out((len(done), pg.n)))
+                            for i, sl in enumerate(done):
+                                self._finish(running.pop(sl), out[i], sts[i])
+                if not running and not waiting:
+                    with self.cv:
+                        if not self.queues.get(gid):
+                            break  # nothing left for this graph; later requests start a new round
         finally:
+            if session is not None:
+                session.close()
             self.registry.release(gid)
+
+    def _serve_groups(self, pg, reqs):
+        """Requests served by one-shot solves: plain PageRank (one solve per
+        parameter set, shared by its requests), and PPR as single-vector solves
+        (small groups) or one batched solve per group."""
+        by_params = collections.defaultdict(list)
+        for r in reqs:
+            by_params[(r.kind, r.alpha, r.max_iter, r.tol)].append(r)
+        for (kind, alpha, max_iter, tol), group in by_params.items():
+            if kind == "pr":
+                ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol, out=self._out(pg.n))
+                self.stats["pr_solves"] += 1
+                for r in group:
+                    self._finish(r, ranks, st)
+            elif len(group) < self.ppr_min_batch:
+                for r in group:
+                    ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol,
+                                            personalization=_teleport(pg.n, r.seeds), out=self._out(pg.n))
+                    self.stats["ppr_single"] += 1
+                    self._finish(r, ranks, st)
+            else:
+                for s in range(0, len(group), self.max_columns):
+                    part = group[s:s + self.max_columns]
+                    ranks, sts = pg.pagerank_seeds([r.seeds for r in part], alpha=alpha, max_iter=max_iter,
+                                                   tol=tol, out=self._out((len(part), pg.n)))
+                    self.stats["ppr_batches"] += 1
+                    self.stats["ppr_columns"] += len(part)
+                    for j, r in enumerate(part):
+                        self._finish(r, ranks[j], sts[j])
 
     def _run_multi(self, work):
         gids = [gid for gid, _ in work]

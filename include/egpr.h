@@ -216,6 +216,39 @@ EGPR_API int egpr_pagerank_seeds(egpr_graph* g, double alpha, int32_t max_iter, 
                         const int32_t* seed_ptr, const int32_t* seeds, uint32_t flags, double* out,
                         egpr_stats* stats);
 
+/* ---- continuous batching of personalised PageRank ---------------------- */
+
+/*
+ * No counterpart in the reference.  A session keeps one batched solve of a
+ * prepared graph running so that requests can join it while it runs: slots
+ * (columns of the CSR x dense SpMM, 1..512, rounded up to a multiple of 32)
+ * are filled by egpr_session_admit between steps, egpr_session_step runs a
+ * few sweeps of every running column, and a finished column is collected
+ * (FP64 correction sweep unless EGPR_FLAG_NO_CORRECTION, normalisation, copy
+ * to the host) and its slot freed while the other columns keep sweeping.
+ * Every column has the maths, stop rule (err < tol * n) and sweep limit of a
+ * seed-set solve of egpr_pagerank_seeds on its own; alpha and tol are the
+ * session's.  Calls on a session lock its graph.  A graph with live sessions
+ * refuses egpr_graph_destroy and layout changes of the batched solve.
+ */
+typedef struct egpr_session egpr_session;
+
+EGPR_API int egpr_session_create(egpr_graph* g, double alpha, double tol, int32_t slots, egpr_session** out);
+/* count requests with seed sets seeds[seed_ptr[i] .. seed_ptr[i+1]) each, up
+ * to max_iter sweeps of their own; slots_out[count] receives their slots.
+ * Fails (EGPR_INVALID_ARGUMENT) without admitting any when fewer slots are free. */
+EGPR_API int egpr_session_admit(egpr_session* s, int32_t count, const int32_t* seed_ptr, const int32_t* seeds,
+                                int32_t max_iter, int32_t* slots_out);
+/* Runs up to `sweeps` sweeps of the running columns; done_slots (capacity:
+ * the session's slots) receives every finished, not yet collected slot. */
+EGPR_API int egpr_session_step(egpr_session* s, int32_t sweeps, int32_t* done_slots, int32_t* ndone);
+/* Results of finished slots: out is count x n (row i = slots[i]); stats
+ * (nullable) count entries, iterations counted from each column's start. */
+EGPR_API int egpr_session_collect(egpr_session* s, int32_t count, const int32_t* slots, uint32_t flags, double* out,
+                                  egpr_stats* stats);
+EGPR_API int egpr_session_info(const egpr_session* s, int32_t* slots, int32_t* running, int32_t* done);
+EGPR_API int egpr_session_destroy(egpr_session* s);
+
 /*
  * Many independent graphs in one persistent launch per sweep: the work
  * tiles of all graphs form one queue; every graph keeps its own residual,

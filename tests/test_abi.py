@@ -97,6 +97,11 @@ def test_bad_arguments_are_refused_through_the_abi_before_any_device_work():
         ("egpr_pagerank_csr", (None, 3, ep, 2, None, 1, 0.85, 10, 1e-6, p, None), b"NULL argument"),
         ("egpr_pagerank_csr", (vp, 3, ep, 2, None, 1, 0.85, 10, 1e-6, None, None), b"NULL argument"),
         ("egpr_cache_stats_get", (None,), b"NULL argument"),
+        ("egpr_session_create", (None, 0.85, 1e-6, 32, ctypes.byref(handle)), b"NULL argument"),
+        ("egpr_session_admit", (None, 1, p, p, 10, p), b"NULL session"),
+        ("egpr_session_step", (None, 4, p, ctypes.byref(ctypes.c_int32())), b"NULL session"),
+        ("egpr_session_collect", (None, 1, p, 0, p, None), b"NULL session"),
+        ("egpr_session_info", (None, None, None, None), b"NULL argument"),
     ]
     for name, args, msg in cases:
         rc = getattr(lib, name)(*args)
@@ -104,6 +109,7 @@ def test_bad_arguments_are_refused_through_the_abi_before_any_device_work():
         assert msg in lib.egpr_last_error(), (name, lib.egpr_last_error())
     assert handle.value is None  # nothing was created
     assert lib.egpr_graph_destroy(None) == _native.EGPR_SUCC  # destroying nothing is allowed
+    assert lib.egpr_session_destroy(None) == _native.EGPR_SUCC
 
 
 def test_a_missing_device_is_an_error_status_not_a_crash():

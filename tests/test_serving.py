@@ -58,6 +58,52 @@ class FakePrepared:
             FakePrepared.live -= 1
 
 
+class FakeSession:
+    """Stands in for _native.Session: a request's answer comes from the oracle
+    when it is admitted and it finishes after ceil(iterations / sweeps) steps;
+    admissions and steps are recorded in order."""
+
+    def __init__(self, graph, alpha=0.85, tol=1e-6, slots=32):
+        self.g, self.alpha, self.tol, self.slots, self.n = graph, alpha, tol, slots, graph.n
+        self.cols = {}  # slot -> [ranks, stats, steps left]
+        FakePrepared.calls.append(("session", self.n))
+
+    def info(self):
+        running = sum(1 for c in self.cols.values() if c[2] > 0)
+        done = len(self.cols) - running
+        return {"slots": self.slots, "running": running, "done": done, "free": self.slots - len(self.cols)}
+
+    def admit(self, seed_sets, max_iter=100):
+        free = [j for j in range(self.slots) if j not in self.cols][: len(seed_sets)]
+        assert len(free) == len(seed_sets)
+        for j, s in zip(free, seed_sets):
+            p = np.zeros(self.n)
+            p[np.unique(s)] = 1.0
+            r, it, _ = oracle.pagerank_push(self.g.V, self.g.E, self.g.W, alpha=self.alpha, max_iter=max_iter,
+                                            tol=self.tol, teleport=p / p.sum())
+            self.cols[j] = [r, {"iterations": it}, it]
+        FakePrepared.calls.append(("admit", self.n, len(seed_sets)))
+        return free
+
+    def step(self, sweeps=4):
+        FakePrepared.calls.append(("step", self.n))
+        time.sleep(0.002)
+        for c in self.cols.values():
+            c[2] = max(0, c[2] - sweeps)
+        return [j for j, c in self.cols.items() if c[2] == 0]
+
+    def collect(self, slots, out=None):
+        rows = np.array([self.cols[j][0] for j in slots])
+        sts = [self.cols.pop(j)[1] for j in slots]
+        if out is not None:
+            out[:] = rows
+            return out, sts
+        return rows, sts
+
+    def close(self):
+        pass
+
+
 def fake_multi(graphs, alpha, max_iter, tol):
     FakePrepared.calls.append(("multi", len(graphs)))
     outs, sts = [], []
@@ -74,6 +120,7 @@ def fake_engine(monkeypatch):
     FakePrepared.live = 0
     monkeypatch.setattr(_native, "PreparedGraph", FakePrepared)
     monkeypatch.setattr(_native, "pagerank_multi", fake_multi)
+    monkeypatch.setattr(_native, "Session", FakeSession)
     yield
 
 
@@ -110,9 +157,9 @@ def test_requests_are_folded_and_answers_match_standalone(fake_engine):
         alone, it, _ = oracle.pagerank_push(V, E, W, teleport=tele)
         assert np.array_equal(ranks, alone) and st["iterations"] == it
     srv.close()
-    solves = [c for c in FakePrepared.calls if c[0] in ("pr", "ppr")]
+    solves = [c for c in FakePrepared.calls if c[0] in ("pr", "ppr", "admit")]
     assert len(solves) < len(reqs)  # folding happened
-    assert any(c[0] == "ppr" and c[2] > 1 for c in solves)
+    assert any(c[0] == "admit" and c[2] > 1 for c in solves)  # several PPR requests joined one batched solve
     lat = serving.latency_summary(reqs)
     assert lat["count"] == 60 and lat["p99_ms"] >= lat["p50_ms"]
 
@@ -149,7 +196,7 @@ def test_plain_requests_of_small_graphs_share_a_launch_past_a_threshold(fake_eng
 def test_a_few_ppr_requests_are_solved_one_by_one(fake_engine):
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=1, ppr_min_batch=4)
+    srv = serving.Server(reg, workers=1, ppr_min_batch=4, sessions=False)
     rng = np.random.default_rng(1)
     reqs = [serving.Request(2, "ppr", seeds=rng.choice(src[2][0].shape[0] - 1, 3, replace=False)) for _ in range(3)]
     for r in reqs:
@@ -164,6 +211,40 @@ def test_a_few_ppr_requests_are_solved_one_by_one(fake_engine):
     srv.close()
     assert not any(c[0] == "ppr" for c in FakePrepared.calls)
     assert srv.stats["ppr_single"] == 3
+    reg.close()
+
+
+def test_requests_arriving_mid_solve_join_the_running_batched_solve(fake_engine):
+    """Continuous batching: PPR requests that arrive while a graph's batched
+    solve is running are admitted into it between steps (no waiting for the
+    running requests to finish), and every answer is its answer alone."""
+    src = _sources()
+    reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
+    srv = serving.Server(reg, workers=1, session_sweeps=2)
+    rng = np.random.default_rng(4)
+    n = src[3][0].shape[0] - 1
+    early = [serving.Request(3, "ppr", seeds=rng.choice(n, 3, replace=False), max_iter=200, tol=1e-9)
+             for _ in range(3)]
+    late = [serving.Request(3, "ppr", seeds=rng.choice(n, 2, replace=False), max_iter=200, tol=1e-9)
+            for _ in range(4)]
+    for r in early:
+        srv.submit(r)
+    while not any(c[0] == "step" for c in FakePrepared.calls):
+        time.sleep(0.001)
+    for r in late:  # the early requests are on the device now
+        srv.submit(r)
+    for r in early + late:
+        ranks, st = r.future.result(timeout=60)
+        p = np.zeros(n)
+        p[np.unique(r.seeds)] = 1.0
+        alone, it, _ = oracle.pagerank_push(*src[3], teleport=p / p.sum(), max_iter=200, tol=1e-9)
+        assert np.array_equal(ranks, alone) and st["iterations"] == it
+    srv.close()
+    events = [c[0] for c in FakePrepared.calls if c[0] in ("session", "admit", "step")]
+    assert events.count("session") == 1  # one running solve served both waves
+    first_admit, second_admit = [i for i, e in enumerate(events) if e == "admit"][:2]
+    assert "step" in events[first_admit:second_admit]  # the second wave joined after the solve had started
+    assert max(r.done_at for r in early) > min(r.arrival for r in late)  # ... while the first wave was running
     reg.close()
 
 
