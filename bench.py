@@ -426,9 +426,9 @@ def run_ours(args):
     # the batched-PPR and serving configs, measured after the timed region
     ppr = served = None
     if rank == 0 and world == 1 and args.with_ppr:
-        res = measure_ppr(args)
-        if res is not None:
-            ppr = {"config": res[1], **res[0]}
+        got = measure_ppr(args)
+        if got is not None:
+            ppr = {"config": got[1], **got[0]}
     if rank == 0 and world == 1 and args.with_serving:
         out, cfg = measure_serving(args)
         served = {"config": cfg, **out}
@@ -611,23 +611,37 @@ def measure_serving(args):
     budget = int(args.serving_hbm_gb * 2**30)
     reg = serving.GraphRegistry(src, budget_bytes=budget)
     warm_s = reg.warm(range(count))  # graphs are loaded before traffic starts
-    srv = serving.Server(reg, workers=int(os.environ.get("EGPR_SERVING_WORKERS", "4")))
+    workers = int(os.environ.get("EGPR_SERVING_WORKERS", "4"))
     times = serving.poisson_arrivals(1000.0, n_req, seed=2001)
+    # steady state: a warm-up burst of every request (host and device memory
+    # pools grown, every graph's batched layout built) before any measured
+    # replay, so neither mode pays first-use costs the other does not
+    n_warm = n_req
+    warm = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
+    srv_w = serving.Server(reg, workers=workers)
+    serving.replay(srv_w, warm, np.zeros(n_req))
+    srv_w.close()
+    srv = serving.Server(reg, workers=workers)
     wall = serving.replay(srv, reqs, times)
     srv.close()
     lat = serving.latency_summary(reqs)
     # the same arrivals without continuous batching: PPR requests that arrive
     # while a graph is being served wait for its running solve to end
     again = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
-    srv1 = serving.Server(reg, workers=int(os.environ.get("EGPR_SERVING_WORKERS", "4")), sessions=False)
+    srv1 = serving.Server(reg, workers=workers, sessions=False)
     wall1 = serving.replay(srv1, again, times)
     srv1.close()
     lat_one_shot = serving.latency_summary(again)
     # capacity: the same requests all at once (queued requests fold into batched solves)
     burst = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
-    srv2 = serving.Server(reg, workers=int(os.environ.get("EGPR_SERVING_WORKERS", "4")))
+    srv2 = serving.Server(reg, workers=workers)
     burst_wall = serving.replay(srv2, burst, np.zeros(n_req))
     srv2.close()
+    burst1 = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
+    srv3 = serving.Server(reg, workers=workers, sessions=False)
+    burst1_wall = serving.replay(srv3, burst1, np.zeros(n_req))
+    srv3.close()
+    long_solves = measure_long_solves(workers)
     # plain unbatched per-request solves of a sample, on the same GPU
     sample = reqs[:: max(1, n_req // 200)]
     plain_lat = []
@@ -647,6 +661,7 @@ def measure_serving(args):
                        f"R-MAT graphs n log-uniform in [1e3, {max_n:.0e}] (ids >= n dropped), edgefactor "
                        "uniform in [8, 32], seeds 2000-2063, alpha 0.85, tol 1e-6",
            "requests": n_req, "hbm_budget_gb": args.serving_hbm_gb,
+           "warmup": f"a burst of all {n_warm} requests before the measured replays",
            "graphs_loaded_before_traffic_s": warm_s,
            "total_nnz": int(sum(len(v[1]) for v in src.values()))}
     out = {"latency": lat, "solves_per_s": n_req / wall, "offered_req_per_s": 1000.0,
@@ -654,13 +669,48 @@ def measure_serving(args):
            "without_continuous_batching": {"latency": lat_one_shot, "solves_per_s": n_req / wall1,
                                            "server_stats": dict(srv1.stats)},
            "capacity_burst": {"solves_per_s": n_req / burst_wall, "wall_s": burst_wall,
-                              "server_stats": dict(srv2.stats)},
+                              "server_stats": dict(srv2.stats),
+                              "without_continuous_batching": {"solves_per_s": n_req / burst1_wall,
+                                                              "wall_s": burst1_wall,
+                                                              "server_stats": dict(srv3.stats)}},
            "plain_unbatched_service_ms": {"p50": float(np.percentile(plain, 50) * 1e3),
                                           "p99": float(np.percentile(plain, 99) * 1e3),
                                           "mean": float(plain.mean() * 1e3)},
-           "plain_unbatched_capacity_solves_per_s": float(1.0 / plain.mean())}
+           "plain_unbatched_capacity_solves_per_s": float(1.0 / plain.mean()),
+           "long_solves": long_solves}
     reg.close()
     return out, cfg
+
+
+def measure_long_solves(workers):
+    """Continuous batching where it pays: fixed-sweep PPR requests (100 sweeps,
+    tol 0, 1-16 seeds) at 2000 req/s on one R-MAT scale-16 graph (seed 3,
+    edgefactor 16), served with sessions and with one-shot batched solves only."""
+    from eggpu_b200 import serving, synth
+
+    c = synth.rmat(scale=16, edgefactor=16, seed=3)
+    reg = serving.GraphRegistry({0: (c.V, c.E, None)}, budget_bytes=8 << 30)
+    reg.warm([0])
+    n = c.V.shape[0] - 1
+    rng = np.random.Generator(np.random.PCG64(6))
+    seeds = [rng.choice(n, int(rng.integers(1, 17)), replace=False) for _ in range(2000)]
+    times = serving.poisson_arrivals(2000.0, len(seeds), seed=7)
+    out = {"config": "R-MAT scale 16 (seed 3, edgefactor 16), 2000 PPR requests of 100 sweeps (tol 0) with 1-16 "
+                     "seeds (numpy PCG64 seed 6), Poisson arrivals at 2000 req/s (seed 7), after a warm-up replay "
+                     "of 300 requests"}
+    for label, sessions in (("with_continuous_batching", True), ("without_continuous_batching", False)):
+        warm = [serving.Request(0, "ppr", seeds=s, tol=0.0, max_iter=100, keep_result=False) for s in seeds[:300]]
+        srv = serving.Server(reg, workers=workers, sessions=sessions)
+        serving.replay(srv, warm, times[:300])
+        srv.close()
+        reqs = [serving.Request(0, "ppr", seeds=s, tol=0.0, max_iter=100, keep_result=False) for s in seeds]
+        srv = serving.Server(reg, workers=workers, sessions=sessions)
+        wall = serving.replay(srv, reqs, times)
+        srv.close()
+        out[label] = {"latency": serving.latency_summary(reqs), "solves_per_s": len(reqs) / wall,
+                      "server_stats": dict(srv.stats)}
+    reg.close()
+    return out
 
 
 def run_precision25(args):

@@ -265,8 +265,9 @@ class PreparedGraph:
               "egpr_graph_set_stream")
 
     def pagerank(self, alpha=0.85, max_iter=100, tol=1e-6, personalization=None, correction=True, out=None):
-        """Returns (ranks float64[n], stats dict)."""
-        res = np.empty(self.n, np.float64) if out is None else out
+        """Returns (ranks float64[n], stats dict).  out: optional float64[n]
+        result array (page-locked memory makes the copy back faster)."""
+        res = self._vec_out(out)
         pers = None if personalization is None else _f64(personalization)
         if pers is not None and pers.shape[0] != self.n:
             raise ValueError("personalization must have n entries")
@@ -282,12 +283,18 @@ class PreparedGraph:
               "egpr_pagerank_enqueue")
 
     def collect(self, out=None, copy=True):
-        res = None
-        if copy:
-            res = np.empty(self.n, np.float64) if out is None else out
+        res = self._vec_out(out) if copy else None
         st = EgprStats()
         check(lib.egpr_pagerank_collect(self.handle, _ptr(res), ctypes.byref(st)), "egpr_pagerank_collect")
         return res, st.as_dict()
+
+    def _vec_out(self, out):
+        if out is None:
+            return np.empty(self.n, np.float64)
+        if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (self.n,)
+                or not out.flags.c_contiguous or not out.flags.writeable):
+            raise ValueError(f"out must be a writeable C-contiguous float64 array of shape ({self.n},)")
+        return out
 
     def _batch_out(self, k, out):
         if out is None:
@@ -399,8 +406,9 @@ class Session:
         k = len(slots)
         if out is None:
             out = np.empty((k, self.n), np.float64)
-        elif out.shape != (k, self.n) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
-            raise ValueError(f"out must be a C-contiguous float64 array of shape {(k, self.n)}")
+        elif (not isinstance(out, np.ndarray) or out.shape != (k, self.n) or out.dtype != np.float64
+              or not out.flags["C_CONTIGUOUS"] or not out.flags.writeable):
+            raise ValueError(f"out must be a writeable C-contiguous float64 array of shape {(k, self.n)}")
         sl = np.asarray(slots, np.int32)
         sts = (EgprStats * max(k, 1))()
         flags = 0 if correction else EGPR_FLAG_NO_CORRECTION

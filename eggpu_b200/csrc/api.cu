@@ -412,7 +412,7 @@ static int solve_single(egpr_graph* g, double alpha, int32_t max_iter, double to
         if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
     }
     NvtxRange nv_read("egpr readback");
-    if ((rc = cuda_ok(cudaMemcpyAsync(out, g->out.p, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ranks")))
+    if ((rc = download_d2h(out, g->out.p, (size_t)g->n * sizeof(double), s, "D2H ranks")))
         return rc;
     SolveOut o;
     if ((rc = read_single_state(g, s, &o))) return rc;
@@ -1031,7 +1031,7 @@ int egpr_pagerank_collect(egpr_graph* g, double* out_ranks, egpr_stats* stats) {
     }
     cudaStream_t s = g->stream;
     if (out_ranks &&
-        (rc = cuda_ok(cudaMemcpyAsync(out_ranks, g->out.p, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ranks")))
+        (rc = download_d2h(out_ranks, g->out.p, (size_t)g->n * sizeof(double), s, "D2H ranks")))
         return rc;
     SolveOut o;
     if ((rc = read_single_state(g, s, &o))) return rc;
@@ -1122,7 +1122,7 @@ int egpr_pagerank_multi(int32_t count, egpr_graph* const* graphs, double alpha, 
     if ((rc = cuda_ok(cudaEventRecord(mp->ev1, s), "event"))) return rc;
     for (size_t i = 0; i < live.size(); ++i) {
         egpr_graph* g = live[i];
-        if ((rc = cuda_ok(cudaMemcpyAsync(outs[live_idx[i]], g->out.p, (size_t)g->n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H ranks")))
+        if ((rc = download_d2h(outs[live_idx[i]], g->out.p, (size_t)g->n * sizeof(double), s, "D2H ranks")))
             return rc;
     }
     std::vector<GraphState> st(live.size());

@@ -309,6 +309,10 @@ int default_chunks_per_warp();  // EGPR_CHUNKS_PER_WARP, else 8
 int default_row_cost();         // EGPR_ROW_COST, else 4
 int32_t default_spmm_chunk();   // EGPR_SPMM_CHUNK, else 1024
 int export_in_col(const egpr_graph* g, int32_t* host, cudaStream_t s);
+// D2H of a result after the work enqueued on s: a plain async copy into
+// page-locked memory (or under 1 MiB); into pageable memory through the
+// page-locked staging pool, returning once the bytes are in dst.
+int download_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s, const char* what);
 
 // Binned single-graph sweep (bins.cu).
 bool bins_wanted(int32_t n, int64_t nnz);  // build the binned layout for this graph (EGPR_BINS, size)

@@ -1156,6 +1156,48 @@ int staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     return rc;
 }
 
+// D2H copy into a pageable host array through the staging pool, after the
+// work already enqueued on s: up to kStageSlots chunk copies in flight while
+// host threads move finished chunks out.  Returns once every byte is in dst.
+int staged_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    StagePool& P = stage_pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    for (int k = 0; k < kStageSlots; ++k)
+        if (!P.slot[k]) {
+            const cudaError_t e = cudaHostAlloc(&P.slot[k], kStageBytes, cudaHostAllocPortable);
+            if (e != cudaSuccess) {
+                P.slot[k] = nullptr;
+                cudaGetLastError();
+                int rc = cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "D2H (pageable)");
+                return rc ? rc : cuda_ok(cudaStreamSynchronize(s), "D2H (pageable)");
+            }
+        }
+    cudaEvent_t ev[kStageSlots] = {};
+    int rc = EGPR_SUCC;
+    for (int k = 0; k < kStageSlots && !rc; ++k)
+        rc = cuda_ok(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming), "event");
+    const size_t chunks = (bytes + kStageBytes - 1) / kStageBytes;
+    auto issue = [&](size_t i) {
+        const int k = (int)(i % kStageSlots);
+        const size_t off = i * kStageBytes, len = std::min(kStageBytes, bytes - off);
+        int r = cuda_ok(cudaMemcpyAsync(P.slot[k], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost, s),
+                        "D2H (staged)");
+        return r ? r : cuda_ok(cudaEventRecord(ev[k], s), "event");
+    };
+    for (size_t i = 0; i < std::min<size_t>(chunks, kStageSlots) && !rc; ++i) rc = issue(i);
+    for (size_t i = 0; i < chunks && !rc; ++i) {
+        const int k = (int)(i % kStageSlots);
+        const size_t off = i * kStageBytes, len = std::min(kStageBytes, bytes - off);
+        if ((rc = cuda_ok(cudaEventSynchronize(ev[k]), "staging"))) break;
+        parallel_memcpy(static_cast<char*>(dst) + off, P.slot[k], len);
+        if (i + kStageSlots < chunks) rc = issue(i + kStageSlots);
+    }
+    if (rc) cudaStreamSynchronize(s);  // no copy may still write into a slot once the pool is unlocked
+    for (int k = 0; k < kStageSlots; ++k)
+        if (ev[k]) cudaEventDestroy(ev[k]);
+    return rc;
+}
+
 struct HostInputs {
     cudaStream_t stream;            // the upload's stream: drained before unregistering
     std::vector<void*> registered;  // registered here, unregistered when the upload is done
@@ -1202,6 +1244,13 @@ int upload_h2d(void* dst, const void* src, size_t bytes, bool locked, cudaStream
     if (bytes == 0) return EGPR_SUCC;
     if (locked) return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), what);
     return staged_h2d(dst, src, bytes, s);
+}
+
+int download_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s, const char* what) {
+    if (bytes == 0) return EGPR_SUCC;
+    if (bytes < ((size_t)1 << 20) || host_page_locked(dst))
+        return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), what);
+    return staged_d2h(dst, src, bytes, s);
 }
 
 int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const double* W) {

@@ -38,6 +38,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdlib>
@@ -771,6 +772,13 @@ __global__ void k_sp_tele_rows_at(const int32_t* __restrict__ tv, int32_t nt, in
     if (t < nt) meta[tv[t]] |= (uint32_t)(row0 + t + 1);
 }
 
+// Teleport entry writes of a session: tele[at[i]] = val[i] (distinct at).
+__global__ void k_sp_tele_write(float* __restrict__ tele, const uint64_t* __restrict__ at,
+                                const float* __restrict__ val, int64_t count) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) tele[at[i]] = val[i];
+}
+
 // X0 = 1/n on live columns, 0 on padding columns and on row n of both
 // iterates (grid.y = panel, 16-byte stores); column states.
 __global__ void k_sp_init(float* X0, float* X1, ColState* cols, int32_t n, int32_t npanels, int32_t k, double alpha,
@@ -942,9 +950,16 @@ struct SpmmWork {
     ~SpmmWork() {
         if (cg_exec) cudaGraphExecDestroy(cg_exec);
         if (cg) cudaGraphDestroy(cg);
-        for (DevBuf* b : {&src, &c32, &c64, &chunks, &X0, &X1, &out64, &cols, &parts, &span_cnt, &gacc, &colsum, &ctl,
-                          &meta, &params, &out, &tele, &tele_v})
-            b->release();
+        for (DevBuf* b : buffers()) b->release();
+    }
+    // Frees the buffers in the order of stream s (no wait for the device, so
+    // other graphs' solves on other streams keep running).
+    void release_on(cudaStream_t s) {
+        for (DevBuf* b : buffers()) b->release_on(s);
+    }
+    std::array<DevBuf*, 18> buffers() {
+        return {&src, &c32, &c64, &chunks, &X0, &X1, &out64, &cols, &parts, &span_cnt, &gacc, &colsum, &ctl,
+                &meta, &params, &out, &tele, &tele_v};
     }
 };
 
@@ -1173,9 +1188,8 @@ int solve_group(egpr_graph* g, SpmmWork& w, double alpha, int32_t max_iter, doub
     }
     if ((rc = cuda_ok(cudaGetLastError(), "spmm finish"))) return rc;
     if ((rc = cuda_ok(cudaEventRecord(g->ev1, s), "event"))) return rc;
-    if (out && (rc = cuda_ok(cudaMemcpyAsync(out, w.out.p, (size_t)kg * n * sizeof(double), cudaMemcpyDeviceToHost, s),
-                             "D2H ranks")))  // out == NULL: device timing only (the tuner)
-        return rc;
+    // out == NULL: device timing only (the tuner)
+    if (out && (rc = download_d2h(out, w.out.p, (size_t)kg * n * sizeof(double), s, "D2H ranks"))) return rc;
     std::vector<ColState> hc((size_t)npanels * kLanes);
     Ctl ctl;
     if ((rc = cuda_ok(cudaMemcpyAsync(hc.data(), w.cols.p, hc.size() * sizeof(ColState), cudaMemcpyDeviceToHost, s),
@@ -1299,14 +1313,25 @@ struct SessionState {
     std::vector<double> started, device_s;      // per slot: admission time, device time while live
     std::unordered_map<int32_t, int32_t> row_of_vertex;
     std::vector<int32_t> row_vertex;  // teleport row -> vertex
-    std::vector<float> tt;            // teleport rows x (npanels * 32)
+    // teleport matrix (rows x npanels * 32) on the device only: admissions and
+    // collections queue entry writes (last write wins), applied by a scatter
+    // before the next step
+    std::unordered_map<uint64_t, float> tele_writes;
+    int32_t tele_cap_rows = 0;        // rows the device teleport buffer holds
     int32_t rows_on_device = 0;       // rows whose meta bits are set
     bool tele_dirty = false;
-    DevBuf out_row;
+    DevBuf out_row, tele_upd;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     ~SessionState() {
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
+        // stream-ordered frees: closing a session does not wait for the
+        // solves of other graphs running on other streams
+        if (g) {
+            w.release_on(g->stream);
+            out_row.release_on(g->stream);
+            tele_upd.release_on(g->stream);
+        }
         out_row.release();
     }
 };
@@ -1350,13 +1375,45 @@ int session_upload(SessionState& S, int32_t active, cudaStream_t s) {
     SpmmWork& w = S.w;
     int rc;
     if (S.tele_dirty) {
-        const size_t bytes = std::max<size_t>(S.tt.size(), 1) * sizeof(float);
-        if ((rc = w.tele.grow_on(bytes, s))) return rc;
-        if (!S.tt.empty() &&
-            (rc = cuda_ok(cudaMemcpyAsync(w.tele.p, S.tt.data(), S.tt.size() * sizeof(float), cudaMemcpyHostToDevice, s),
-                          "H2D teleport")))
-            return rc;
         const int32_t nrows = (int32_t)S.row_vertex.size();
+        const size_t ld = (size_t)S.npanels * kLanes;
+        if (nrows > S.tele_cap_rows) {  // grow: zeroed, the old rows copied over
+            const int32_t cap = std::max(nrows, std::max(2 * S.tele_cap_rows, 256));
+            DevBuf nb;
+            if ((rc = nb.grow_on((size_t)cap * ld * sizeof(float), s))) return rc;
+            if ((rc = cuda_ok(cudaMemsetAsync(nb.p, 0, (size_t)cap * ld * sizeof(float), s), "memset")) ||
+                (S.tele_cap_rows > 0 &&
+                 (rc = cuda_ok(cudaMemcpyAsync(nb.p, w.tele.p, (size_t)S.tele_cap_rows * ld * sizeof(float),
+                                               cudaMemcpyDeviceToDevice, s), "D2D teleport")))) {
+                nb.release_on(s);
+                return rc;
+            }
+            w.tele.release_on(s);
+            w.tele = nb;
+            S.tele_cap_rows = cap;
+        }
+        const size_t nw = S.tele_writes.size();
+        if (nw > 0) {
+            std::vector<uint64_t> at;
+            std::vector<float> val;
+            at.reserve(nw);
+            val.reserve(nw);
+            for (const auto& kv : S.tele_writes) {
+                at.push_back(kv.first);
+                val.push_back(kv.second);
+            }
+            if ((rc = S.tele_upd.grow_on(nw * (sizeof(uint64_t) + sizeof(float)), s)) ||
+                (rc = cuda_ok(cudaMemcpyAsync(S.tele_upd.p, at.data(), nw * sizeof(uint64_t), cudaMemcpyHostToDevice, s),
+                              "H2D teleport writes")) ||
+                (rc = cuda_ok(cudaMemcpyAsync(S.tele_upd.as<uint64_t>() + nw, val.data(), nw * sizeof(float),
+                                              cudaMemcpyHostToDevice, s), "H2D teleport writes")))
+                return rc;
+            k_sp_tele_write<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(
+                w.tele.as<float>(), S.tele_upd.as<uint64_t>(),
+                reinterpret_cast<const float*>(S.tele_upd.as<uint64_t>() + nw), (int64_t)nw);
+            // the host arrays may go: pageable copies return once their data is staged
+            S.tele_writes.clear();
+        }
         if (nrows > S.rows_on_device) {
             const int32_t nt = nrows - S.rows_on_device;
             if ((rc = w.tele_v.grow_on((size_t)nt * sizeof(int32_t), s)) ||
@@ -1456,11 +1513,10 @@ int session_admit(SessionState& S, int32_t count, const int32_t* seed_ptr, const
                 r = (int32_t)S.row_vertex.size();
                 S.row_of_vertex.emplace(v, r);
                 S.row_vertex.push_back(v);
-                S.tt.resize((size_t)(r + 1) * ld, 0.f);
             } else {
                 r = it->second;
             }
-            S.tt[(size_t)r * ld + j] = val;
+            S.tele_writes[(uint64_t)r * (uint64_t)ld + (uint64_t)j] = val;
             S.rows_of[(size_t)j].push_back(r);
         }
         // the panel's sweep count: that of its live columns, if any
@@ -1597,8 +1653,7 @@ int session_collect(SessionState& S, int32_t count, const int32_t* slots, uint32
                                       S.out_row.as<int32_t>());
     if ((rc = cuda_ok(cudaGetLastError(), "session collect"))) return rc;
     if ((rc = cuda_ok(cudaEventRecord(S.e1, s), "event"))) return rc;
-    if (out && (rc = cuda_ok(cudaMemcpyAsync(out, S.w.out.p, (size_t)count * n * sizeof(double), cudaMemcpyDeviceToHost,
-                                             s), "D2H ranks")))
+    if (out && (rc = download_d2h(out, S.w.out.p, (size_t)count * n * sizeof(double), s, "D2H ranks")))
         return rc;
     if ((rc = cuda_ok(cudaStreamSynchronize(s), "session collect"))) return rc;
     float ms = 0.f;
@@ -1619,7 +1674,7 @@ int session_collect(SessionState& S, int32_t count, const int32_t* slots, uint32
             st.bytes_per_iter = (int64_t)S.npanels * (S.w.epad * 8 + 2 * ((int64_t)n + 1) * kLanes * 4 + 4 * (int64_t)n);
         }
         // free the slot: its teleport entries go, its state is a free column again
-        for (int32_t r : S.rows_of[(size_t)j]) S.tt[(size_t)r * ld + j] = 0.f;
+        for (int32_t r : S.rows_of[(size_t)j]) S.tele_writes[(uint64_t)r * (uint64_t)ld + (uint64_t)j] = 0.f;
         S.rows_of[(size_t)j].clear();
         std::memset(&S.cols[(size_t)j], 0, sizeof(ColState));
         S.cols[(size_t)j].done = 1;

@@ -5,12 +5,14 @@ registry.  The server keeps prepared graphs (inbound CSR and rank state) on
 the device, admits graphs by HBM bytes with least-recently-used eviction of
 idle graphs, and serves requests as they arrive:
 
-* continuous batching of PPR: a graph with PPR requests waiting keeps one
+* continuous batching of PPR for long solves: a graph with several PPR
+  requests waiting whose solves are expected to take many sweeps keeps one
   batched SpMM solve running (``egpr_session``); requests that arrive while it
   runs join it in free column slots between steps of a few sweeps, each
   leaves it (FP64 correction, normalisation, copy out) as soon as its own stop
-  rule fires, and its slot is reused; requests with other alpha / tol, and
-  a lone request when no batched solve is running, take one-shot solves;
+  rule fires, and its slot is reused;
+* other PPR requests waiting for a graph share one one-shot batched solve
+  (``egpr_pagerank_seeds``; fewer than six go as single-vector solves);
 * queued plain requests for a graph share one solve (their answer is
   identical);
 * solves on different graphs run concurrently from a pool of worker threads,
@@ -170,15 +172,30 @@ class Server:
     """Serves Request objects; submit() returns a Future resolving to (ranks, stats)."""
 
     def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True, pinned=True,
-                 multi_min=8, ppr_min_batch=1, sessions=True, session_slots=32, session_sweeps=4, session_min=2):
+                 multi_min=8, ppr_min_batch=1, sessions=True, session_slots=256, session_sweeps=4, session_min=6,
+                 session_min_sweeps=48, session_max_bytes=2 << 30):
         self.registry = registry
         # continuous batching: a graph with at least session_min PPR requests
         # waiting gets a running batched solve (egpr_session) of session_slots
-        # column slots; requests join it between steps of session_sweeps sweeps
+        # column slots; requests join it between steps of session_sweeps sweeps.
+        # A sweep of a 32-column panel costs about as much as four or five
+        # single-vector sweeps, so fewer waiting requests take one-shot solves
+        # (the batched entry's own threshold is six columns as well).
         self.sessions = bool(sessions)
         self.session_slots = int(session_slots)
         self.session_sweeps = int(session_sweeps)
         self.session_min = int(session_min)
+        # a session's iterates and results take 16 bytes per slot and vertex:
+        # its slots are cut (in panels of 32, at least one) to session_max_bytes
+        self.session_max_bytes = int(session_max_bytes)
+        # ... and only for requests whose solves are long: a session pays when
+        # requests arriving during a solve would otherwise wait for many
+        # sweeps.  The expected sweep count is max_iter for fixed-sweep
+        # requests (tol 0), else a running mean of the counts seen for the same
+        # graph and parameters (unknown: one-shot solves, which record it).
+        # session_min_sweeps <= 0 drops the condition.
+        self.session_min_sweeps = int(session_min_sweeps)
+        self.sweeps_seen = {}  # (graph, alpha, tol) -> running mean of PPR sweep counts
         # PPR groups smaller than this go through the dense single-vector
         # entry one request at a time; otherwise through egpr_pagerank_seeds,
         # which itself solves fewer than six columns as single-vector solves
@@ -273,7 +290,22 @@ class Server:
     def _finish(self, req, ranks, stats):
         req.done_at = time.perf_counter()
         req.iterations = int(stats["iterations"])
+        if req.kind == "ppr":
+            key = (req.graph, req.alpha, req.tol)
+            old = self.sweeps_seen.get(key)
+            self.sweeps_seen[key] = req.iterations if old is None else 0.8 * old + 0.2 * req.iterations
         req.future.set_result((ranks if req.keep_result else None, stats))
+
+    def _session_slots(self, n):
+        fit = self.session_max_bytes // (16 * max(int(n), 1)) // 32 * 32
+        return max(32, min(self.session_slots, fit))
+
+    def _long_solves(self, gid, r):
+        """Whether PPR requests like r on graph gid are expected to take at least session_min_sweeps sweeps."""
+        if self.session_min_sweeps <= 0:
+            return True
+        expected = r.max_iter if r.tol <= 0 else self.sweeps_seen.get((gid, r.alpha, r.tol))
+        return expected is not None and expected >= self.session_min_sweeps
 
     def _out(self, shape):
         # page-locked up to pinned_max_bytes: pinning a fresh multi-GB block
@@ -307,9 +339,9 @@ class Server:
                 ppr = [r for r in pending if r.kind == "ppr"]
                 others = [r for r in pending if r.kind != "ppr"]
                 pending = []
-                if session is None and len(ppr) >= self.session_min:
+                if session is None and len(ppr) >= self.session_min and self._long_solves(gid, ppr[0]):
                     r0 = ppr[0]
-                    session = _native.Session(pg, alpha=r0.alpha, tol=r0.tol, slots=self.session_slots)
+                    session = _native.Session(pg, alpha=r0.alpha, tol=r0.tol, slots=self._session_slots(pg.n))
                     self.stats["sessions"] += 1
                 if session is not None:
                     fits = [r for r in ppr if r.alpha == session.alpha and r.tol == session.tol]

@@ -135,7 +135,7 @@ def _sources(k=5):
 def test_requests_are_folded_and_answers_match_standalone(fake_engine):
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=2, ppr_min_batch=2)
+    srv = serving.Server(reg, workers=2, ppr_min_batch=2, session_min=2, session_min_sweeps=0)
     rng = np.random.default_rng(0)
     reqs = []
     for i in range(60):
@@ -220,7 +220,7 @@ def test_requests_arriving_mid_solve_join_the_running_batched_solve(fake_engine)
     running requests to finish), and every answer is its answer alone."""
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=1, session_sweeps=2)
+    srv = serving.Server(reg, workers=1, session_sweeps=2, session_min=2, session_min_sweeps=0)
     rng = np.random.default_rng(4)
     n = src[3][0].shape[0] - 1
     early = [serving.Request(3, "ppr", seeds=rng.choice(n, 3, replace=False), max_iter=200, tol=1e-9)
@@ -245,6 +245,34 @@ def test_requests_arriving_mid_solve_join_the_running_batched_solve(fake_engine)
     first_admit, second_admit = [i for i, e in enumerate(events) if e == "admit"][:2]
     assert "step" in events[first_admit:second_admit]  # the second wave joined after the solve had started
     assert max(r.done_at for r in early) > min(r.arrival for r in late)  # ... while the first wave was running
+    reg.close()
+
+
+def test_sessions_open_only_for_long_solves(fake_engine):
+    """A burst of short solves (a stop rule whose sweep count is not known yet,
+    or is known to be short) takes one-shot batched solves; fixed-sweep
+    requests of at least session_min_sweeps sweeps open a session."""
+    src = _sources()
+    reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
+    srv = serving.Server(reg, workers=1, session_min=2, session_min_sweeps=32)
+    rng = np.random.default_rng(5)
+    n = src[1][0].shape[0] - 1
+
+    def burst(**kw):
+        FakePrepared.calls = []
+        reqs = [serving.Request(1, "ppr", seeds=rng.choice(n, 2, replace=False), **kw) for _ in range(8)]
+        for r in reqs:
+            srv.submit(r)
+        for r in reqs:
+            r.future.result(timeout=60)
+        return [c[0] for c in FakePrepared.calls]
+
+    assert "session" not in burst(tol=1e-6)  # nothing known yet
+    assert srv.sweeps_seen[(1, 0.85, 1e-6)] < 32
+    assert "session" not in burst(tol=1e-6)  # known to be short
+    assert "session" not in burst(tol=0.0, max_iter=8)  # fixed and short
+    assert "session" in burst(tol=0.0, max_iter=40)  # fixed and long
+    srv.close()
     reg.close()
 
 
@@ -274,7 +302,8 @@ def test_served_results_equal_standalone_results_on_gpu():
         c = synth.rmat(scale=scale, edgefactor=ef, seed=2000 + i)
         src[i] = (c.V, c.E, None)
     reg = serving.GraphRegistry(src, budget_bytes=1 << 34)
-    srv = serving.Server(reg, workers=3, ppr_min_batch=2)  # batched and single PPR solves both occur
+    # batched, session and single PPR solves all occur
+    srv = serving.Server(reg, workers=3, ppr_min_batch=2, session_min=2, session_min_sweeps=0)
     rng = np.random.default_rng(1)
     reqs = []
     for i in range(300):
