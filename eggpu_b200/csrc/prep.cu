@@ -7,8 +7,9 @@
 //   k_out_weight_exact  FP64 out-weight sum per source after sanitising each
 //                    weight, bit-identical to the sequential sum in row order
 //                    (pagerank.cu:301-316): four lanes per source (a warp for
-//                    sources of more than 64 entries) where the sum is provably
-//                    order-free, one thread per source otherwise
+//                    sources of more than 64 entries, 4096-entry segments on
+//                    several warps for more than 16384) where the sum is
+//                    provably order-free, one thread per source otherwise
 //   k_in_degree      in-degree histogram over valid endpoints (:315)
 //   exclusive scan   in_row (:319-320)
 //   radix sort       stable LSD sort of the entries by destination: entries of
@@ -259,7 +260,7 @@ __device__ __forceinline__ void out_weight_row(const int32_t* __restrict__ E, co
     for (int32_t p = b + sub; p < e; p += G) {
         const int32_t v = E[p];
         if (v >= 0 && v < n) {
-            const double w = sanitize_w(W[p]);
+            const double w = W ? sanitize_w(W[p]) : 1.0;  // unit weights: q = 0, every sum exact
             s += w;
             ++c;
             if (w > 0.0) q = min(q, lsb_exponent(w));
@@ -292,6 +293,40 @@ __device__ __forceinline__ void out_weight_store(int64_t u, double s, int32_t c,
 }
 
 constexpr int32_t kOutWeightShort = 64;  // sources with more entries are summed by a whole warp
+// Sources with more than kOutWeightHuge entries are summed in segments of
+// kOutWeightSeg entries by several warps; each segment's sums go into the
+// source's accumulator and the last segment to arrive finishes the source.
+// A segment's sum is one of the source's partial sums, so the exactness test
+// above covers the segments and their FP64 atomic adds, in any order.
+constexpr int32_t kOutWeightHuge = 16384;
+constexpr int32_t kOutWeightSeg = 4096;
+
+struct HugeAcc {
+    double s;          // sum of the segments' sums
+    int32_t c;         // valid entries
+    int32_t q;         // lowest set bit exponent of the nonzero weights
+    uint32_t arrived;  // segments added so far
+    int32_t pad;
+};
+
+struct OutSegs {
+    int4* seg;           // (source, segment, accumulator, segments of the source)
+    uint32_t* seg_count;
+    HugeAcc* acc;
+    uint32_t* acc_count;
+};
+
+// Lists the segments of source u (called by one thread for a huge source).
+__device__ __forceinline__ void list_segments(const OutSegs& H, int32_t u, int32_t len) {
+    const int32_t nseg = (len + kOutWeightSeg - 1) / kOutWeightSeg;
+    const uint32_t h = atomicAdd(H.acc_count, 1u);
+    H.acc[h].s = 0.0;
+    H.acc[h].c = 0;
+    H.acc[h].q = 4096;
+    H.acc[h].arrived = 0u;
+    const uint32_t s0 = atomicAdd(H.seg_count, (uint32_t)nseg);
+    for (int32_t j = 0; j < nseg; ++j) H.seg[s0 + (uint32_t)j] = make_int4(u, j, (int32_t)h, nseg);
+}
 
 // Sources [r0, r1), four lanes each; a source with more than kOutWeightShort
 // entries is listed for k_out_weight_long instead.
@@ -300,7 +335,7 @@ __global__ void k_out_weight_exact(const int32_t* __restrict__ V, const int32_t*
                                    double* __restrict__ outw, uint32_t* __restrict__ hub_key,
                                    uint32_t* __restrict__ hub_val, int32_t* __restrict__ serial_rows,
                                    uint32_t* __restrict__ serial_count, int32_t* __restrict__ long_rows,
-                                   uint32_t* __restrict__ long_count) {
+                                   uint32_t* __restrict__ long_count, OutSegs H) {
     constexpr int G = 4;
     const int lane = threadIdx.x & 31, sub = lane & (G - 1), grp = lane / G;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -312,7 +347,10 @@ __global__ void k_out_weight_exact(const int32_t* __restrict__ V, const int32_t*
             b = V[u];
             e = V[u + 1];
             if (e - b > kOutWeightShort) {
-                if (sub == 0) long_rows[atomicAdd(long_count, 1u)] = (int32_t)u;
+                if (sub == 0) {
+                    if (e - b > kOutWeightHuge) list_segments(H, (int32_t)u, e - b);
+                    else long_rows[atomicAdd(long_count, 1u)] = (int32_t)u;
+                }
                 e = b;  // the group still takes part in the shuffles
             }
         }
@@ -325,16 +363,18 @@ __global__ void k_out_weight_exact(const int32_t* __restrict__ V, const int32_t*
     }
 }
 
-// The long sources listed by k_out_weight_exact, one warp each.
+// The long sources listed by k_out_weight_exact, one warp each, then the
+// segments of the huge ones (weighted or not).
 __global__ void k_out_weight_long(const int32_t* __restrict__ V, const int32_t* __restrict__ E,
                                   const double* __restrict__ W, int32_t n, const int32_t* __restrict__ long_rows,
                                   const uint32_t* __restrict__ long_count, double* __restrict__ outw,
                                   uint32_t* __restrict__ hub_key, uint32_t* __restrict__ hub_val,
-                                  int32_t* __restrict__ serial_rows, uint32_t* __restrict__ serial_count) {
+                                  int32_t* __restrict__ serial_rows, uint32_t* __restrict__ serial_count,
+                                  OutSegs H) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const uint32_t k = *long_count;
+    const uint32_t k = long_count ? *long_count : 0u;
     for (int64_t i = warp; i < (int64_t)k; i += nwarps) {
         const int32_t u = long_rows[i];
         double s;
@@ -342,6 +382,36 @@ __global__ void k_out_weight_long(const int32_t* __restrict__ V, const int32_t* 
         int q;
         out_weight_row<32>(E, W, n, V[u], V[u + 1], lane, s, c, q);
         if (lane == 0) out_weight_store(u, s, c, q, outw, hub_key, hub_val, serial_rows, serial_count);
+    }
+    // segments of the huge sources: the last segment of a source to arrive finishes it
+    const uint32_t ns = *H.seg_count;
+    for (int64_t i = warp; i < (int64_t)ns; i += nwarps) {
+        const int4 sg = H.seg[i];
+        const int32_t u = sg.x, b = V[u] + sg.y * kOutWeightSeg, e = min(V[u + 1], b + kOutWeightSeg);
+        double s;
+        int32_t c;
+        int q;
+        out_weight_row<32>(E, W, n, b, e, lane, s, c, q);
+        if (lane == 0) {
+            HugeAcc& A = H.acc[sg.z];
+            if (s != 0.0) atomicAdd(&A.s, s);
+            atomicAdd(&A.c, c);
+            atomicMin(&A.q, q);
+            __threadfence();
+            if (atomicAdd(&A.arrived, 1u) == (uint32_t)(sg.w - 1)) {
+                __threadfence();
+                const double ts = __ldcg(&A.s);
+                const int32_t tc = __ldcg(&A.c);
+                const int tq = __ldcg(&A.q);
+                if (W) {
+                    out_weight_store(u, ts, tc, tq, outw, hub_key, hub_val, serial_rows, serial_count);
+                } else {  // unit weights: the count
+                    outw[u] = (double)tc;
+                    hub_key[u] = ~(uint32_t)tc;
+                    hub_val[u] = (uint32_t)u;
+                }
+            }
+        }
     }
 }
 
@@ -366,12 +436,16 @@ __global__ void k_out_weight_serial(const int32_t* __restrict__ V, const int32_t
 // order, so one warp counts a row.
 __global__ void k_out_degree(const int32_t* __restrict__ V, const int32_t* __restrict__ E, int32_t n, int32_t r0,
                              int32_t r1, double* __restrict__ outw, uint32_t* __restrict__ hub_key,
-                             uint32_t* __restrict__ hub_val) {
+                             uint32_t* __restrict__ hub_val, OutSegs H) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t u = r0 + warp; u < r1; u += nwarps) {
         const int32_t b = V[u], e = V[u + 1];
+        if (e - b > kOutWeightHuge) {  // counted in segments by k_out_weight_long
+            if (lane == 0) list_segments(H, (int32_t)u, e - b);
+            continue;
+        }
         int32_t c = 0;
         for (int32_t p = b + lane; p < e; p += 32) {
             const int32_t v = E[p];
@@ -553,17 +627,29 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_
     int rc = EGPR_SUCC;
     // 8-bit digits: with 4096-item tiles a digit's run averages 16 items, so
     // the runs written out are 64-byte pieces (11-bit digits, one pass fewer,
-    // leave 2-item runs and were slower in total)
-    const int passes = (bits + 7) / 8;
+    // leave 2-item runs and were slower in total).  Where one or two 9-bit
+    // digits save a whole pass (25-bit keys: 9 + 8 + 8 instead of 8 + 8 + 8 + 1)
+    // they are used: 8-item runs, one pass of the data fewer.
+    int passes = (bits + 7) / 8;
+    int nine = 0;  // leading passes of 9-bit digits
+    if (passes > 1 && bits <= 9 * (passes - 1)) {
+        passes -= 1;
+        nine = bits - 8 * passes;
+    }
     const int64_t ntiles = (len + kSortTile - 1) / kSortTile;
-    uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles << 8, &rc);
+    uint32_t* hist = tmp.get<uint32_t>((size_t)ntiles << (nine ? 9 : 8), &rc);
     if (!hist) return rc;
     uint32_t *kin = keys, *vin = vals, *kout = keys_alt, *vout = vals_alt, *v2in = vals2, *v2out = vals2_alt;
+    int shift = 0;
     for (int p = 0; p < passes; ++p) {
-        const int shift = p * 8;
         const bool last = p == passes - 1 && !keys_needed;
-        rc = vals2 ? radix_pass<8, true>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, v2in, v2out)
-                   : radix_pass<8, false>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, nullptr, nullptr);
+        if (p < nine)
+            rc = vals2 ? radix_pass<9, true>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, v2in, v2out)
+                       : radix_pass<9, false>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, nullptr, nullptr);
+        else
+            rc = vals2 ? radix_pass<8, true>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, v2in, v2out)
+                       : radix_pass<8, false>(kin, vin, kout, vout, len, shift, last, ntiles, hist, s, nullptr, nullptr);
+        shift += p < nine ? 9 : 8;
         if (rc) return rc;
         std::swap(kin, kout);
         std::swap(vin, vout);
@@ -1292,6 +1378,13 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         uint32_t* serial_count = W ? tmp.get<uint32_t>(1, &rc) : nullptr;
         int32_t* long_rows = W ? tmp.get<int32_t>((size_t)n, &rc) : nullptr;  // per piece: sources of many entries
         uint32_t* long_count = W ? tmp.get<uint32_t>(1, &rc) : nullptr;
+        // per piece: segments of the sources of very many entries, and their accumulators
+        OutSegs segs;
+        const size_t max_huge = (size_t)(m / kOutWeightHuge) + 1;
+        segs.seg = tmp.get<int4>((size_t)(m / kOutWeightSeg) + max_huge, &rc);
+        segs.seg_count = tmp.get<uint32_t>(1, &rc);
+        segs.acc = tmp.get<HugeAcc>(max_huge, &rc);
+        segs.acc_count = tmp.get<uint32_t>(1, &rc);
         if (rc) return rc;
         if (W) cudaMemsetAsync(serial_count, 0, sizeof(uint32_t), s);
         // in_row, hub_slot: bulk copies of a stage's rows may read up to 3 elements past the end.
@@ -1343,17 +1436,20 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
                 int32_t r_end = n;
                 if (i + 1 < pieces) r_end = (int32_t)(std::upper_bound(V, V + n + 1, (int32_t)b) - V) - 1;
                 if (r_end > r_done) {
+                    cudaMemsetAsync(segs.seg_count, 0, sizeof(uint32_t), s);
+                    cudaMemsetAsync(segs.acc_count, 0, sizeof(uint32_t), s);
                     if (dW) {
                         cudaMemsetAsync(long_count, 0, sizeof(uint32_t), s);
                         k_out_weight_exact<<<grid_for((int64_t)(r_end - r_done) * 8), kThreads, 0, s>>>(
                             dV, dE, dW, n, r_done, r_end, g->outw.as<double>(), hkey, hval, serial_rows,
-                            serial_count, long_rows, long_count);
-                        k_out_weight_long<<<148 * 8, kThreads, 0, s>>>(dV, dE, dW, n, long_rows, long_count,
-                                                                       g->outw.as<double>(), hkey, hval,
-                                                                       serial_rows, serial_count);
-                    } else
+                            serial_count, long_rows, long_count, segs);
+                    } else {
                         k_out_degree<<<grid_for((int64_t)(r_end - r_done) * 32), kThreads, 0, s>>>(
-                            dV, dE, n, r_done, r_end, g->outw.as<double>(), hkey, hval);
+                            dV, dE, n, r_done, r_end, g->outw.as<double>(), hkey, hval, segs);
+                    }
+                    k_out_weight_long<<<148 * 8, kThreads, 0, s>>>(dV, dE, dW, n, long_rows, long_count,
+                                                                   g->outw.as<double>(), hkey, hval, serial_rows,
+                                                                   serial_count, segs);
                     r_done = r_end;
                 }
                 if (b > a)

@@ -85,6 +85,42 @@ def test_out_weight_sums_bit_exact_with_the_sequential_sum(kind):
     assert np.array_equal(outw.view(np.uint64), oout.view(np.uint64))
 
 
+@pytest.mark.parametrize("kind", ["unweighted", "fp32_values", "full_doubles", "mixed_scales"])
+def test_out_weight_sums_of_huge_rows_bit_exact(kind):
+    """Sources of more than 16384 entries are summed in segments by several
+    warps: the sums (and unit-weight counts) stay bit-identical to the
+    sequential sum, including rows that need the sequential path."""
+    rng = np.random.Generator(np.random.PCG64(42))
+    n = 1 << 17
+    rows = {0: 60000, 1: 20000, 7: 16385, 9: 16384}  # over, at and just past the segment threshold
+    V = np.zeros(n + 1, np.int64)
+    cols = []
+    for u in range(n):
+        k = rows.get(u, int(rng.integers(0, 8)))
+        cols.append(np.sort(rng.choice(n, k, replace=False)) if k else np.zeros(0, np.int64))
+        V[u + 1] = V[u] + k
+    E = np.concatenate(cols).astype(np.int32)
+    V = V.astype(np.int32)
+    m = len(E)
+    if kind == "unweighted":
+        W = None
+    elif kind == "fp32_values":
+        W = (1.0 - rng.random(m, dtype=np.float32)).astype(np.float64)
+    elif kind == "full_doubles":
+        W = rng.random(m)
+    else:
+        W = rng.random(m) * np.where(rng.random(m) < 0.5, 2.0**60, 2.0**-40)
+        W[rng.random(m) < 0.01] = 0.0
+        W[rng.random(m) < 0.001] = np.nan
+    pg = _native.PreparedGraph(V, E, W)
+    r, c, _, _, outw = pg.export_inbound()
+    orow, ocol, _, _, oout = oracle.build_inbound(V, E, W)
+    assert np.array_equal(outw.view(np.uint64), oout.view(np.uint64))
+    assert np.array_equal(r, orow) and np.array_equal(c, ocol)
+    ranks, st = pg.pagerank(alpha=0.85, max_iter=100, tol=1e-6)
+    _check_against_oracle(V, E, W, ranks, st, 0.85, 100, 1e-6)
+
+
 @pytest.mark.parametrize("case", golden_small_cases(), ids=lambda c: c[0])
 def test_reference_small_cases_through_the_api(case, monkeypatch):
     monkeypatch.setenv("EASYGRAPH_ENABLE_GPU", "TRUE")
