@@ -5,14 +5,19 @@ registry.  The server keeps prepared graphs (inbound CSR and rank state) on
 the device, admits graphs by HBM bytes with least-recently-used eviction of
 idle graphs, and serves requests as they arrive:
 
-* continuous batching of PPR for long solves: a graph with several PPR
-  requests waiting whose solves are expected to take many sweeps keeps one
-  batched SpMM solve running (``egpr_session``); requests that arrive while it
-  runs join it in free column slots between steps of a few sweeps, each
-  leaves it (FP64 correction, normalisation, copy out) as soon as its own stop
-  rule fires, and its slot is reused;
-* other PPR requests waiting for a graph share one one-shot batched solve
-  (``egpr_pagerank_seeds``; fewer than six go as single-vector solves);
+* PPR requests waiting for a graph share one one-shot batched solve
+  (``egpr_pagerank_seeds``; fewer than six go as single-vector solves), so
+  the batch grows with the queue;
+* optionally (``sessions=True``), slot-level continuous batching of PPR for
+  long solves: a graph with several PPR requests waiting whose solves are
+  expected to take many sweeps keeps one batched SpMM solve running
+  (``egpr_session``); requests that arrive while it runs join it in free
+  column slots between steps of a few sweeps, each leaves it (FP64
+  correction, normalisation, copy out) as soon as its own stop rule fires,
+  and its slot is reused.  Off by default: on B200 a session step costs
+  host round trips and an FP64 correction pass per collection, and one-shot
+  batches measured as fast or faster in every regime tried (requests of
+  1-100 sweeps, graphs of 2^16-2^20 vertices, 200-2000 req/s);
 * queued plain requests for a graph share one solve (their answer is
   identical);
 * solves on different graphs run concurrently from a pool of worker threads,
@@ -172,7 +177,7 @@ class Server:
     """Serves Request objects; submit() returns a Future resolving to (ranks, stats)."""
 
     def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True, pinned=True,
-                 multi_min=8, ppr_min_batch=1, sessions=True, session_slots=256, session_sweeps=4, session_min=6,
+                 multi_min=8, ppr_min_batch=1, sessions=False, session_slots=256, session_sweeps=4, session_min=6,
                  session_min_sweeps=48, session_max_bytes=2 << 30):
         self.registry = registry
         # continuous batching: a graph with at least session_min PPR requests

@@ -135,7 +135,7 @@ def _sources(k=5):
 def test_requests_are_folded_and_answers_match_standalone(fake_engine):
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=2, ppr_min_batch=2, session_min=2, session_min_sweeps=0)
+    srv = serving.Server(reg, workers=2, ppr_min_batch=2, sessions=True, session_min=2, session_min_sweeps=0)
     rng = np.random.default_rng(0)
     reqs = []
     for i in range(60):
@@ -220,7 +220,7 @@ def test_requests_arriving_mid_solve_join_the_running_batched_solve(fake_engine)
     running requests to finish), and every answer is its answer alone."""
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=1, session_sweeps=2, session_min=2, session_min_sweeps=0)
+    srv = serving.Server(reg, workers=1, session_sweeps=2, sessions=True, session_min=2, session_min_sweeps=0)
     rng = np.random.default_rng(4)
     n = src[3][0].shape[0] - 1
     early = [serving.Request(3, "ppr", seeds=rng.choice(n, 3, replace=False), max_iter=200, tol=1e-9)
@@ -254,7 +254,7 @@ def test_sessions_open_only_for_long_solves(fake_engine):
     requests of at least session_min_sweeps sweeps open a session."""
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=1, session_min=2, session_min_sweeps=32)
+    srv = serving.Server(reg, workers=1, sessions=True, session_min=2, session_min_sweeps=32)
     rng = np.random.default_rng(5)
     n = src[1][0].shape[0] - 1
 
@@ -303,7 +303,7 @@ def test_served_results_equal_standalone_results_on_gpu():
         src[i] = (c.V, c.E, None)
     reg = serving.GraphRegistry(src, budget_bytes=1 << 34)
     # batched, session and single PPR solves all occur
-    srv = serving.Server(reg, workers=3, ppr_min_batch=2, session_min=2, session_min_sweeps=0)
+    srv = serving.Server(reg, workers=3, ppr_min_batch=2, sessions=True, session_min=2, session_min_sweeps=0)
     rng = np.random.default_rng(1)
     reqs = []
     for i in range(300):
