@@ -543,11 +543,14 @@ def run_batch(args):
         nnz += pg.nnz
         graphs.append(pg)
     _native.pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6)
-    reps = max(1, args.steps // 50)
-    t0 = time.perf_counter()
-    for _ in range(reps):
+    # median over repetitions: an occasional call costs several times the
+    # others (host page faults of the fresh result block)
+    walls = []
+    for _ in range(max(5, args.steps // 20)):
+        t0 = time.perf_counter()
         outs, sts = _native.pagerank_multi(graphs, alpha=0.85, max_iter=100, tol=1e-6)
-    wall = (time.perf_counter() - t0) / reps
+        walls.append(time.perf_counter() - t0)
+    wall = statistics.median(walls)
     dev = sts[0]["kernel_seconds"]
     its = [s["iterations"] for s in sts]
     t0 = time.perf_counter()
