@@ -18,8 +18,9 @@ the same graph, the oracle's OpenMP restatement of the reference's CPU path
 timed on the host, the scale-22 config (R-MAT scale 22, seed 1, unweighted)
 measured the same way as a secondary object, and (one GPU) the batched-PPR
 config (R-MAT scale 20, k=256 seed sets) and the serving config (Poisson
-arrivals over 64 graphs, with and without session-level continuous batching), each
-measured after the timed region.
+arrivals over 64 graphs, and long solves on one large graph, each with and
+without session-level continuous batching), each measured after the timed
+region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload rmat25w|rmat22|rmat<scale>[w]|ppr|batch|serving|precision25]
@@ -32,6 +33,7 @@ same workload and prints the same metric.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import re
@@ -585,6 +587,15 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def quiet_gc():
+    """Before a measured replay: collect, then move every live object (the
+    load generator's request lists, futures and locks among them) out of the
+    collector's reach, so that a full collection over them does not land
+    inside the replay as a pause of the serving threads."""
+    gc.collect()
+    gc.freeze()
+
+
 def measure_serving(args):
     from eggpu_b200 import _native, serving, synth
 
@@ -624,24 +635,35 @@ def measure_serving(args):
     srv_w = serving.Server(reg, workers=workers)
     serving.replay(srv_w, warm, np.zeros(n_req))
     srv_w.close()
+    # ... then the first 2,000 arrivals at their own times (the result sizes
+    # of single requests, whose page-locked buffers the burst did not ask for)
+    warm = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs[:2000]]
+    srv_w = serving.Server(reg, workers=workers)
+    serving.replay(srv_w, warm, times[:2000])
+    srv_w.close()
     srv = serving.Server(reg, workers=workers)
+    quiet_gc()
     wall = serving.replay(srv, reqs, times)
     srv.close()
     lat = serving.latency_summary(reqs)
-    # the same arrivals with slot-level continuous batching (egpr_session; the
-    # server opens sessions only for long solves, which this traffic has not)
+    # the same arrivals with one-shot batching only (no egpr_session; the
+    # default server opens sessions only for long solves on large graphs,
+    # which this traffic has not)
     again = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
-    srv1 = serving.Server(reg, workers=workers, sessions=True)
+    srv1 = serving.Server(reg, workers=workers, sessions=False)
+    quiet_gc()
     wall1 = serving.replay(srv1, again, times)
     srv1.close()
-    lat_sessions = serving.latency_summary(again)
+    lat_one_shot = serving.latency_summary(again)
     # capacity: the same requests all at once (queued requests fold into batched solves)
     burst = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
     srv2 = serving.Server(reg, workers=workers)
+    quiet_gc()
     burst_wall = serving.replay(srv2, burst, np.zeros(n_req))
     srv2.close()
     burst1 = [serving.Request(r.graph, r.kind, seeds=r.seeds, keep_result=False) for r in reqs]
-    srv3 = serving.Server(reg, workers=workers, sessions=True)
+    srv3 = serving.Server(reg, workers=workers, sessions=False)
+    quiet_gc()
     burst1_wall = serving.replay(srv3, burst1, np.zeros(n_req))
     srv3.close()
     long_solves = measure_long_solves(workers)
@@ -664,17 +686,18 @@ def measure_serving(args):
                        f"R-MAT graphs n log-uniform in [1e3, {max_n:.0e}] (ids >= n dropped), edgefactor "
                        "uniform in [8, 32], seeds 2000-2063, alpha 0.85, tol 1e-6",
            "requests": n_req, "hbm_budget_gb": args.serving_hbm_gb,
-           "warmup": f"a burst of all {n_warm} requests before the measured replays",
+           "warmup": f"a burst of all {n_warm} requests, then the first 2,000 at their arrival times, before the "
+                     "measured replays",
+           "gc": "Python's collector run and live objects frozen before each measured replay",
            "graphs_loaded_before_traffic_s": warm_s,
            "total_nnz": int(sum(len(v[1]) for v in src.values()))}
     out = {"latency": lat, "solves_per_s": n_req / wall, "offered_req_per_s": 1000.0,
            "server_stats": dict(srv.stats), "admissions": reg.admissions, "evictions": reg.evictions,
-           "with_sessions": {"latency": lat_sessions, "solves_per_s": n_req / wall1,
-                             "server_stats": dict(srv1.stats)},
+           "one_shot": {"latency": lat_one_shot, "solves_per_s": n_req / wall1, "server_stats": dict(srv1.stats)},
            "capacity_burst": {"solves_per_s": n_req / burst_wall, "wall_s": burst_wall,
                               "server_stats": dict(srv2.stats),
-                              "with_sessions": {"solves_per_s": n_req / burst1_wall, "wall_s": burst1_wall,
-                                                "server_stats": dict(srv3.stats)}},
+                              "one_shot": {"solves_per_s": n_req / burst1_wall, "wall_s": burst1_wall,
+                                           "server_stats": dict(srv3.stats)}},
            "plain_unbatched_service_ms": {"p50": float(np.percentile(plain, 50) * 1e3),
                                           "p99": float(np.percentile(plain, 99) * 1e3),
                                           "mean": float(plain.mean() * 1e3)},
@@ -685,29 +708,31 @@ def measure_serving(args):
 
 
 def measure_long_solves(workers):
-    """Long solves, where slot-level continuous batching is meant to pay:
-    fixed-sweep PPR requests (100 sweeps, tol 0, 1-16 seeds) at 2000 req/s on
-    one R-MAT scale-16 graph (seed 3, edgefactor 16), served with sessions and
-    with one-shot batched solves only."""
+    """Long solves on a large graph, where slot-level continuous batching
+    pays: fixed-sweep PPR requests (100 sweeps, tol 0, 1-16 seeds) at 200 req/s
+    on one R-MAT scale-20 graph (seed 3, edgefactor 16), served by the default
+    server (which runs them in an egpr_session) and with one-shot batched
+    solves only."""
     from eggpu_b200 import serving, synth
 
-    c = synth.rmat(scale=16, edgefactor=16, seed=3)
-    reg = serving.GraphRegistry({0: (c.V, c.E, None)}, budget_bytes=8 << 30)
+    c = synth.rmat(scale=20, edgefactor=16, seed=3)
+    reg = serving.GraphRegistry({0: (c.V, c.E, None)}, budget_bytes=16 << 30)
     reg.warm([0])
     n = c.V.shape[0] - 1
     rng = np.random.Generator(np.random.PCG64(6))
     seeds = [rng.choice(n, int(rng.integers(1, 17)), replace=False) for _ in range(2000)]
-    times = serving.poisson_arrivals(2000.0, len(seeds), seed=7)
-    out = {"config": "R-MAT scale 16 (seed 3, edgefactor 16), 2000 PPR requests of 100 sweeps (tol 0) with 1-16 "
-                     "seeds (numpy PCG64 seed 6), Poisson arrivals at 2000 req/s (seed 7), after a warm-up replay "
-                     "of 300 requests"}
-    for label, sessions in (("with_sessions", True), ("one_shot", False)):
+    times = serving.poisson_arrivals(200.0, len(seeds), seed=7)
+    out = {"config": "R-MAT scale 20 (seed 3, edgefactor 16), 2000 PPR requests of 100 sweeps (tol 0) with 1-16 "
+                     "seeds (numpy PCG64 seed 6), Poisson arrivals at 200 req/s (seed 7), after a warm-up replay "
+                     "of 300 requests; Python's collector run and live objects frozen before each measured replay"}
+    for label, sessions in (("default", True), ("one_shot", False)):
         warm = [serving.Request(0, "ppr", seeds=s, tol=0.0, max_iter=100, keep_result=False) for s in seeds[:300]]
         srv = serving.Server(reg, workers=workers, sessions=sessions)
         serving.replay(srv, warm, times[:300])
         srv.close()
         reqs = [serving.Request(0, "ppr", seeds=s, tol=0.0, max_iter=100, keep_result=False) for s in seeds]
         srv = serving.Server(reg, workers=workers, sessions=sessions)
+        quiet_gc()
         wall = serving.replay(srv, reqs, times)
         srv.close()
         out[label] = {"latency": serving.latency_summary(reqs), "solves_per_s": len(reqs) / wall,

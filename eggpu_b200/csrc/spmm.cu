@@ -817,17 +817,21 @@ __global__ void k_sp_init(float* X0, float* X1, ColState* cols, int32_t n, int32
 }
 
 // A session's newly admitted columns start at x0 = 1/n in the iterate their
-// panel reads next (X[panel sweeps & 1]); row n stays zero.  cols_new[i] is
-// a column index p * 32 + lane, par_new[i] its buffer.
-__global__ void k_sp_init_cols(float* X0, float* X1, int32_t n, const int32_t* __restrict__ cols_new,
-                               const int32_t* __restrict__ par_new, int32_t count) {
+// panel reads next (X[panel sweeps & 1]); row n stays zero.  Per listed panel
+// pn[i]: the bit mask of its new columns and their buffer (all of a panel's
+// new columns share its sweep count).  A warp writes one 128-byte row of a
+// panel, masked, so the writes are whole lines instead of one sector per value.
+__global__ void k_sp_init_cols(float* X0, float* X1, int32_t n, const int32_t* __restrict__ pn,
+                               const uint32_t* __restrict__ mask, const int32_t* __restrict__ par, int32_t count) {
     const float x0 = (float)(1.0 / (double)n);
-    const int32_t i = blockIdx.y;
-    if (i >= count) return;
-    const int32_t j = cols_new[i], p = j / kLanes, c = j - p * kLanes;
-    float* x = (par_new[i] ? X1 : X0) + (size_t)p * ((size_t)n + 1) * kLanes + c;
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
-        x[(size_t)v * kLanes] = x0;
+    const int64_t per = (int64_t)n * kLanes;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)count * per;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t i = (int32_t)(t / per);
+        const int64_t r = t - (int64_t)i * per;  // row * 32 + column
+        if ((mask[i] >> (r & (kLanes - 1))) & 1u)
+            (par[i] ? X1 : X0)[(size_t)pn[i] * ((size_t)n + 1) * kLanes + (size_t)r] = x0;
+    }
 }
 
 // Rank sum of each column's final FP32 iterate (runs when the FP64 correction
@@ -1320,6 +1324,11 @@ struct SessionState {
     int32_t tele_cap_rows = 0;        // rows the device teleport buffer holds
     int32_t rows_on_device = 0;       // rows whose meta bits are set
     bool tele_dirty = false;
+    // what the device holds: the column states equal the host mirror unless
+    // an admission or a collection changed them since; the parameter block is
+    // that of params_cap (-1: stale)
+    bool cols_dirty = true;
+    int32_t params_cap = -1;
     DevBuf out_row, tele_upd;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     ~SessionState() {
@@ -1337,6 +1346,7 @@ struct SessionState {
 };
 
 int session_params(SessionState& S, int32_t step_cap, cudaStream_t s) {
+    if (S.params_cap == step_cap) return EGPR_SUCC;  // the device already holds this block
     egpr_graph* g = S.g;
     SpmmWork& base = *g->spmm;
     SpmmWork& w = S.w;
@@ -1368,7 +1378,9 @@ int session_params(SessionState& S, int32_t step_cap, cudaStream_t s) {
     P.gacc = w.gacc.as<unsigned long long>();
     P.ctl = w.ctl.as<Ctl>();
     P.step_cap = step_cap;
-    return cuda_ok(cudaMemcpyAsync(w.params.p, &P, sizeof(P), cudaMemcpyHostToDevice, s), "H2D params");
+    const int rc = cuda_ok(cudaMemcpyAsync(w.params.p, &P, sizeof(P), cudaMemcpyHostToDevice, s), "H2D params");
+    S.params_cap = rc ? -1 : step_cap;
+    return rc;
 }
 
 int session_upload(SessionState& S, int32_t active, cudaStream_t s) {
@@ -1391,6 +1403,7 @@ int session_upload(SessionState& S, int32_t active, cudaStream_t s) {
             w.tele.release_on(s);
             w.tele = nb;
             S.tele_cap_rows = cap;
+            S.params_cap = -1;  // the parameter block holds the teleport buffer's address
         }
         const size_t nw = S.tele_writes.size();
         if (nw > 0) {
@@ -1429,11 +1442,13 @@ int session_upload(SessionState& S, int32_t active, cudaStream_t s) {
     Ctl c{};
     c.active = active;
     c.cap = 1 << 30;
-    if ((rc = cuda_ok(cudaMemcpyAsync(w.cols.p, S.cols.data(), S.cols.size() * sizeof(ColState), cudaMemcpyHostToDevice,
-                                      s), "H2D cols")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(w.ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D ctl")))
-        return rc;
-    return EGPR_SUCC;
+    if (S.cols_dirty) {
+        if ((rc = cuda_ok(cudaMemcpyAsync(w.cols.p, S.cols.data(), S.cols.size() * sizeof(ColState),
+                                          cudaMemcpyHostToDevice, s), "H2D cols")))
+            return rc;
+        S.cols_dirty = false;
+    }
+    return cuda_ok(cudaMemcpyAsync(w.ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D ctl");
 }
 
 int session_create(egpr_graph* g, double alpha, double tol, int32_t slots, SessionState** out) {
@@ -1500,7 +1515,8 @@ int session_admit(SessionState& S, int32_t count, const int32_t* seed_ptr, const
         sets[(size_t)i] = std::move(sv);
     }
     const int32_t ld = S.npanels * kLanes;
-    std::vector<int32_t> cols_new, par_new;
+    std::vector<uint32_t> panel_mask((size_t)S.npanels, 0u);
+    std::vector<int32_t> panel_par((size_t)S.npanels, 0);
     const double x0 = (double)(float)(1.0 / (double)n);
     const double t0 = wall_seconds();
     for (int32_t i = 0; i < count; ++i) {
@@ -1534,25 +1550,29 @@ int session_admit(SessionState& S, int32_t count, const int32_t* seed_ptr, const
         S.state[(size_t)j] = kSlotRunning;
         S.started[(size_t)j] = t0;
         S.device_s[(size_t)j] = 0.0;
-        cols_new.push_back(j);
-        par_new.push_back(base & 1);
+        panel_mask[(size_t)p] |= 1u << (j - p * kLanes);
+        panel_par[(size_t)p] = base & 1;  // every new column of the panel starts at its sweep count
         slots_out[i] = j;
     }
     S.tele_dirty = true;
+    S.cols_dirty = true;
     // the new columns' start vectors (stream order: before the next step)
     cudaStream_t s = g->stream;
     int rc;
-    const size_t cn = cols_new.size();
-    if ((rc = S.w.colsum.grow_on(2 * cn * sizeof(int32_t), s)) ||
-        (rc = cuda_ok(cudaMemcpyAsync(S.w.colsum.p, cols_new.data(), cn * sizeof(int32_t), cudaMemcpyHostToDevice, s),
-                      "H2D columns")) ||
-        (rc = cuda_ok(cudaMemcpyAsync(S.w.colsum.as<int32_t>() + cn, par_new.data(), cn * sizeof(int32_t),
-                                      cudaMemcpyHostToDevice, s), "H2D columns")))
+    std::vector<int32_t> lst;  // panel, mask, buffer of each panel with new columns
+    for (int32_t p = 0; p < S.npanels; ++p)
+        if (panel_mask[(size_t)p]) lst.push_back(p);
+    const size_t cn = lst.size();
+    for (size_t i = 0; i < cn; ++i) lst.push_back((int32_t)panel_mask[(size_t)lst[i]]);
+    for (size_t i = 0; i < cn; ++i) lst.push_back(panel_par[(size_t)lst[i]]);
+    if ((rc = S.w.colsum.grow_on(lst.size() * sizeof(int32_t), s)) ||
+        (rc = cuda_ok(cudaMemcpyAsync(S.w.colsum.p, lst.data(), lst.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                      s), "H2D columns")))
         return rc;
-    k_sp_init_cols<<<dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 255) / 256, 148 * 4)),
-                          (unsigned)cn), 256, 0, s>>>(S.w.X0.as<float>(), S.w.X1.as<float>(), n,
-                                                      S.w.colsum.as<int32_t>(), S.w.colsum.as<int32_t>() + cn,
-                                                      (int32_t)cn);
+    const int32_t* dl = S.w.colsum.as<int32_t>();
+    k_sp_init_cols<<<grid_1d((int64_t)cn * n * kLanes), 256, 0, s>>>(
+        S.w.X0.as<float>(), S.w.X1.as<float>(), n, dl, reinterpret_cast<const uint32_t*>(dl + cn), dl + 2 * cn,
+        (int32_t)cn);
     if ((rc = cuda_ok(cudaGetLastError(), "session admit"))) return rc;
     // the colsum buffer is reused by the next call: the copies must be done
     return cuda_ok(cudaStreamSynchronize(s), "session admit");
@@ -1681,6 +1701,7 @@ int session_collect(SessionState& S, int32_t count, const int32_t* slots, uint32
         S.state[(size_t)j] = kSlotFree;
     }
     S.tele_dirty = true;
+    S.cols_dirty = true;  // the device holds the collection's view of the states
     return EGPR_SUCC;
 }
 

@@ -8,16 +8,16 @@ idle graphs, and serves requests as they arrive:
 * PPR requests waiting for a graph share one one-shot batched solve
   (``egpr_pagerank_seeds``; fewer than six go as single-vector solves), so
   the batch grows with the queue;
-* optionally (``sessions=True``), slot-level continuous batching of PPR for
-  long solves: a graph with several PPR requests waiting whose solves are
-  expected to take many sweeps keeps one batched SpMM solve running
-  (``egpr_session``); requests that arrive while it runs join it in free
-  column slots between steps of a few sweeps, each leaves it (FP64
-  correction, normalisation, copy out) as soon as its own stop rule fires,
-  and its slot is reused.  Off by default: on B200 a session step costs
-  host round trips and an FP64 correction pass per collection, and one-shot
-  batches measured as fast or faster in every regime tried (requests of
-  1-100 sweeps, graphs of 2^16-2^20 vertices, 200-2000 req/s);
+* slot-level continuous batching of PPR for long solves on large graphs: a
+  graph of at least ``session_min_nnz`` inbound entries with several PPR
+  requests waiting whose solves are expected to take many sweeps keeps one
+  batched SpMM solve running (``egpr_session``); requests that arrive while it
+  runs join it in free column slots between steps of a few sweeps, each
+  leaves it (FP64 correction, normalisation, copy out) as soon as its own stop
+  rule fires, and its slot is reused.  On B200 this beat one-shot batches for
+  60-100-sweep requests on an R-MAT scale-20 graph (p50 -14%, p99 -10% at
+  200 req/s) and lost on scale-16/18 graphs, where a step's host round trips
+  and each collection's FP64 correction pass outweigh the sweeps;
 * queued plain requests for a graph share one solve (their answer is
   identical);
 * solves on different graphs run concurrently from a pool of worker threads,
@@ -177,8 +177,8 @@ class Server:
     """Serves Request objects; submit() returns a Future resolving to (ranks, stats)."""
 
     def __init__(self, registry, workers=4, max_columns=256, multi_max_n=200_000, fold_multi=True, pinned=True,
-                 multi_min=8, ppr_min_batch=1, sessions=False, session_slots=256, session_sweeps=4, session_min=6,
-                 session_min_sweeps=48, session_max_bytes=2 << 30):
+                 multi_min=8, ppr_min_batch=1, sessions=True, session_slots=256, session_sweeps=4, session_min=6,
+                 session_min_sweeps=48, session_min_nnz=8_000_000, session_max_bytes=2 << 30):
         self.registry = registry
         # continuous batching: a graph with at least session_min PPR requests
         # waiting gets a running batched solve (egpr_session) of session_slots
@@ -198,8 +198,12 @@ class Server:
         # sweeps.  The expected sweep count is max_iter for fixed-sweep
         # requests (tol 0), else a running mean of the counts seen for the same
         # graph and parameters (unknown: one-shot solves, which record it).
-        # session_min_sweeps <= 0 drops the condition.
+        # session_min_sweeps <= 0 drops the condition.  Graphs of fewer than
+        # session_min_nnz inbound entries take one-shot solves: there a step's
+        # host round trips and the FP64 correction pass of each collection
+        # outweigh the sweeps, and one-shot batches measured faster.
         self.session_min_sweeps = int(session_min_sweeps)
+        self.session_min_nnz = int(session_min_nnz)
         self.sweeps_seen = {}  # (graph, alpha, tol) -> running mean of PPR sweep counts
         # PPR groups smaller than this go through the dense single-vector
         # entry one request at a time; otherwise through egpr_pagerank_seeds,
@@ -220,6 +224,7 @@ class Server:
         self.queues = collections.defaultdict(collections.deque)  # graph id -> pending requests
         self.running = set()  # graph ids with a solve in flight
         self.cv = threading.Condition()
+        self._tls = threading.local()  # per worker thread: a reusable page-locked result buffer
         self.stop = False
         self.stats = collections.Counter()
         self.threads = [threading.Thread(target=self._worker, daemon=True) for _ in range(int(workers))]
@@ -305,18 +310,31 @@ class Server:
         fit = self.session_max_bytes // (16 * max(int(n), 1)) // 32 * 32
         return max(32, min(self.session_slots, fit))
 
-    def _long_solves(self, gid, r):
-        """Whether PPR requests like r on graph gid are expected to take at least session_min_sweeps sweeps."""
+    def _long_solves(self, gid, r, pg):
+        """Whether PPR requests like r on graph gid (prepared as pg) are expected to take at least
+        session_min_sweeps sweeps, on a graph large enough for a session to pay."""
+        if getattr(pg, "nnz", self.session_min_nnz) < self.session_min_nnz:
+            return False
         if self.session_min_sweeps <= 0:
             return True
         expected = r.max_iter if r.tol <= 0 else self.sweeps_seen.get((gid, r.alpha, r.tol))
         return expected is not None and expected >= self.session_min_sweeps
 
-    def _out(self, shape):
+    def _out(self, shape, reqs=()):
         # page-locked up to pinned_max_bytes: pinning a fresh multi-GB block
-        # costs more than the faster copy saves
-        nbytes = 8 * int(np.prod(shape))
-        return _native.pinned_empty(shape) if self.pinned and nbytes <= self.pinned_max_bytes else None
+        # costs more than the faster copy saves.  When none of the requests
+        # keeps its result, the worker thread's own page-locked buffer is
+        # reused (no allocation, no page-locking on the request's path).
+        count = int(np.prod(shape))
+        if not (self.pinned and 8 * count <= self.pinned_max_bytes):
+            return None
+        if any(r.keep_result for r in reqs) or not reqs:
+            return _native.pinned_empty(shape)
+        buf = getattr(self._tls, "scratch", None)
+        if buf is None or buf.size < count:
+            buf = _native.pinned_empty(self.pinned_max_bytes // 8)
+            self._tls.scratch = buf
+        return buf[:count].reshape(shape)
 
     def _run(self, work):
         if len(work) > 1:
@@ -344,7 +362,7 @@ class Server:
                 ppr = [r for r in pending if r.kind == "ppr"]
                 others = [r for r in pending if r.kind != "ppr"]
                 pending = []
-                if session is None and len(ppr) >= self.session_min and self._long_solves(gid, ppr[0]):
+                if session is None and len(ppr) >= self.session_min and self._long_solves(gid, ppr[0], pg):
                     r0 = ppr[0]
                     session = _native.Session(pg, alpha=r0.alpha, tol=r0.tol, slots=self._session_slots(pg.n))
                     self.stats["sessions"] += 1
@@ -370,9 +388,11 @@ class Server:
                         done = session.step(self.session_sweeps)
                         self.stats["session_steps"] += 1
                         if done:
-                            out, sts = session.collect(done, out=self._out((len(done), pg.n)))
+                            out, sts = session.collect(done, out=self._out((len(done), pg.n), [running[sl] for sl in done]))
                             for i, sl in enumerate(done):
                                 self._finish(running.pop(sl), out[i], sts[i])
+                if session is None:
+                    break  # no running solve: the worker goes back to the scheduler, as the one-shot path does
                 if not running and not waiting:
                     with self.cv:
                         if not self.queues.get(gid):
@@ -391,21 +411,21 @@ class Server:
             by_params[(r.kind, r.alpha, r.max_iter, r.tol)].append(r)
         for (kind, alpha, max_iter, tol), group in by_params.items():
             if kind == "pr":
-                ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol, out=self._out(pg.n))
+                ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol, out=self._out(pg.n, group))
                 self.stats["pr_solves"] += 1
                 for r in group:
                     self._finish(r, ranks, st)
             elif len(group) < self.ppr_min_batch:
                 for r in group:
                     ranks, st = pg.pagerank(alpha=alpha, max_iter=max_iter, tol=tol,
-                                            personalization=_teleport(pg.n, r.seeds), out=self._out(pg.n))
+                                            personalization=_teleport(pg.n, r.seeds), out=self._out(pg.n, [r]))
                     self.stats["ppr_single"] += 1
                     self._finish(r, ranks, st)
             else:
                 for s in range(0, len(group), self.max_columns):
                     part = group[s:s + self.max_columns]
                     ranks, sts = pg.pagerank_seeds([r.seeds for r in part], alpha=alpha, max_iter=max_iter,
-                                                   tol=tol, out=self._out((len(part), pg.n)))
+                                                   tol=tol, out=self._out((len(part), pg.n), part))
                     self.stats["ppr_batches"] += 1
                     self.stats["ppr_columns"] += len(part)
                     for j, r in enumerate(part):

@@ -21,6 +21,7 @@ class FakePrepared:
     def __init__(self, V, E, W=None):
         self.V, self.E, self.W = V, E, W
         self.n = len(V) - 1
+        self.nnz = len(E)
         with FakePrepared.lock:
             FakePrepared.live += 1
 
@@ -135,7 +136,8 @@ def _sources(k=5):
 def test_requests_are_folded_and_answers_match_standalone(fake_engine):
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=2, ppr_min_batch=2, sessions=True, session_min=2, session_min_sweeps=0)
+    srv = serving.Server(reg, workers=2, ppr_min_batch=2, sessions=True, session_min=2, session_min_sweeps=0,
+                         session_min_nnz=0)
     rng = np.random.default_rng(0)
     reqs = []
     for i in range(60):
@@ -220,7 +222,8 @@ def test_requests_arriving_mid_solve_join_the_running_batched_solve(fake_engine)
     running requests to finish), and every answer is its answer alone."""
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=1, session_sweeps=2, sessions=True, session_min=2, session_min_sweeps=0)
+    srv = serving.Server(reg, workers=1, session_sweeps=2, sessions=True, session_min=2, session_min_sweeps=0,
+                         session_min_nnz=0)
     rng = np.random.default_rng(4)
     n = src[3][0].shape[0] - 1
     early = [serving.Request(3, "ppr", seeds=rng.choice(n, 3, replace=False), max_iter=200, tol=1e-9)
@@ -251,10 +254,11 @@ def test_requests_arriving_mid_solve_join_the_running_batched_solve(fake_engine)
 def test_sessions_open_only_for_long_solves(fake_engine):
     """A burst of short solves (a stop rule whose sweep count is not known yet,
     or is known to be short) takes one-shot batched solves; fixed-sweep
-    requests of at least session_min_sweeps sweeps open a session."""
+    requests of at least session_min_sweeps sweeps open a session, unless the
+    graph has fewer than session_min_nnz inbound entries."""
     src = _sources()
     reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
-    srv = serving.Server(reg, workers=1, sessions=True, session_min=2, session_min_sweeps=32)
+    srv = serving.Server(reg, workers=1, sessions=True, session_min=2, session_min_sweeps=32, session_min_nnz=0)
     rng = np.random.default_rng(5)
     n = src[1][0].shape[0] - 1
 
@@ -272,6 +276,10 @@ def test_sessions_open_only_for_long_solves(fake_engine):
     assert "session" not in burst(tol=1e-6)  # known to be short
     assert "session" not in burst(tol=0.0, max_iter=8)  # fixed and short
     assert "session" in burst(tol=0.0, max_iter=40)  # fixed and long
+    srv.close()
+    srv = serving.Server(reg, workers=1, sessions=True, session_min=2, session_min_sweeps=32,
+                         session_min_nnz=10**9)
+    assert "session" not in burst(tol=0.0, max_iter=40)  # long, but on a graph too small for a session
     srv.close()
     reg.close()
 
@@ -303,7 +311,8 @@ def test_served_results_equal_standalone_results_on_gpu():
         src[i] = (c.V, c.E, None)
     reg = serving.GraphRegistry(src, budget_bytes=1 << 34)
     # batched, session and single PPR solves all occur
-    srv = serving.Server(reg, workers=3, ppr_min_batch=2, sessions=True, session_min=2, session_min_sweeps=0)
+    srv = serving.Server(reg, workers=3, ppr_min_batch=2, sessions=True, session_min=2, session_min_sweeps=0,
+                         session_min_nnz=0)
     rng = np.random.default_rng(1)
     reqs = []
     for i in range(300):
@@ -329,4 +338,30 @@ def test_served_results_equal_standalone_results_on_gpu():
         assert abs(st["iterations"] - rst["iterations"]) <= 1
         assert np.abs(ranks - ref).sum() <= 1e-6
     assert srv.stats["ppr_columns"] >= srv.stats["ppr_batches"]
+    reg.close()
+
+
+def test_dropped_results_reuse_the_worker_buffer(fake_engine):
+    """Results nobody keeps land in the worker thread's own reusable buffer;
+    a kept result always gets an array of its own."""
+    src = _sources()
+    reg = serving.GraphRegistry(src, budget_bytes=1 << 40)
+    srv = serving.Server(reg, workers=1)
+    dropped = [serving.Request(0, "pr", keep_result=False) for _ in range(2)]
+    kept = [serving.Request(0, "pr") for _ in range(2)]
+    a = srv._out((3, 100), dropped)
+    b = srv._out(100, dropped[:1])
+    assert np.shares_memory(a, b)  # the same buffer, reshaped
+    c = srv._out(100, kept)
+    d = srv._out(100, dropped + kept[:1])
+    assert not np.shares_memory(c, a) and not np.shares_memory(d, a) and not np.shares_memory(c, d)
+    for r in dropped + kept:
+        srv.submit(r)
+    for r in dropped:
+        ranks, st = r.future.result(timeout=60)
+        assert ranks is None and st["iterations"] > 0
+    for r in kept:
+        ranks, _ = r.future.result(timeout=60)
+        assert ranks is not None and np.isclose(ranks.sum(), 1.0)
+    srv.close()
     reg.close()
