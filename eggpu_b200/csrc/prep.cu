@@ -1508,8 +1508,8 @@ int prepare_graph(egpr_graph* g, const int32_t* V, const int32_t* E, const doubl
         // hubs, and 16,352 from 2^24 vertices: the shared memory the hubs take is
         // L1 the sweep's other loads lose, and measured on B200 the smaller cache
         // wins once the rank vector no longer fits L2 (R-MAT scale 25 weighted:
-        // 2.32 ms per sweep with 16K hubs, 2.37 with 24K, 2.56 with 32K; scale 22:
-        // 0.232, 0.228, 0.227 ms)
+        // 2.02 ms per sweep with 16K hubs, 2.06 with 8K, 2.08 with 24K, 2.32 with
+        // 32K; scale 22: 0.236, 0.224, 0.222 ms with 8K, 24K, 32K)
         const char* hub_env = std::getenv("EGPR_HUBS");
         const int32_t hub_default = n >= (1 << 24) ? 16384 - 32 : 24576 - 32;
         const int32_t hub_want = hub_env ? std::max(0, std::atoi(hub_env)) : hub_default;
