@@ -1246,6 +1246,10 @@ int staged_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
 // work already enqueued on s: up to kStageSlots chunk copies in flight while
 // host threads move finished chunks out.  Returns once every byte is in dst.
 int staged_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    // the work that produces the result finishes before the pool is taken, so
+    // another thread's upload or download does not wait on this stream's kernels
+    int rc0 = cuda_ok(cudaStreamSynchronize(s), "D2H (staged)");
+    if (rc0) return rc0;
     StagePool& P = stage_pool();
     std::lock_guard<std::mutex> lk(P.mu);
     for (int k = 0; k < kStageSlots; ++k)
